@@ -1,0 +1,301 @@
+"""galaxy-engine_b200 -- B200 Barnes-Hut gravity step for Galaxy Engine.
+
+Python binding of the C ABI in ``include/ge_bh.h`` (libgebh.so, built in-tree
+by ``build.py``).  The names mirror the reference's gravity call surface
+(NarcisCalin/Galaxy-Engine):
+
+=============================  ==============================================
+this module                    reference
+=============================  ==============================================
+``Simulation.upload``          ``Physics::flattenParticles`` (physics.cpp:354-390)
+``Simulation.download``        ``Physics::readFlattenBack`` (physics.cpp:542-565)
+``integrate_start``            ``Physics::integrateStart`` (physics.cpp:1069-1112)
+``bounding_box``               ``boundingBox`` (globalLogic.cpp:1083-1099)
+``compute_morton_keys``        ``Morton::computeMortonKeys`` (morton.cpp:27-38)
+``sort_particles_by_morton_key``  ``Morton::sortParticlesByMortonKey`` (morton.cpp:40-63)
+``build_tree``                 ``Quadtree`` / ``Octree`` (quadtree.cpp:5-292)
+``calculate_force_from_grid``  ``Physics::calculateForceFromGrid`` (physics.cpp:91-205)
+``integrate_end``              ``Physics::integrateEnd`` (physics.cpp:1114-1125)
+``step``                       the gravity block of ``updateScene`` (globalLogic.cpp:1155-1370)
+=============================  ==============================================
+
+There is no CPU fallback: constructing a Simulation without a B200-class GPU
+or without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgebh.so")
+
+PREC_FAST, PREC_EXACT, PREC_MIXED = 0, 1, 2
+STATUS = {0: "GE_OK", 1: "GE_ERR_ARG", 2: "GE_ERR_NO_DEVICE", 3: "GE_ERR_CUDA",
+          4: "GE_ERR_CAPACITY", 5: "GE_ERR_STATE", 6: "GE_ERR_TIMEOUT", 7: "GE_ERR_OOM",
+          8: "GE_ERR_UNSUPPORTED"}
+EMPTY = 0xFFFFFFFF
+
+
+class GeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """ge_params (include/ge_bh.h)."""
+    _fields_ = [
+        ("dims", C.c_int32), ("precision", C.c_int32), ("G", C.c_float), ("theta", C.c_float),
+        ("eps2", C.c_float), ("dt", C.c_float), ("leaf_cap", C.c_uint32),
+        ("size_gate", C.c_float), ("min_size", C.c_float), ("node_cap_factor", C.c_float),
+        ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Stats(C.Structure):
+    """ge_stats (include/ge_bh.h)."""
+    _fields_ = [
+        ("n", C.c_int64), ("nodes", C.c_int64), ("depth", C.c_int32), ("steps", C.c_int32),
+        ("interactions", C.c_uint64), ("bbox", C.c_float * 4), ("ms_last_step", C.c_float),
+        ("stage_ms", C.c_float * 8),
+    ]
+
+
+_vp = C.c_void_p
+_LIB = None
+
+# Every symbol include/ge_bh.h declares, with its ctypes signature.
+SIGNATURES = {
+    "ge_abi_version": ([], C.c_int),
+    "ge_params_default": ([C.POINTER(Params), C.c_int], None),
+    "ge_create": ([C.POINTER(Params), C.POINTER(_vp)], C.c_int),
+    "ge_destroy": ([_vp], C.c_int),
+    "ge_last_error": ([_vp], C.c_char_p),
+    "ge_set_params": ([_vp, C.POINTER(Params)], C.c_int),
+    "ge_set_stream": ([_vp, _vp], C.c_int),
+    "ge_sync": ([_vp], C.c_int),
+    "ge_get_stats": ([_vp, C.POINTER(Stats)], C.c_int),
+    "ge_upload": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
+    "ge_download": ([_vp] + [_vp] * 11, C.c_int),
+    "ge_upload_pinned": ([_vp, _vp], C.c_int),
+    "ge_download_prev_vel": ([_vp, _vp, _vp, _vp], C.c_int),
+    "ge_step": ([_vp, C.c_int32], C.c_int),
+    "ge_profile_step": ([_vp], C.c_int),
+    "ge_frame_host": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
+    "ge_integrate_start": ([_vp], C.c_int),
+    "ge_bounding_box": ([_vp, _vp], C.c_int),
+    "ge_compute_morton_keys": ([_vp, _vp], C.c_int),
+    "ge_sort_by_morton_key": ([_vp, _vp], C.c_int),
+    "ge_build_tree": ([_vp], C.c_int),
+    "ge_compute_forces": ([_vp], C.c_int),
+    "ge_integrate_end": ([_vp], C.c_int),
+    "ge_set_count_interactions": ([_vp, C.c_int32], C.c_int),
+    "ge_export_tree": ([_vp, C.c_int64, _vp] + [_vp] * 8, C.c_int),
+}
+
+
+def lib():
+    """Load libgebh.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run galaxy-engine_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _LIB = L
+    return _LIB
+
+
+def default_params(dims=2, **kw):
+    """ge_params_default, then keyword overrides (softening= sets eps2 the
+    way the reference walk uses it: squared in 2D, as-is in 3D)."""
+    p = Params()
+    lib().ge_params_default(C.byref(p), dims)
+    soft = kw.pop("softening", None)
+    if soft is not None:
+        p.eps2 = soft * soft if dims == 2 else soft
+    for k, v in kw.items():
+        if k == "domain":
+            for a in range(3):
+                p.domain[a] = v[a]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Simulation:
+    """One resident simulation on the GPU (a ge_ctx)."""
+
+    def __init__(self, params=None, **kw):
+        L = lib()
+        if params is None:
+            params = default_params(**kw)
+        self.params = params
+        h = _vp()
+        rc = L.ge_create(C.byref(params), C.byref(h))
+        if rc != 0:
+            raise GeError(rc, "ge_create failed (a B200-class CUDA device is required)")
+        self._h = h
+        self.dims = params.dims
+        self.n = 0
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().ge_last_error(self._h)
+            raise GeError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ge_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_params(self, params):
+        self._check(lib().ge_set_params(self._h, C.byref(params)))
+        self.params = params
+
+    def set_stream(self, cuda_stream_handle):
+        self._check(lib().ge_set_stream(self._h, _vp(cuda_stream_handle) if cuda_stream_handle else None))
+
+    def stats(self):
+        s = Stats()
+        self._check(lib().ge_get_stats(self._h, C.byref(s)))
+        return s
+
+    def sync(self):
+        self._check(lib().ge_sync(self._h))
+
+    # -- state ------------------------------------------------------------
+    def upload(self, state):
+        """state: dict with x, y, (z,) vx, vy, (vz,) m and optional id, ax, ay, az."""
+        g = state.get
+        arrs = {k: _f32(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "ax", "ay", "az")}
+        ids = None if g("id") is None else np.ascontiguousarray(g("id"), np.uint32)
+        n = len(arrs["x"])
+        self._keep = (arrs, ids)
+        self._check(lib().ge_upload(self._h, n, _ptr(arrs["x"]), _ptr(arrs["y"]), _ptr(arrs["z"]),
+                                    _ptr(arrs["vx"]), _ptr(arrs["vy"]), _ptr(arrs["vz"]),
+                                    _ptr(arrs["m"]), _ptr(ids), _ptr(arrs["ax"]),
+                                    _ptr(arrs["ay"]), _ptr(arrs["az"])))
+        self.n = n
+
+    def upload_pinned(self, pinned):
+        p = None if pinned is None else np.ascontiguousarray(pinned, np.uint8)
+        self._check(lib().ge_upload_pinned(self._h, _ptr(p)))
+
+    def download(self):
+        n, d3 = self.n, self.dims == 3
+        out = {k: np.empty(n, np.float32) for k in ("x", "y", "vx", "vy", "ax", "ay", "m")}
+        if d3:
+            for k in ("z", "vz", "az"):
+                out[k] = np.empty(n, np.float32)
+        out["id"] = np.empty(n, np.uint32)
+        g = out.get
+        self._check(lib().ge_download(self._h, _ptr(g("x")), _ptr(g("y")), _ptr(g("z")),
+                                      _ptr(g("vx")), _ptr(g("vy")), _ptr(g("vz")),
+                                      _ptr(g("ax")), _ptr(g("ay")), _ptr(g("az")),
+                                      _ptr(g("m")), _ptr(g("id"))))
+        return out
+
+    def download_prev_vel(self):
+        n = self.n
+        pv = [np.empty(n, np.float32) for _ in range(self.dims)]
+        self._check(lib().ge_download_prev_vel(self._h, _ptr(pv[0]), _ptr(pv[1]),
+                                               _ptr(pv[2]) if self.dims == 3 else None))
+        return pv
+
+    # -- the step ---------------------------------------------------------
+    def step(self, nsteps=1):
+        self._check(lib().ge_step(self._h, int(nsteps)))
+
+    def profile_step(self):
+        self._check(lib().ge_profile_step(self._h))
+        return list(self.stats().stage_ms)
+
+    def frame_host(self, state):
+        """One frame on host arrays (modified in place; Morton order on return)."""
+        g = state.get
+        for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m"):
+            if g(k) is not None:
+                assert state[k].dtype == np.float32 and state[k].flags.c_contiguous
+        n = len(state["x"])
+        self._check(lib().ge_frame_host(self._h, n, _ptr(g("x")), _ptr(g("y")), _ptr(g("z")),
+                                        _ptr(g("vx")), _ptr(g("vy")), _ptr(g("vz")),
+                                        _ptr(g("ax")), _ptr(g("ay")), _ptr(g("az")),
+                                        _ptr(g("m")), _ptr(g("id"))))
+        self.n = n
+
+    # -- stage calls mirroring the reference surface ------------------------
+    def integrate_start(self):
+        self._check(lib().ge_integrate_start(self._h))
+
+    def bounding_box(self):
+        out = np.zeros(4, np.float32)
+        self._check(lib().ge_bounding_box(self._h, _ptr(out)))
+        return out[: (3 if self.dims == 2 else 4)]
+
+    def compute_morton_keys(self):
+        keys = np.zeros(self.n, np.uint64)
+        self._check(lib().ge_compute_morton_keys(self._h, _ptr(keys)))
+        return keys
+
+    def sort_particles_by_morton_key(self):
+        perm = np.zeros(self.n, np.uint32)
+        self._check(lib().ge_sort_by_morton_key(self._h, _ptr(perm)))
+        return perm
+
+    def build_tree(self):
+        self._check(lib().ge_build_tree(self._h))
+
+    def calculate_force_from_grid(self):
+        self._check(lib().ge_compute_forces(self._h))
+
+    def integrate_end(self):
+        self._check(lib().ge_integrate_end(self._h))
+
+    def count_interactions(self, enable=True):
+        self._check(lib().ge_set_count_interactions(self._h, 1 if enable else 0))
+
+    def export_tree(self):
+        """The tree as the reference's globalNodes: pre-order numpy arrays."""
+        cnt = C.c_int64(0)
+        st = self.stats()
+        cap = int(st.nodes) + 1
+        d, q = self.dims, 1 << self.dims
+        out = dict(pos=np.zeros((cap, d), np.float32), size=np.zeros(cap, np.float32),
+                   com=np.zeros((cap, d), np.float32), mass=np.zeros(cap, np.float32),
+                   start=np.zeros(cap, np.uint32), end=np.zeros(cap, np.uint32),
+                   next=np.zeros(cap, np.uint32), child=np.zeros((cap, q), np.uint32))
+        self._check(lib().ge_export_tree(self._h, cap, C.byref(cnt), _ptr(out["pos"]),
+                                         _ptr(out["size"]), _ptr(out["com"]), _ptr(out["mass"]),
+                                         _ptr(out["start"]), _ptr(out["end"]), _ptr(out["next"]),
+                                         _ptr(out["child"])))
+        k = cnt.value
+        return {a: v[:k] for a, v in out.items()}

@@ -1,0 +1,93 @@
+// ge_internal.h -- device buffer layout and kernel launchers shared by the
+// C-ABI host code (ge_api.cu) and the kernel files.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ge {
+
+// Particle state, structure-of-arrays, in Morton order.  z/vz/az are unused
+// in 2D.  pvx..pvz (prevVel) and pinned are optional (nullptr).
+struct State {
+    float *x, *y, *z;
+    float *vx, *vy, *vz;
+    float *ax, *ay, *az;
+    float *m;
+    uint32_t *id;
+    float *pvx, *pvy, *pvz;
+    uint8_t *pinned;
+};
+
+// Tree nodes, structure-of-arrays.
+//   walk    float4  2D: {com.x, com.y, mass, size^2}   3D: {com.x, com.y, com.z, mass}
+//   size2   float   3D only: size^2
+//   info    uint4   {first_child, child_mask, start, end}; child_mask bit q set when
+//                   child slot q is occupied; children are stored contiguously from
+//                   first_child in increasing q; child_mask == 0 marks a leaf
+//   cell    float4  {corner.x, corner.y, corner.z, size} (build only)
+//   level   uint32  first node of each level (nodes are stored level by level)
+struct Tree {
+    float4 *walk;
+    float *size2;
+    uint4 *info;
+    float4 *cell;
+    uint32_t *level;      // [kMaxLevels + 2]
+    uint32_t *lvl_alloc;  // [kMaxLevels + 2] per-level child allocation counters
+    uint32_t *meta;       // [4] {node_count, levels, bar_count, bar_gen}
+    int64_t cap;
+};
+
+// Scratch for bounding box, keys and sort.
+struct SortScratch {
+    uint64_t *keys[2];     // 2D: (key << 28 | index) packed; 3D: keys
+    uint32_t *vals[2];     // 3D: indices
+    uint32_t *hist;        // [8][256] per-pass digit counts
+    uint32_t *status;      // [8][tiles][256] decoupled look-back words
+    uint32_t *tile_ctr;    // [8]
+    int64_t tiles;
+    float4 *bbox_part;     // per-block min/max partials (2 float4 per block)
+    uint32_t *bbox_ctr;    // [1]
+    float4 *bbox;          // [1] {x, y, z, size}
+    int bbox_blocks;
+};
+
+struct StepParams {
+    int n;
+    float dt, half_dt;
+    float G, theta2, eps2;
+    uint32_t leaf_cap;
+    float size_gate, min_size;
+    int periodic;
+    float domain[3], half_domain[3];
+};
+
+constexpr int kBBoxThreads = 256;
+constexpr int kSortTile = 4096;   // keys per look-back tile (256 threads x 16)
+
+// --- launchers (each runs on `st`) ----------------------------------------
+// integrateStart (kick + drift) fused with the bounding-box reduction; the
+// last block finalises the root box and seeds the root node.
+cudaError_t launch_kick_drift_bbox(int dims, const State &s, const StepParams &p, bool kick_drift,
+                                   SortScratch &ss, Tree &t, uint32_t *err, cudaStream_t st);
+// Morton keys from the root box plus the digit histograms of every pass
+cudaError_t launch_keys(int dims, const State &s, int n, SortScratch &ss, cudaStream_t st);
+// all radix passes; leaves the sorted keys in ss.keys[0] (and vals[0])
+cudaError_t launch_sort(int dims, int n, SortScratch &ss, uint32_t *err, cudaStream_t st);
+// gather of the state into `out` by the sorted order
+cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
+                           const State &out, bool with_acc, cudaStream_t st);
+// order (sorted slot -> previous index) copy-out for the stage API
+cudaError_t launch_perm_out(int dims, int n, const SortScratch &ss, uint32_t *perm,
+                            cudaStream_t st);
+cudaError_t launch_keys_out(int dims, int n, const SortScratch &ss, uint64_t *keys,
+                            cudaStream_t st);
+// tree build + mass/centre of mass (one cooperative launch)
+cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
+                         int num_sms, cudaStream_t st);
+// tree walk; integrate_end fuses integrateEnd (v += a*dt/2)
+cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
+                        const Tree &t, bool integrate_end, unsigned long long *inter_count,
+                        uint32_t *err, cudaStream_t st);
+cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+
+}  // namespace ge

@@ -1,0 +1,298 @@
+// ge_sort.cu -- Morton keys, stable LSD radix sort, state permutation.
+//
+// Reference: Morton::computeMortonKeys[3D] (GalaxyEngine/src/Physics/morton.cpp:27-38,
+// :92-112) and Morton::sortParticlesByMortonKey[3D] (:40-63, :114-138).
+//
+// Keys are bit-exact with the reference: the same IEEE single operations
+// (clamp, subtract, divide, scale, truncate) and the same interleave.  The
+// reference sorts with std::sort, whose order among equal keys is
+// unspecified; this sort is stable, so equal keys keep their current order.
+//
+// 2D keys use 36 bits.  They are packed with the particle's current index as
+// (key << 28) | index, so each pass moves one 8-byte word per particle
+// (N < 2^28).  3D keys use 63 bits and travel with a separate 32-bit index.
+//
+// Each pass is one kernel: a tile of 4096 keys is ranked in shared memory
+// (warp-private digit counters, __match_any_sync for the ranks of equal
+// digits), the tile's per-digit counts are published, and the exclusive
+// prefix over earlier tiles is found by decoupled look-back on per-tile
+// status words (bounded waits).  Digit histograms of every pass are computed
+// once, by the key kernel.
+#include "ge_device.cuh"
+#include "ge_internal.h"
+
+namespace ge {
+
+constexpr int kRadix = 256;
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kItems = kSortTile / kSortThreads;  // 16
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1;
+
+__host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 5 : 8; }
+__host__ __device__ constexpr int key_shift0(int dims) { return dims == 2 ? 28 : 0; }
+
+template <int D>
+__global__ void __launch_bounds__(256)
+k_keys(State s, int n, const float4 *bbox, uint64_t *keys, uint32_t *vals, uint32_t *hist,
+       uint32_t *status, int64_t status_words, uint32_t *tile_ctr) {
+    constexpr int P = key_passes(D), S0 = key_shift0(D);
+    __shared__ uint32_t sh[P][kRadix];
+    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+    // clear the look-back status words for this step's passes
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < status_words;
+         i += (int64_t)gridDim.x * blockDim.x)
+        status[i] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x < 8) tile_ctr[threadIdx.x] = 0u;
+    __syncthreads();
+    const float4 bb = *bbox;
+    float hx, hy, hz;
+    if (D == 2) {
+        float ext = bb.w > 1e-6f ? bb.w : 1e-6f;   // std::max(posSize.z, 1e-6f)
+        hx = fadd(bb.x, ext); hy = fadd(bb.y, ext); hz = 0.0f;
+    } else {
+        hx = fadd(bb.x, bb.w); hy = fadd(bb.y, bb.w); hz = fadd(bb.z, bb.w);
+    }
+    const int stride = gridDim.x * blockDim.x;
+    // iterate whole warps so that __match_any_sync sees full warps
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        int i = base + threadIdx.x;
+        bool ok = i < n;
+        uint64_t word = 0;
+        if (ok) {
+            if (D == 2) {
+                uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 262144.0f, 262143ull);
+                uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 262144.0f, 262143ull);
+                uint64_t key = spread2(ix) | (spread2(iy) << 1);
+                word = (key << 28) | (uint64_t)i;
+                keys[i] = word;
+            } else {
+                uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 2097151.0f, 2097151ull);
+                uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 2097151.0f, 2097151ull);
+                uint64_t iz = scale_to_grid(s.z[i], bb.z, hz, 2097151.0f, 2097151ull);
+                word = spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2);
+                keys[i] = word;
+                vals[i] = (uint32_t)i;
+            }
+        }
+#pragma unroll
+        for (int ps = 0; ps < P; ps++) {
+            uint32_t d = ok ? (uint32_t)((word >> (S0 + 8 * ps)) & 0xFFu) : 0x100u;
+            unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (ok && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1))
+                atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) {
+        uint32_t c = (&sh[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// One stable counting pass over digit (word >> shift) & 255.
+template <bool PAIRS>
+__global__ void __launch_bounds__(kSortThreads)
+k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
+             const uint32_t *__restrict__ vin, uint32_t *__restrict__ vout, int n, int shift,
+             const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
+             uint32_t *err) {
+    __shared__ uint32_t s_whist[kSortWarps][kRadix];
+    __shared__ uint32_t s_off[kRadix];
+    __shared__ uint32_t s_scan[kSortWarps];
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&s_whist[0][0])[i] = 0u;
+    // exclusive scan of this pass's global digit counts (thread = digit)
+    uint32_t g = hist[tid];
+    uint32_t incl = g;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_scan[w] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int ww = 0; ww < w; ww++) wbase += s_scan[ww];
+    const uint32_t gexcl = wbase + incl - g;
+    const int tile = (int)s_tile;
+    const int base = tile * kSortTile + w * 32 * kItems;
+
+    uint64_t k[kItems];
+    uint32_t v[kItems], rk[kItems], dg[kItems];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+        int idx = base + it * 32 + lane;
+        bool ok = idx < n;
+        k[it] = ok ? kin[idx] : 0ull;
+        if (PAIRS) v[it] = ok ? vin[idx] : 0u;
+        dg[it] = ok ? (uint32_t)((k[it] >> shift) & 0xFFu) : 0x100u;
+    }
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+        uint32_t d = dg[it];
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        uint32_t prev = 0;
+        int leader = __ffs(peers) - 1;
+        if (d < 0x100u && lane == leader) {
+            prev = s_whist[w][d];
+            s_whist[w][d] = prev + (uint32_t)__popc(peers);
+        }
+        prev = __shfl_sync(0xffffffffu, prev, leader);
+        rk[it] = prev + (uint32_t)__popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps and the tile total
+    {
+        const int d = tid;
+        uint32_t sum = 0;
+#pragma unroll
+        for (int ww = 0; ww < kSortWarps; ww++) {
+            uint32_t c = s_whist[ww][d];
+            s_whist[ww][d] = sum;
+            sum += c;
+        }
+        volatile uint32_t *st = status;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            st[d] = kFlagInc | sum;
+        } else {
+            st[(int64_t)tile * kRadix + d] = kFlagAgg | sum;
+            int t = tile - 1;
+            uint32_t spins = 0;
+            while (t >= 0) {
+                uint32_t word = st[(int64_t)t * kRadix + d];
+                if ((word & ~kValMask) == 0u) {
+                    if (++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
+                    continue;
+                }
+                excl += word & kValMask;
+                if ((word & ~kValMask) == kFlagInc) break;
+                --t;
+            }
+            st[(int64_t)tile * kRadix + d] = kFlagInc | ((excl + sum) & kValMask);
+        }
+        s_off[d] = gexcl + excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+        uint32_t d = dg[it];
+        if (d < 0x100u) {
+            uint32_t pos = s_off[d] + s_whist[w][d] + rk[it];
+            if (pos < (uint32_t)n) {   // always true unless a look-back wait gave up
+                kout[pos] = k[it];
+                if (PAIRS) vout[pos] = v[it];
+            }
+        }
+    }
+}
+
+template <int D>
+__global__ void k_permute(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                          int n, State in, State out, int with_acc) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t j = (D == 2) ? (uint32_t)(keys[k] & 0x0FFFFFFFull) : vals[k];
+        if (j >= (uint32_t)n) j = (uint32_t)k;   // only after a failed sort (error word set)
+        out.x[k] = in.x[j]; out.y[k] = in.y[j];
+        out.vx[k] = in.vx[j]; out.vy[k] = in.vy[j];
+        out.m[k] = in.m[j];
+        out.id[k] = in.id[j];
+        if (D == 3) { out.z[k] = in.z[j]; out.vz[k] = in.vz[j]; }
+        if (with_acc) {
+            out.ax[k] = in.ax[j]; out.ay[k] = in.ay[j];
+            if (D == 3) out.az[k] = in.az[j];
+        }
+        if (in.pvx) {
+            out.pvx[k] = in.pvx[j]; out.pvy[k] = in.pvy[j];
+            if (D == 3) out.pvz[k] = in.pvz[j];
+        }
+        if (in.pinned) out.pinned[k] = in.pinned[j];
+    }
+}
+
+template <int D>
+__global__ void k_perm_out(const uint64_t *keys, const uint32_t *vals, int n, uint32_t *perm,
+                           uint64_t *kout) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        if (perm) perm[k] = (D == 2) ? (uint32_t)(keys[k] & 0x0FFFFFFFull) : vals[k];
+        if (kout) kout[k] = (D == 2) ? (keys[k] >> 28) : keys[k];
+    }
+}
+
+static int grid_for(int n, int threads, int cap) {
+    int b = (n + threads - 1) / threads;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : b;
+}
+
+cudaError_t launch_keys(int dims, const State &s, int n, SortScratch &ss, cudaStream_t st) {
+    int blocks = grid_for(n, 256, 148 * 8);
+    int64_t words = (int64_t)key_passes(dims) * ss.tiles * kRadix;
+    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * 8 * kRadix, st);
+    if (e != cudaSuccess) return e;
+    if (dims == 2)
+        k_keys<2><<<blocks, 256, 0, st>>>(s, n, ss.bbox, ss.keys[0], ss.vals[0], ss.hist,
+                                          ss.status, words, ss.tile_ctr);
+    else
+        k_keys<3><<<blocks, 256, 0, st>>>(s, n, ss.bbox, ss.keys[0], ss.vals[0], ss.hist,
+                                          ss.status, words, ss.tile_ctr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort(int dims, int n, SortScratch &ss, uint32_t *err, cudaStream_t st) {
+    const int P = key_passes(dims), S0 = key_shift0(dims);
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    int cur = 0;
+    for (int ps = 0; ps < P; ps++) {
+        uint32_t *status = ss.status + (int64_t)ps * ss.tiles * kRadix;
+        if (dims == 2)
+            k_radix_pass<false><<<tiles, kSortThreads, 0, st>>>(
+                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, S0 + 8 * ps,
+                ss.hist + ps * kRadix, status, ss.tile_ctr + ps, err);
+        else
+            k_radix_pass<true><<<tiles, kSortThreads, 0, st>>>(
+                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, S0 + 8 * ps,
+                ss.hist + ps * kRadix, status, ss.tile_ctr + ps, err);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        cur ^= 1;
+    }
+    // an odd number of passes leaves the result in buffer 1: swap the roles
+    if (cur == 1) {
+        uint64_t *tk = ss.keys[0]; ss.keys[0] = ss.keys[1]; ss.keys[1] = tk;
+        uint32_t *tv = ss.vals[0]; ss.vals[0] = ss.vals[1]; ss.vals[1] = tv;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
+                           const State &out, bool with_acc, cudaStream_t st) {
+    int blocks = grid_for(n, 256, 148 * 16);
+    if (dims == 2)
+        k_permute<2><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, in, out, with_acc);
+    else
+        k_permute<3><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, in, out, with_acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_perm_out(int dims, int n, const SortScratch &ss, uint32_t *perm,
+                            cudaStream_t st) {
+    int blocks = grid_for(n, 256, 148 * 16);
+    if (dims == 2) k_perm_out<2><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, perm, nullptr);
+    else k_perm_out<3><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, perm, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_keys_out(int dims, int n, const SortScratch &ss, uint64_t *keys,
+                            cudaStream_t st) {
+    int blocks = grid_for(n, 256, 148 * 16);
+    if (dims == 2) k_perm_out<2><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, nullptr, keys);
+    else k_perm_out<3><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, nullptr, keys);
+    return cudaGetLastError();
+}
+
+}  // namespace ge

@@ -1,0 +1,171 @@
+/*
+ * ge_bh.h -- C ABI of the B200 Barnes-Hut gravity step (libgebh.so).
+ *
+ * Drop-in for Galaxy Engine's per-frame gravity path (paths relative to the
+ * NarcisCalin/Galaxy-Engine checkout):
+ *
+ *   integrateStart -> boundingBox -> computeMortonKeys -> sortParticlesByMortonKey
+ *   -> Quadtree/Octree build -> calculateForceFromGrid -> integrateEnd
+ *   (GalaxyEngine/src/globalLogic.cpp:1155-1370 in 2D, :1584-1719 in 3D)
+ *
+ * Conventions
+ *   - Every call returns a ge_status; 0 is success.  ge_last_error() returns a
+ *     message for the last failure on that context.
+ *   - Host buffers are caller-owned and only read/written during the call.
+ *     Device state is owned by the context and stays resident between calls.
+ *   - Particles are kept in Morton order: every step re-sorts them, exactly as
+ *     the reference re-sorts its particle vectors every frame.  The uint32
+ *     `id` array travels with the particles so results can be matched by id.
+ *   - One host thread per context; different contexts are independent.  All
+ *     device work of a context runs on its stream (ge_set_stream).
+ *   - No entry point falls back to the CPU: without a usable CUDA device,
+ *     ge_create fails with GE_ERR_NO_DEVICE.
+ */
+#ifndef GE_BH_H
+#define GE_BH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GE_ABI_VERSION 1
+
+typedef enum {
+    GE_OK = 0,
+    GE_ERR_ARG = 1,        /* invalid argument */
+    GE_ERR_NO_DEVICE = 2,  /* no CUDA device / wrong architecture */
+    GE_ERR_CUDA = 3,       /* CUDA runtime error (see ge_last_error) */
+    GE_ERR_CAPACITY = 4,   /* node or stack capacity exceeded; raise node_cap_factor */
+    GE_ERR_STATE = 5,      /* call made in the wrong state (e.g. no particles) */
+    GE_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up */
+    GE_ERR_OOM = 7,        /* device allocation failed or HBM budget exceeded */
+    GE_ERR_UNSUPPORTED = 8 /* option not supported by this build */
+} ge_status;
+
+typedef enum {
+    GE_PREC_FAST = 0,   /* FP32; MAC and tree arithmetic exactly as the reference,
+                           force terms with rsqrt and FMA */
+    GE_PREC_EXACT = 1,  /* FP32 with the reference's own rounding for every
+                           operation (1/sqrtf, no contraction); for parity checks */
+    GE_PREC_MIXED = 2   /* FP32 interactions on cell-relative positions, Kahan-
+                           compensated accumulation and leapfrog update */
+} ge_precision;
+
+/*
+ * Parameters.  Replaces the reference's UpdateVariables fields used on the
+ * gravity path (GalaxyEngine/include/parameters.h:97-129,138,147,318).
+ */
+typedef struct {
+    int32_t dims;            /* 2 (quadtree) or 3 (octree) */
+    int32_t precision;       /* ge_precision */
+    float G;                 /* myVar.G */
+    float theta;             /* myVar.theta */
+    float eps2;              /* value added to r^2: softening^2 in the 2D walk
+                                (physics.cpp:100), softening in 3D (physics3D.cpp:166) */
+    float dt;                /* myVar.timeFactor */
+    uint32_t leaf_cap;       /* max particles in a leaf below the size gate (reference: 4) */
+    float size_gate;         /* reference: 2.0f (quadtree.cpp:16) */
+    float min_size;          /* reference: 1e-6f */
+    float node_cap_factor;   /* node capacity = factor * N + 1024 (reference reserves 4N / 8N) */
+    int32_t periodic;        /* periodic wrap (isPeriodicBoundaryEnabled && !infiniteDomain) */
+    float domain[3];         /* domainSize / domainSize3D */
+    int32_t track_prev_vel;  /* keep prevVel as the reference does (integrateStart) */
+    int32_t reserved[7];
+} ge_params;
+
+typedef struct {
+    int64_t n;               /* particles */
+    int64_t nodes;           /* nodes in the last tree */
+    int32_t depth;           /* levels in the last tree */
+    int32_t steps;           /* steps run on this context */
+    uint64_t interactions;   /* accepted monopoles + leaf pairs (j != i) in the last
+                                force pass, when counting is enabled */
+    float bbox[4];           /* last root box: x, y, (z,) size */
+    float ms_last_step;      /* device time of the last ge_step call / nsteps */
+    float stage_ms[8];       /* last ge_profile_step: kick+bbox, keys, sort, permute,
+                                build, walk, total, unused */
+} ge_stats;
+
+typedef struct ge_ctx ge_ctx;
+
+/* --- lifecycle -------------------------------------------------------- */
+/* Fills the reference defaults: theta 0.8, softening 1.5 (eps2 = 2.25 in 2D,
+   1.5 in 3D), dt 0.045, G 6.674e-11, leaf_cap 4, size_gate 2, min_size 1e-6. */
+void ge_params_default(ge_params *p, int dims);
+int ge_create(const ge_params *p, ge_ctx **out);
+int ge_destroy(ge_ctx *ctx);
+const char *ge_last_error(const ge_ctx *ctx);
+int ge_set_params(ge_ctx *ctx, const ge_params *p);
+/* Run the context's work on an existing cudaStream_t (NULL: the context's own). */
+int ge_set_stream(ge_ctx *ctx, void *cuda_stream);
+int ge_sync(ge_ctx *ctx);
+int ge_get_stats(ge_ctx *ctx, ge_stats *out);
+int ge_abi_version(void);
+
+/* --- state I/O (host SoA buffers; z/vz/az ignored in 2D; NULL = skip) -- */
+/* replaces Physics::flattenParticles (physics.cpp:354-390): the state goes to
+   the device once and stays resident.  Accelerations start at 0 as in the
+   reference's fresh particles (particle.h:49); ax/ay/az may seed them. */
+int ge_upload(ge_ctx *ctx, int64_t n, const float *x, const float *y, const float *z,
+              const float *vx, const float *vy, const float *vz, const float *m,
+              const uint32_t *id, const float *ax, const float *ay, const float *az);
+/* replaces Physics::readFlattenBack (physics.cpp:542-565) */
+int ge_download(ge_ctx *ctx, float *x, float *y, float *z, float *vx, float *vy, float *vz,
+                float *ax, float *ay, float *az, float *m, uint32_t *id);
+/* optional per-particle pin flags (ParticleRendering::isPinned, particle.h:100),
+   in the current particle order; NULL clears them */
+int ge_upload_pinned(ge_ctx *ctx, const uint8_t *pinned);
+int ge_download_prev_vel(ge_ctx *ctx, float *pvx, float *pvy, float *pvz);
+
+/* --- the fused step ---------------------------------------------------- */
+/* nsteps full frames on the resident state (globalLogic.cpp:1155-1370 /
+   :1584-1719 with dt != 0), all on the device. */
+int ge_step(ge_ctx *ctx, int32_t nsteps);
+/* one frame with per-stage CUDA-event timing into ge_stats.stage_ms */
+int ge_profile_step(ge_ctx *ctx);
+/* One frame on HOST buffers: upload, step, download, all inside the call.
+   This is the reference-facing drop-in for the gravity block of
+   updateScene(): arrays are updated in place and come back in Morton order
+   (id says which particle is where), like the reference's pParticles. */
+int ge_frame_host(ge_ctx *ctx, int64_t n, float *x, float *y, float *z, float *vx, float *vy,
+                  float *vz, float *ax, float *ay, float *az, float *m, uint32_t *id);
+
+/* --- stage calls mirroring the reference surface (for parity tests) ---- */
+/* Physics::integrateStart (physics.cpp:1069-1112) */
+int ge_integrate_start(ge_ctx *ctx);
+/* boundingBox / boundingBox3D (globalLogic.cpp:1083-1099 / :1460-1477); out:
+   {x, y, size} in 2D, {x, y, z, size} in 3D */
+int ge_bounding_box(ge_ctx *ctx, float *out);
+/* Morton::computeMortonKeys[3D] (morton.cpp:27-38 / :92-112) for the current
+   order and root box; keys_out (optional) receives them */
+int ge_compute_morton_keys(ge_ctx *ctx, uint64_t *keys_out);
+/* Morton::sortParticlesByMortonKey[3D] (morton.cpp:40-63 / :114-138): stable
+   radix sort of the keys and the gather of the whole state; perm_out
+   (optional) receives the index each slot came from */
+int ge_sort_by_morton_key(ge_ctx *ctx, uint32_t *perm_out);
+/* Quadtree / Octree construction with mass and centre of mass
+   (quadtree.cpp:5-292) over the current (sorted) order */
+int ge_build_tree(ge_ctx *ctx);
+/* Physics::calculateForceFromGrid[3D] (physics.cpp:91-205 / physics3D.cpp:131-253):
+   accelerations of every particle from the current tree */
+int ge_compute_forces(ge_ctx *ctx);
+/* Physics::integrateEnd (physics.cpp:1114-1125) */
+int ge_integrate_end(ge_ctx *ctx);
+/* enable per-particle interaction counting in ge_compute_forces (stats) */
+int ge_set_count_interactions(ge_ctx *ctx, int32_t enable);
+
+/* --- tree export: the reference's globalNodes in DFS pre-order --------- */
+/* Returns the node count in *count.  Arrays (capacity cap nodes; any may be
+   NULL): pos/com [cap*dims], size, mass [cap], start, end, next [cap],
+   child [cap * 2^dims] with child[q], q = xbit | ybit<<1 (| zbit<<2), the
+   reference's subGrids[x][y]([z]); 0xFFFFFFFF marks an empty slot. */
+int ge_export_tree(ge_ctx *ctx, int64_t cap, int64_t *count, float *pos, float *size,
+                   float *com, float *mass, uint32_t *start, uint32_t *end, uint32_t *next,
+                   uint32_t *child);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,70 @@
+"""CPU: the C-ABI library loads, exports every symbol include/ge_bh.h declares,
+and refuses to run without a GPU (there is no CPU fallback)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, gpu_available
+
+HEADER = os.path.join(ROOT, "include", "ge_bh.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ge_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_reference_surface():
+    names = declared_functions()
+    for need in ("ge_create", "ge_destroy", "ge_step", "ge_upload", "ge_download",
+                 "ge_bounding_box", "ge_compute_morton_keys", "ge_sort_by_morton_key",
+                 "ge_build_tree", "ge_compute_forces", "ge_integrate_start",
+                 "ge_integrate_end", "ge_export_tree", "ge_frame_host"):
+        assert need in names
+
+
+def test_library_exports_every_declared_symbol(ge):
+    L = ge.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding knows every one of them
+    assert sorted(ge.SIGNATURES) == declared_functions()
+
+
+def test_abi_version_and_defaults(ge):
+    assert ge.lib().ge_abi_version() == 1
+    p = ge.default_params(2)
+    assert p.dims == 2 and abs(p.theta - 0.8) < 1e-7 and abs(p.eps2 - 2.25) < 1e-6
+    assert p.leaf_cap == 4 and p.size_gate == 2.0 and abs(p.dt - 0.045) < 1e-7
+    p3 = ge.default_params(3)
+    assert abs(p3.eps2 - 1.5) < 1e-6 and p3.node_cap_factor == 8.0
+    p = ge.default_params(2, softening=0.01, theta=0.7)
+    assert abs(p.eps2 - 1e-4) < 1e-10 and abs(p.theta - 0.7) < 1e-7
+
+
+def test_struct_layouts_match_header(ge):
+    # ge_params: 10 scalars + domain[3] + track_prev_vel + reserved[7] (4 bytes each)
+    assert C.sizeof(ge.Params) == 4 * (11 + 3 + 1 + 7)
+    # ge_stats: 84 bytes of fields, padded to the 8-byte alignment of its int64 members
+    assert C.sizeof(ge.Stats) == 88
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU refusal")
+def test_no_cpu_fallback_without_gpu(ge):
+    with pytest.raises(ge.GeError) as ei:
+        ge.Simulation(ge.default_params(2))
+    assert ei.value.code == 2    # GE_ERR_NO_DEVICE
+
+
+def test_invalid_params_rejected(ge):
+    L = ge.lib()
+    p = ge.default_params(2)
+    p.dims = 4
+    h = C.c_void_p()
+    assert L.ge_create(C.byref(p), C.byref(h)) == 1
+    p = ge.default_params(2)
+    p.leaf_cap = 0
+    assert L.ge_create(C.byref(p), C.byref(h)) == 1
