@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the Barnes-Hut gravity step on B200.
+
+Workload (one GPU): the 2D two-disk system, N = 1,048,576 (two exponential
+disks of 524,288 particles, centres 10 apart, relative speed 0.5), G = 1,
+theta 0.7, softening 0.005 (eps2 = 2.5e-5), dt 1e-3, leaf capacity 4 (the
+reference's), FP32.  A step is one full frame of the gravity path:
+kick + drift, bounding box, Morton keys, radix sort, gather, tree build,
+tree walk + second half kick.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU, each stepping its own replica of the workload
+(a single simulation does not shard: every particle's walk reads the whole
+tree); value = all particles stepped on all ranks / max time over ranks.
+
+The JSON line carries value (device time, inputs resident, L2 flushed
+between steps), e2e (host buffers through ge_frame_host, copies inside the
+timed region), the walk kernel's roofline, the tree-build roofline, FP64
+direct-sum accuracy on 16,384 sampled particles, the CPU baseline and clocks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib
+import json
+import math
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s and p50/p99 step latency, batched vs plain, at <=1e-3 force err"
+UNIT = "particle-steps/s"
+N_DEFAULT = 1 << 20
+THETA, SOFT, DT, LEAF = 0.7, 0.005, 1e-3, 4
+FLOPEQ_PER_INTERACTION = {2: 18.0, 3: 24.0}   # 2 x FP32 instruction slots (9 / 12)
+SM_COUNT, LANES = 148, 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--theta", type=float, default=THETA)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-frames", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d.get("sm_max_mhz", 1965.0)), "measured"
+    return 6650.0, 1965.0, "fallback"
+
+
+class ClockSampler:
+    """SM clock and throttle reasons sampled through NVML while running."""
+
+    def __init__(self, dev_index, period=0.01):
+        self.samples, self.period, self.dev = [], period, dev_index
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        nv = self.nv
+        names = {
+            "gpu_idle": getattr(nv, "nvmlClocksEventReasonGpuIdle", 0x1),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        seen = set()
+        for _, rs in self.samples:
+            for k, bit in names.items():
+                if rs & bit and k != "gpu_idle":
+                    seen.add(k)
+        mhz = sorted(m for m, _ in self.samples)
+        return {"sm_mhz": float(mhz[len(mhz) // 2]), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(seen), "samples": len(mhz)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(ics, n):
+    return ics.two_disks2d(n, seed=0)
+
+
+def cpu_baseline(O, st, frames, params_kw):
+    """The oracle's frame with the application's dispatch (AVX2 walk above 5000
+    particles) on all host cores, timed over `frames` frames of the workload."""
+    prm = O.make_params(dims=2, theta=params_kw["theta"], eps2=params_kw["eps2"],
+                        leaf_cap=params_kw["leaf_cap"], dt=params_kw["dt"])
+    fr = {k: np.array(v, copy=True) for k, v in st.items()}
+    fr["ax"] = np.zeros(len(fr["x"]), np.float32)
+    fr["ay"] = np.zeros(len(fr["x"]), np.float32)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    O.frame(prm, fr, walk_kind=2, nthreads=cores)          # untimed warm-up frame
+    t0 = time.perf_counter()
+    stage = np.zeros(8)
+    for _ in range(frames):
+        s, _, _ = O.frame(prm, fr, walk_kind=2, nthreads=cores)
+        stage += s
+    dt = (time.perf_counter() - t0) / frames
+    return dt, cores, stage / frames
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ics = importlib.import_module("galaxy-engine_b200.ics")
+    st = workload(ics, args.n)
+    kw = dict(theta=args.theta, eps2=SOFT * SOFT, leaf_cap=LEAF, dt=DT)
+    prm = O.make_params(dims=2, **kw)
+    fr = {k: np.array(v, copy=True) for k, v in st.items()}
+    fr["ax"] = np.zeros(len(fr["x"]), np.float32)
+    fr["ay"] = np.zeros(len(fr["x"]), np.float32)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    for _ in range(max(1, min(args.warmup, 2))):
+        O.frame(prm, fr, walk_kind=2, nthreads=cores)
+    times = []
+    budget = 150.0
+    t_all = time.perf_counter()
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        O.frame(prm, fr, walk_kind=2, nthreads=cores)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget:
+            break
+    t = float(np.mean(times))
+    value = args.n / t
+    sample = (f"{len(times)} full frames of the {args.n}-particle two-disk workload "
+              f"(oracle frame: reference tree build restated, AVX2 walk as the application "
+              f"dispatches it), {cores} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic",
+        "config": {"workload": "two-disk 2D Barnes-Hut", "n": args.n, "theta": args.theta,
+                   "softening": SOFT, "dt": DT, "leaf_cap": LEAF, "G": 1.0},
+        "p50_ms": float(np.percentile(times, 50)) * 1e3,
+        "p99_ms": float(np.percentile(times, 99)) * 1e3,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ge = importlib.import_module("galaxy-engine_b200")
+    ics = importlib.import_module("galaxy-engine_b200.ics")
+    n = args.n
+    st = workload(ics, n)
+    p = ge.default_params(2, G=1.0, theta=args.theta, softening=SOFT, dt=DT, leaf_cap=LEAF,
+                          precision=ge.PREC_FAST)
+    stream = torch.cuda.Stream()
+    sim = ge.Simulation(p)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(st)
+    sim.step(args.warmup)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    K = args.steps
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        for k in range(K):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0[k].record(stream)
+            sim.step(1)
+            e1[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    times = np.array([e0[k].elapsed_time(e1[k]) for k in range(K)])
+    total_ms = float(times.sum())
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * K / (total_ms * 1e-3)
+
+    # per-stage profile, interaction count, accuracy (untimed)
+    stage = np.zeros(8)
+    for _ in range(3):
+        stage += np.array(sim.profile_step())
+    stage /= 3
+    sim.count_interactions(True)
+    sim.step(1)
+    inter = sim.stats().interactions
+    sim.count_interactions(False)
+    stats = sim.stats()
+    out = sim.download()
+    rng = np.random.Generator(np.random.PCG64(1))
+    idx = np.sort(rng.choice(n, size=min(16384, n), replace=False)).astype(np.uint32)
+    fx, fy = sim.direct_sum_f64(idx)
+    err = np.hypot(out["ax"][idx] - fx, out["ay"][idx] - fy) / np.hypot(fx, fy)
+
+    # e2e through the C ABI with pinned host buffers, copies inside the timed region
+    ke = max(1, min(args.e2e_steps, K))
+    host = {}
+    for k in ("x", "y", "vx", "vy", "ax", "ay", "m"):
+        host[k] = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+        host[k][:] = out[k]
+    host["id"] = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    host["id"][:] = out["id"]
+    sim.frame_host(host)   # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        sim.frame_host(host)
+    e2e_s = (time.perf_counter() - t0) / ke
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    bytes_h2d = n * 4 * 8
+    bytes_d2h = n * 4 * 8
+
+    hbm_gbs, sm_max_mhz, peak_src = measured_peaks()
+    clocks = clk.summary()
+    walk_ms = float(stage[5])
+    build_ms = float(stage[1] + stage[2] + stage[3] + stage[4])
+    fp32_peak = SM_COUNT * LANES * 2 * sm_max_mhz * 1e6 / 1e12
+    walk_tflops = inter * FLOPEQ_PER_INTERACTION[2] / (walk_ms * 1e-3) / 1e12
+    build_bytes = 216.0 * n + 40.0 * stats.nodes
+    build_gbs = build_bytes / (build_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "walk_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "two-disk 2D Barnes-Hut (plain, one simulation per GPU)",
+                   "n": n, "theta": args.theta, "softening": SOFT, "dt": DT,
+                   "leaf_cap": LEAF, "G": 1.0, "precision": "fast",
+                   "l2": "flushed (256 MB write) before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+        "interactions_per_s": inter / (total_ms * 1e-3 / K) if K else None,
+        "interactions_per_step": int(inter), "nodes": int(stats.nodes), "depth": int(stats.depth),
+        "force_err_vs_fp64": {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)),
+                              "max": float(err.max()), "sample": int(len(idx))},
+        "stage_ms": {"kick_drift_bbox": stage[0], "keys": stage[1], "sort": stage[2],
+                     "permute": stage[3], "build": stage[4], "walk": stage[5]},
+        "clocks": clocks,
+        "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bytes_h2d,
+                "d2h_bytes_per_step": bytes_d2h, "steps": ke,
+                "api": "ge_frame_host (pinned host SoA buffers)"},
+        "gpu_launches": 10 * K,
+        "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": walk_tflops / fp32_peak,
+                     "traffic": traffic,
+                     "peak_source": "nominal FP32 SIMT: 148 SM x 128 lanes x 2 x sm_max_mhz",
+                     "algorithmic": "18 flop-equivalents (9 FP32 issue slots) per credited interaction"},
+        "build_roofline": {"bound": "hbm", "achieved": build_gbs, "peak": hbm_gbs, "unit": "GB/s",
+                           "frac": build_gbs / hbm_gbs, "peak_source": peak_src,
+                           "algorithmic": "216 B/particle + 40 B/node (keys, 5 sort passes, gather, nodes)"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        t_cpu, cores, cstage = cpu_baseline(
+            O, st, args.cpu_frames, dict(theta=args.theta, eps2=SOFT * SOFT, leaf_cap=LEAF, dt=DT))
+        line["cpu_baseline"] = {
+            "value": n / t_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{args.cpu_frames} full frames of the same {n}-particle workload "
+                      f"(oracle frame, AVX2 walk as the application dispatches it)",
+            "ms_per_frame": t_cpu * 1e3,
+            "stage_ms": {"integrate_start": cstage[0], "bbox": cstage[1], "keys": cstage[2],
+                         "sort_gather": cstage[3], "build": cstage[4], "walk": cstage[5],
+                         "integrate_end": cstage[6]}}
+    sim.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -95,6 +95,8 @@ SIGNATURES = {
     "ge_integrate_end": ([_vp], C.c_int),
     "ge_set_count_interactions": ([_vp, C.c_int32], C.c_int),
     "ge_export_tree": ([_vp, C.c_int64, _vp] + [_vp] * 8, C.c_int),
+    "ge_direct_sum_f64": ([_vp, C.c_int64, _vp, _vp, _vp, _vp], C.c_int),
+    "ge_sums_f64": ([_vp, _vp], C.c_int),
 }
 
 
@@ -282,6 +284,21 @@ class Simulation:
 
     def count_interactions(self, enable=True):
         self._check(lib().ge_set_count_interactions(self._h, 1 if enable else 0))
+
+    def direct_sum_f64(self, idx):
+        """FP64 direct-sum accelerations of the particles at indices idx of the
+        current order (the accuracy reference)."""
+        idx = np.ascontiguousarray(idx, np.uint32)
+        out = [np.zeros(len(idx), np.float64) for _ in range(self.dims)]
+        self._check(lib().ge_direct_sum_f64(self._h, len(idx), _ptr(idx), _ptr(out[0]),
+                                            _ptr(out[1]), _ptr(out[2]) if self.dims == 3 else None))
+        return out
+
+    def sums_f64(self):
+        """{kinetic energy, p_x, p_y, p_z, total mass} in FP64."""
+        out = np.zeros(5, np.float64)
+        self._check(lib().ge_sums_f64(self._h, _ptr(out)))
+        return out
 
     def export_tree(self):
         """The tree as the reference's globalNodes: pre-order numpy arrays."""

@@ -637,6 +637,49 @@ int ge_integrate_end(ge_ctx *c) {
     return GE_OK;
 }
 
+int ge_direct_sum_f64(ge_ctx *c, int64_t nt, const uint32_t *idx, double *ax, double *ay,
+                      double *az) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (nt < 0 || (nt > 0 && (!idx || !ax || !ay))) return fail(c, GE_ERR_ARG, "bad sample");
+    if (nt == 0) return GE_OK;
+    for (int64_t k = 0; k < nt; k++)
+        if ((int64_t)idx[k] >= c->n) return fail(c, GE_ERR_ARG, "sample index out of range");
+    const int D = c->p.dims;
+    uint32_t *d_idx = nullptr;
+    double *d_out = nullptr;
+    GE_CHECK(c, cudaMallocAsync((void **)&d_idx, sizeof(uint32_t) * nt, c->stream));
+    GE_CHECK(c, cudaMallocAsync((void **)&d_out, sizeof(double) * nt * D, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(d_idx, idx, sizeof(uint32_t) * nt, cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, launch_direct_f64(D, cur_state(c), (int)c->n, d_idx, (int)nt, (double)c->p.G,
+                                  (double)c->p.eps2, d_out, c->stream));
+    std::vector<double> h((size_t)(nt * D));
+    GE_CHECK(c, cudaMemcpyAsync(h.data(), d_out, sizeof(double) * nt * D, cudaMemcpyDeviceToHost,
+                                c->stream));
+    GE_CHECK(c, cudaFreeAsync(d_idx, c->stream));
+    GE_CHECK(c, cudaFreeAsync(d_out, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    for (int64_t k = 0; k < nt; k++) {
+        ax[k] = h[(size_t)(k * D)];
+        ay[k] = h[(size_t)(k * D + 1)];
+        if (D == 3 && az) az[k] = h[(size_t)(k * D + 2)];
+    }
+    return GE_OK;
+}
+
+int ge_sums_f64(ge_ctx *c, double *out) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!out) return fail(c, GE_ERR_ARG, "out is NULL");
+    double *d = nullptr;
+    GE_CHECK(c, cudaMallocAsync((void **)&d, sizeof(double) * 5, c->stream));
+    GE_CHECK(c, launch_sums_f64(c->p.dims, cur_state(c), (int)c->n, d, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(out, d, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaFreeAsync(d, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    return GE_OK;
+}
+
 int ge_export_tree(ge_ctx *c, int64_t cap, int64_t *count, float *pos, float *size, float *com,
                    float *mass, uint32_t *start, uint32_t *end, uint32_t *next,
                    uint32_t *child) {

@@ -89,5 +89,9 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         const Tree &t, bool integrate_end, unsigned long long *inter_count,
                         uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+// FP64 diagnostics
+cudaError_t launch_direct_f64(int dims, const State &s, int n, const uint32_t *idx, int nt,
+                              double G, double eps2, double *out, cudaStream_t st);
+cudaError_t launch_sums_f64(int dims, const State &s, int n, double *out, cudaStream_t st);
 
 }  // namespace ge

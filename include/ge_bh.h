@@ -156,6 +156,15 @@ int ge_integrate_end(ge_ctx *ctx);
 /* enable per-particle interaction counting in ge_compute_forces (stats) */
 int ge_set_count_interactions(ge_ctx *ctx, int32_t enable);
 
+/* --- FP64 diagnostics (accuracy reference; not on the step path) ------- */
+/* Direct-sum accelerations in FP64 of the particles at indices idx[0..nt) of
+   the current order: sum over j != i of G m_j d / (|d|^2 + eps2)^(3/2).
+   ax/ay/az (host, nt doubles each; az ignored in 2D). */
+int ge_direct_sum_f64(ge_ctx *ctx, int64_t nt, const uint32_t *idx, double *ax, double *ay,
+                      double *az);
+/* FP64 sums over the state: out = {kinetic energy, p_x, p_y, p_z, total mass} */
+int ge_sums_f64(ge_ctx *ctx, double *out);
+
 /* --- tree export: the reference's globalNodes in DFS pre-order --------- */
 /* Returns the node count in *count.  Arrays (capacity cap nodes; any may be
    NULL): pos/com [cap*dims], size, mass [cap], start, end, next [cap],
