@@ -97,7 +97,9 @@ SIGNATURES = {
     "ge_export_tree": ([_vp, C.c_int64, _vp] + [_vp] * 8, C.c_int),
     "ge_direct_sum_f64": ([_vp, C.c_int64, _vp, _vp, _vp, _vp], C.c_int),
     "ge_sums_f64": ([_vp, _vp], C.c_int),
+    "ge_morton_sort_2d_noalloc": ([C.c_int64, _vp, _vp, _vp, _vp, _vp], C.c_int),
 }
+NOALLOC_MAX_N = 262144   # GE_NOALLOC_MAX_N
 
 
 def lib():

@@ -165,6 +165,33 @@ int ge_direct_sum_f64(ge_ctx *ctx, int64_t nt, const uint32_t *idx, double *ax, 
 /* FP64 sums over the state: out = {kinetic energy, p_x, p_y, p_z, total mass} */
 int ge_sums_f64(ge_ctx *ctx, double *out);
 
+/* --- 2D Morton sort without device allocation --------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory, such as an application that carves its device
+ * memory into a fixed arena up front and accounts for every byte itself, or
+ * a frame loop that must not call cudaMalloc / cudaFree because they can
+ * synchronise the whole device mid-frame.
+ *
+ * Same result as ge_compute_morton_keys + ge_sort_by_morton_key on a context
+ * (root box, Morton keys, stable radix sort), on caller-owned DEVICE buffers:
+ * d_x, d_y (n floats each, read), d_perm (n uint32: the input index that
+ * lands in each sorted slot), d_keys (optional, n uint64: the sorted keys).
+ * `stream` is a cudaStream_t (NULL: the legacy default stream).
+ *
+ * All temporaries live in one fixed-size device array inside the library
+ * (about 4.6 MB on every GPU that loads it, held until the process exits), so
+ * n is limited to GE_NOALLOC_MAX_N; larger n returns GE_ERR_CAPACITY without
+ * launching anything.  The first call on each device looks up that array's
+ * device address (cudaGetSymbolAddress) for the current device; make that
+ * first call before any stream capture.  Every call shares the one array:
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * corrupt each other's results, so serialise them.  The call waits for its
+ * work to finish and returns GE_ERR_TIMEOUT if a bounded device-side wait gave
+ * up.  It calls no allocating routine. */
+#define GE_NOALLOC_MAX_N 262144
+int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const float *d_y, uint32_t *d_perm,
+                              uint64_t *d_keys, void *stream);
+
 /* --- tree export: the reference's globalNodes in DFS pre-order --------- */
 /* Returns the node count in *count.  Arrays (capacity cap nodes; any may be
    NULL): pos/com [cap*dims], size, mass [cap], start, end, next [cap],
