@@ -97,6 +97,7 @@ SIGNATURES = {
     "ge_export_tree": ([_vp, C.c_int64, _vp] + [_vp] * 8, C.c_int),
     "ge_direct_sum_f64": ([_vp, C.c_int64, _vp, _vp, _vp, _vp], C.c_int),
     "ge_sums_f64": ([_vp, _vp], C.c_int),
+    "ge_build_timeline": ([_vp, C.c_int32, _vp, _vp], C.c_int),
     "ge_morton_sort_2d_noalloc": ([C.c_int64, _vp, _vp, _vp, _vp, _vp], C.c_int),
 }
 NOALLOC_MAX_N = 262144   # GE_NOALLOC_MAX_N
@@ -295,6 +296,13 @@ class Simulation:
         self._check(lib().ge_direct_sum_f64(self._h, len(idx), _ptr(idx), _ptr(out[0]),
                                             _ptr(out[1]), _ptr(out[2]) if self.dims == 3 else None))
         return out
+
+    def build_timeline(self):
+        """Device time (ns) at each grid barrier of the last tree build."""
+        ns = np.zeros(256, np.uint64)
+        cnt = C.c_int32(0)
+        self._check(lib().ge_build_timeline(self._h, 256, _ptr(ns), C.byref(cnt)))
+        return ns[: cnt.value].copy()
 
     def sums_f64(self):
         """{kinetic energy, p_x, p_y, p_z, total mass} in FP64."""

@@ -36,7 +36,8 @@ struct ge_ctx {
     Tree tree{};
     uint32_t *d_err = nullptr;
     unsigned long long *d_inter = nullptr;
-    uint32_t *h_meta = nullptr;   // pinned: meta[0..4]
+    uint32_t *h_meta = nullptr;   // pinned copy of the tree meta words
+    int64_t slots = 0;            // node slots of the last build (holes included)
     bool count_inter = false;
     bool tree_valid = false;
     bool keys_valid = false;
@@ -124,7 +125,9 @@ int validate(ge_ctx *c, const ge_params *p) {
 // (Re)allocate every device buffer for n particles.
 int ensure_capacity(ge_ctx *c, int64_t n) {
     const int D = c->p.dims;
-    const int64_t node_cap = (int64_t)(c->p.node_cap_factor * (double)n) + 1024;
+    const int64_t slack = build_node_slack(D, c->num_sms);
+    if (slack <= 0) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
+    const int64_t node_cap = (int64_t)(c->p.node_cap_factor * (double)n) + 1024 + slack;
     if (n <= c->cap_n && node_cap <= c->tree.cap && c->has_prev == (bool)c->p.track_prev_vel)
         return GE_OK;
     if (D == 2 && n >= (1ll << 28)) return fail(c, GE_ERR_ARG, "2D supports N < 2^28");
@@ -169,10 +172,28 @@ int ensure_capacity(ge_ctx *c, int64_t n) {
     if (D == 3) GE_CHECK(c, dalloc(c, &t.size2, (size_t)node_cap));
     GE_CHECK(c, dalloc(c, &t.info, (size_t)node_cap));
     GE_CHECK(c, dalloc(c, &t.cell, (size_t)node_cap));
+    GE_CHECK(c, dalloc(c, &t.aux, (size_t)node_cap));
+    GE_CHECK(c, dalloc(c, &t.pend, (size_t)node_cap));
+    GE_CHECK(c, dalloc(c, &t.small, N / 2 + 1));
+    GE_CHECK(c, dalloc(c, &t.endcnt, N + 1));
+    const int bblocks = build_grid_blocks(D, c->num_sms);
+    if (bblocks < 1) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
+    GE_CHECK(c, dalloc(c, &t.blocksum, (size_t)bblocks));
+    GE_CHECK(c, dalloc(c, &t.src, N + (size_t)node_cap));
+    if (D == 2) {
+        uint2 *l = nullptr;
+        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap));
+        t.link = l;
+    } else {
+        uint4 *l = nullptr;
+        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap));
+        t.link = l;
+    }
     GE_CHECK(c, dalloc(c, &t.level, kMaxLevels + 2));
     GE_CHECK(c, dalloc(c, &t.lvl_alloc, kMaxLevels + 2));
-    GE_CHECK(c, dalloc(c, &t.meta, 8));
-    GE_CHECK(c, cudaMemset(t.meta, 0, 8 * sizeof(uint32_t)));
+    GE_CHECK(c, dalloc(c, &t.meta, 16));
+    GE_CHECK(c, dalloc(c, &t.tl, kTimeline));
+    GE_CHECK(c, cudaMemset(t.meta, 0, 16 * sizeof(uint32_t)));
     c->d_err = t.meta + 4;
     GE_CHECK(c, dalloc(c, &c->d_inter, 1));
     c->cap_n = n;
@@ -183,12 +204,13 @@ int ensure_capacity(ge_ctx *c, int64_t n) {
 
 // Reads back the error word and tree size; clears the error word.
 int check_device(ge_ctx *c) {
-    GE_CHECK(c, cudaMemcpyAsync(c->h_meta, c->tree.meta, 5 * sizeof(uint32_t),
+    GE_CHECK(c, cudaMemcpyAsync(c->h_meta, c->tree.meta, 10 * sizeof(uint32_t),
                                 cudaMemcpyDeviceToHost, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     const uint32_t e = c->h_meta[4];
     c->stats.nodes = c->h_meta[0];
     c->stats.depth = (int32_t)c->h_meta[1];
+    c->slots = c->h_meta[9];
     if (e) {
         GE_CHECK(c, cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), c->stream));
         GE_CHECK(c, cudaStreamSynchronize(c->stream));
@@ -327,7 +349,7 @@ int ge_create(const ge_params *p, ge_ctx **out) {
         return GE_ERR_CUDA;
     }
     for (auto &e : c->ev) cudaEventCreate(&e);
-    if (cudaMallocHost(&c->h_meta, 8 * sizeof(uint32_t)) != cudaSuccess) {
+    if (cudaMallocHost(&c->h_meta, 16 * sizeof(uint32_t)) != cudaSuccess) {
         ge_destroy(c);
         return GE_ERR_CUDA;
     }
@@ -667,6 +689,21 @@ int ge_direct_sum_f64(ge_ctx *c, int64_t nt, const uint32_t *idx, double *ax, do
     return GE_OK;
 }
 
+int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!count || (cap > 0 && !ns)) return fail(c, GE_ERR_ARG, "bad timeline buffers");
+    uint32_t m[8];
+    GE_CHECK(c, cudaMemcpyAsync(m, c->tree.meta, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long tl[kTimeline];
+    GE_CHECK(c, cudaMemcpyAsync(tl, c->tree.tl, sizeof(tl), cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    const int32_t k = (int32_t)(m[7] < (uint32_t)kTimeline ? m[7] : kTimeline);
+    *count = k;
+    for (int32_t i = 0; i < k && i < cap; i++) ns[i] = (uint64_t)(tl[i] - tl[0]);
+    return GE_OK;
+}
+
 int ge_sums_f64(ge_ctx *c, double *out) {
     int rc = require_state(c);
     if (rc) return rc;
@@ -691,17 +728,19 @@ int ge_export_tree(ge_ctx *c, int64_t cap, int64_t *count, float *pos, float *si
     const int64_t nn = c->stats.nodes;
     if (count) *count = nn;
     if (nn > cap) return fail(c, GE_ERR_CAPACITY, "export capacity smaller than the node count");
-    std::vector<float4> w((size_t)nn), cell((size_t)nn);
-    std::vector<uint4> inf((size_t)nn);
-    GE_CHECK(c, cudaMemcpy(w.data(), c->tree.walk, sizeof(float4) * nn, cudaMemcpyDeviceToHost));
-    GE_CHECK(c, cudaMemcpy(cell.data(), c->tree.cell, sizeof(float4) * nn, cudaMemcpyDeviceToHost));
-    GE_CHECK(c, cudaMemcpy(inf.data(), c->tree.info, sizeof(uint4) * nn, cudaMemcpyDeviceToHost));
+    // nodes sit in the first `slots` entries, with unused (hole) slots among them
+    const int64_t ns = c->slots > nn ? c->slots : nn;
+    std::vector<float4> w((size_t)ns), cell((size_t)ns);
+    std::vector<uint4> inf((size_t)ns);
+    GE_CHECK(c, cudaMemcpy(w.data(), c->tree.walk, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
+    GE_CHECK(c, cudaMemcpy(cell.data(), c->tree.cell, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
+    GE_CHECK(c, cudaMemcpy(inf.data(), c->tree.info, sizeof(uint4) * ns, cudaMemcpyDeviceToHost));
     // depth-first pre-order numbering, children in slot order (the reference's
     // emission order, quadtree.cpp:67-87); next = number of descendants
     std::vector<uint32_t> order;
     order.reserve((size_t)nn);
     std::vector<uint32_t> stack{0u};
-    std::vector<uint32_t> newid((size_t)nn, kEmpty);
+    std::vector<uint32_t> newid((size_t)ns, kEmpty);
     while (!stack.empty()) {
         uint32_t k = stack.back();
         stack.pop_back();
@@ -712,7 +751,7 @@ int ge_export_tree(ge_ctx *c, int64_t cap, int64_t *count, float *pos, float *si
         for (int cidx = nc - 1; cidx >= 0; --cidx) stack.push_back(inf[k].x + (uint32_t)cidx);
     }
     if ((int64_t)order.size() != nn) return fail(c, GE_ERR_STATE, "tree is not connected");
-    std::vector<uint32_t> desc((size_t)nn, 0);
+    std::vector<uint32_t> desc((size_t)ns, 0);
     for (int64_t r = nn - 1; r >= 0; --r) {
         const uint32_t k = order[(size_t)r];
         const uint32_t mask = inf[k].y;

@@ -26,14 +26,41 @@ struct State {
 //                   first_child in increasing q; child_mask == 0 marks a leaf
 //   cell    float4  {corner.x, corner.y, corner.z, size} (build only)
 //   level   uint32  first node of each level (nodes are stored level by level)
+//   aux     uint4   {level, number of proper ancestors whose range ends where this
+//                   node's range ends, parent, 0} (build only)
+//   pend    uint32  children whose mass is not final yet (build only)
+//
+// Walk layout (written at the end of the build): one array of "sources" in
+// which particles come first (index j < n, in Morton order) and the nodes
+// follow in depth-first pre-order (index n + pre(k)):
+//   src     float4  2D node {com.x, com.y, mass, size^2}; particle {x, y, m, -1}
+//                   3D node {com.x, com.y, com.z, mass};  particle {x, y, z, m}
+//   link    2D uint2 {skip, descend}; 3D uint4 {skip, descend, size^2 bits, 0}
+//                   (3D particles carry size^2 = -1).  skip is where the walk goes
+//                   after accepting the source (the subtree's successor in
+//                   pre-order, or the next particle of the same leaf), descend
+//                   where it goes when the source is opened (first child, or the
+//                   leaf's first particle).  The walk ends at n + node_count.
+// The pre-order position needs no top-down pass: with C(e) = #{nodes whose
+// range ends at or before e}, pre(k) = C(start_k) + level_k and the subtree
+// successor is C(end_k) + level_k - same_end_ancestors_k.
 struct Tree {
     float4 *walk;
     float *size2;
     uint4 *info;
     float4 *cell;
+    uint4 *aux;
+    uint32_t *pend;
+    uint32_t *small;      // [n / 2] queued small subtrees (build only)
+    uint32_t *endcnt;    // [n + 1] node-end histogram, scanned in place
+    uint32_t *blocksum;   // [build grid] scan partials
+    float4 *src;          // [n + cap]
+    void *link;           // [n + cap] uint2 (2D) / uint4 (3D)
     uint32_t *level;      // [kMaxLevels + 2]
     uint32_t *lvl_alloc;  // [kMaxLevels + 2] per-level child allocation counters
-    uint32_t *meta;       // [4] {node_count, levels, bar_count, bar_gen}
+    uint32_t *meta;       // [8] {node_count, levels, bar_count, bar_gen, err, small,
+                          //      phase-2 nodes, timeline entries}
+    unsigned long long *tl;   // [kTimeline] build timeline (globaltimer ns)
     int64_t cap;
 };
 
@@ -63,6 +90,7 @@ struct StepParams {
 
 constexpr int kBBoxThreads = 256;
 constexpr int kSortTile = 4096;   // keys per look-back tile (256 threads x 16)
+constexpr int kTimeline = 256;    // build timeline entries
 
 // --- launchers (each runs on `st`) ----------------------------------------
 // integrateStart (kick + drift) fused with the bounding-box reduction; the
@@ -81,7 +109,9 @@ cudaError_t launch_perm_out(int dims, int n, const SortScratch &ss, uint32_t *pe
                             cudaStream_t st);
 cudaError_t launch_keys_out(int dims, int n, const SortScratch &ss, uint64_t *keys,
                             cudaStream_t st);
-// tree build + mass/centre of mass (one cooperative launch)
+// tree build + mass/centre of mass + walk layout (one cooperative launch)
+int build_grid_blocks(int dims, int num_sms);
+int64_t build_node_slack(int dims, int num_sms);
 cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
                          int num_sms, cudaStream_t st);
 // tree walk; integrate_end fuses integrateEnd (v += a*dt/2)

@@ -1,4 +1,5 @@
-// ge_tree.cu -- quadtree / octree construction with mass and centre of mass.
+// ge_tree.cu -- quadtree / octree construction with mass and centre of mass,
+// and the depth-first walk layout.
 //
 // Reference: Node::Node, Node::subGridMaker, computeLeafMass, computeInternalMass
 // (GalaxyEngine/src/Physics/quadtree.cpp:5-88, include/Physics/quadtree.h:31-111)
@@ -6,20 +7,29 @@
 //
 // The reference builds recursively: a node over the Morton-sorted range
 // [start, end) is a leaf when ((count <= 4 && size <= 2) || count == 1 ||
-// size <= 1e-6); otherwise the range is cut by std::partition_point on
-// float midpoint compares (y then x; z then y then x in 3D) and one child is
-// made per non-empty quadrant.  This kernel makes the same nodes level by
-// level: one warp per node evaluates the three (seven) partition points with
-// the exact probe sequence of std::partition_point (GNU halving search),
-// resolving log2(G) halving steps per round with G-1 lanes probing the G-1
-// nodes of the next levels of the search's decision tree.  Because the probes
-// are the reference's own, the cut points agree with the reference even where
-// the float compares disagree with the Morton order and the range is not
-// partitioned.  Children of a level are allocated by one atomic per block
-// per batch of nodes; levels are separated by a bounded grid barrier inside
-// one cooperative launch, and masses / centres of mass are then combined
-// bottom-up, level by level, reading children in the reference's x-major
-// subGrids order so every float sum rounds exactly as the reference's does.
+// size <= 1e-6); otherwise the range is cut by std::partition_point on float
+// midpoint compares (y then x; z then y then x in 3D) and one child is made
+// per non-empty quadrant.  Every cut point here is found with the exact probe
+// sequence of std::partition_point (the GNU halving search), so the cut points
+// agree with the reference even where float compares disagree with the Morton
+// order and a range is not partitioned.
+//
+// One cooperative launch, three phases:
+//  1. Nodes of more than kSmallNode particles are split level by level
+//     (bounded grid barrier between levels).  A group of G lanes cuts one
+//     node: G-1 lanes probe the G-1 nodes of the next log2(G) levels of the
+//     search's decision tree per round.  Smaller non-leaf nodes are queued.
+//  2. Each queued node's whole subtree is built by one warp without further
+//     barriers: lane l holds particle start + l, the predicates of all its
+//     particles against a node's midpoint come from one ballot, and the
+//     searches run on those bits.
+//  3. The depth-first walk layout (ge_internal.h) is scattered from the node
+//     ranges: pre(k) = C(start) + level, successor = C(end) + level - same_end,
+//     with C the prefix count of node ends.
+// A node's mass and centre of mass are computed as soon as its last child is
+// final (a per-node pending count), always reading the children in the
+// reference's x-major subGrids order with the reference's rounding, so the
+// sums are bit-identical to the reference's whatever order nodes finish in.
 #include <cfloat>
 
 #include "ge_device.cuh"
@@ -28,7 +38,12 @@
 namespace ge {
 
 constexpr int kBuildThreads = 256;
-constexpr int kBuildWarps = kBuildThreads / 32;
+constexpr uint32_t kSmallNode = 32;
+
+// meta[] words used by the build
+constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 3,
+              kMetaSmall = 5, kMetaP2Alloc = 6, kMetaReal = 8, kMetaSlots = 9;
+constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
 __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_gen,
@@ -47,7 +62,6 @@ __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_
             uint32_t spins = 0;
             while (*vgen == gen) {
                 if (++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -55,12 +69,23 @@ __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_
     __syncthreads();
 }
 
+// Build timeline: one globaltimer stamp per grid barrier (thread 0 only).
+__device__ __forceinline__ void stamp(Tree &t) {
+    unsigned long long ns;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+    const uint32_t i = t.meta[7];
+    if (i < (uint32_t)kTimeline) {
+        t.tl[i] = ns;
+        t.meta[7] = i + 1;
+    }
+}
+
 // std::partition_point(v + first, v + first + len, [mid](float a){ return a < mid; })
-// emulated by G consecutive lanes.  Lane j (1 <= j < G) of the group stands
-// for node j of the search's decision tree (heap order; child 2j when the
-// probe is false, 2j+1 when true); one round evaluates all of them and walks
-// log2(G) steps.  All 32 lanes must call this together; groups may differ in
-// their arguments.
+// emulated by G consecutive lanes.  Lane j (1 <= j < G) of the group stands for
+// node j of the search's decision tree (heap order; child 2j when the probe is
+// false, 2j+1 when true); one round evaluates all of them and walks log2(G)
+// steps.  All 32 lanes call this together; groups may differ in their
+// arguments (len 0 for a group with nothing to search).
 template <int G>
 __device__ __forceinline__ uint32_t group_partition_point(const float *__restrict__ v,
                                                           uint32_t first, uint32_t len,
@@ -96,124 +121,605 @@ __device__ __forceinline__ uint32_t group_partition_point(const float *__restric
     return first;
 }
 
-template <int D>
-__device__ __forceinline__ const float *axis_ptr(const State &s, int a) {
-    return a == 0 ? s.x : (a == 1 ? s.y : s.z);
+// Cut points of one node per group of G lanes: Node::subGridMaker (y, then x
+// in each half) / subGridMaker3D (z, then y in each half, then x in each
+// quarter).  Every lane of the group ends with the group's b[0..Q].
+template <int D, int G>
+__device__ __forceinline__ void cut_group(const State &s, uint32_t st, uint32_t en,
+                                          const float *mid, uint32_t *b) {
+    constexpr int Q = 1 << D;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gl = lane & (G - 1u), gbase = lane & ~(G - 1u);
+    b[0] = st; b[Q] = en;
+    if (D == 2) {
+        b[2] = group_partition_point<G>(s.y, st, en - st, mid[1]);
+        const bool lo = gl < G / 2;
+        const uint32_t f = lo ? st : b[2];
+        const uint32_t l = lo ? b[2] - st : en - b[2];
+        const uint32_t r = group_partition_point<G / 2>(s.x, f, l, mid[0]);
+        b[1] = __shfl_sync(0xffffffffu, r, gbase);
+        b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
+    } else {
+        b[4] = group_partition_point<G>(s.z, st, en - st, mid[2]);
+        const bool lo = gl < G / 2;
+        uint32_t f = lo ? st : b[4];
+        uint32_t l = lo ? b[4] - st : en - b[4];
+        uint32_t r = group_partition_point<G / 2>(s.y, f, l, mid[1]);
+        b[2] = __shfl_sync(0xffffffffu, r, gbase);
+        b[6] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
+        const unsigned g4 = gl / (G / 4);
+        const uint32_t a0 = g4 == 0 ? st : (g4 == 1 ? b[2] : (g4 == 2 ? b[4] : b[6]));
+        const uint32_t a1 = g4 == 0 ? b[2] : (g4 == 1 ? b[4] : (g4 == 2 ? b[6] : en));
+        r = group_partition_point<G / 4>(s.x, a0, a1 - a0, mid[0]);
+        b[1] = __shfl_sync(0xffffffffu, r, gbase);
+        b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 4);
+        b[5] = __shfl_sync(0xffffffffu, r, gbase + 2 * (G / 4));
+        b[7] = __shfl_sync(0xffffffffu, r, gbase + 3 * (G / 4));
+    }
+}
+
+// std::partition_point over predicate bits held in a register (bit r is the
+// predicate of element r), GNU probe sequence, positions relative to bit 0
+__device__ __forceinline__ uint32_t bits_partition_point(uint32_t bits, uint32_t first,
+                                                         uint32_t len) {
+    while (len > 0) {
+        const uint32_t half = len >> 1;
+        const uint32_t probe = first + half;
+        if ((bits >> probe) & 1u) { first = probe + 1; len -= half + 1; }
+        else { len = half; }
+    }
+    return first;
 }
 
 template <int D>
-__global__ void __launch_bounds__(kBuildThreads)
-k_build(State s, StepParams p, Tree t, uint32_t *err) {
-    constexpr int Q = 1 << D;
-    __shared__ uint32_t s_cnt[kBuildWarps], s_off[kBuildWarps], s_base;
-    const int warp = threadIdx.x >> 5;
-    const unsigned lane = threadIdx.x & 31u;
-    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t cap = (uint32_t)t.cap;
-    uint32_t *bar_count = t.meta + 2, *bar_gen = t.meta + 3;
+__device__ __forceinline__ bool is_leaf(const StepParams &p, uint32_t cnt, float size) {
+    // quadtree.cpp:16 / :120 with the leaf capacity and size gate parameterised
+    return ((cnt <= p.leaf_cap && size <= p.size_gate) || cnt == 1u) || size <= p.min_size;
+}
 
-    uint32_t lb = 0, le = 1;
-    int L = 0;
-    if (gtid == 0) t.level[0] = 0;
-    while (true) {
-        for (uint32_t kb = lb + blockIdx.x * kBuildWarps; kb < le;
-             kb += gridDim.x * kBuildWarps) {
-            const uint32_t k = kb + warp;
-            const bool valid = k < le;
-            uint32_t mask = 0, bnd[Q + 1];
-            float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
-            uint32_t st = 0, en = 0;
-            bool leaf = true;
-            if (valid) {
-                // written by other blocks in the previous level: read through L2
-                const uint4 inf = __ldcg(&t.info[k]);
-                cell = __ldcg(&t.cell[k]);
-                st = inf.z; en = inf.w;
-                const uint32_t cnt = en - st;
-                const float size = cell.w;
-                leaf = ((cnt <= p.leaf_cap && size <= p.size_gate) || cnt == 1u) ||
-                       size <= p.min_size;
-            }
-            const float half = fmul(cell.w, 0.5f);
-            if (!leaf) {
-                // children cut points, exactly as Node::subGridMaker[3D]
-                const float midx = fadd(cell.x, half), midy = fadd(cell.y, half);
-                bnd[0] = st; bnd[Q] = en;
-                if (D == 2) {
-                    bnd[2] = group_partition_point<32>(s.y, st, en - st, midy);
-                    const uint32_t f = lane < 16 ? st : bnd[2];
-                    const uint32_t l = lane < 16 ? bnd[2] - st : en - bnd[2];
-                    const uint32_t r = group_partition_point<16>(s.x, f, l, midx);
-                    bnd[1] = __shfl_sync(0xffffffffu, r, 0);
-                    bnd[3] = __shfl_sync(0xffffffffu, r, 16);
-                } else {
-                    const float midz = fadd(cell.z, half);
-                    bnd[4] = group_partition_point<32>(s.z, st, en - st, midz);
-                    uint32_t f = lane < 16 ? st : bnd[4];
-                    uint32_t l = lane < 16 ? bnd[4] - st : en - bnd[4];
-                    uint32_t r = group_partition_point<16>(s.y, f, l, midy);
-                    bnd[2] = __shfl_sync(0xffffffffu, r, 0);
-                    bnd[6] = __shfl_sync(0xffffffffu, r, 16);
-                    const unsigned g = lane >> 3;
-                    f = bnd[2 * g];
-                    l = bnd[2 * g + 2] - bnd[2 * g];
-                    r = group_partition_point<8>(s.x, f, l, midx);
-                    bnd[1] = __shfl_sync(0xffffffffu, r, 0);
-                    bnd[3] = __shfl_sync(0xffffffffu, r, 8);
-                    bnd[5] = __shfl_sync(0xffffffffu, r, 16);
-                    bnd[7] = __shfl_sync(0xffffffffu, r, 24);
-                }
+// computeLeafMass / computeLeafMass3D: sequential sums in the reference's order
+template <int D>
+__device__ __forceinline__ float4 leaf_mass(const State &s, uint32_t st, uint32_t en) {
+    float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+    for (uint32_t i = st; i < en; i++) {
+        const float mi = s.m[i];
+        gm = fadd(gm, mi);
+        c[0] = fadd(c[0], fmul(s.x[i], mi));
+        c[1] = fadd(c[1], fmul(s.y[i], mi));
+        if (D == 3) c[2] = fadd(c[2], fmul(s.z[i], mi));
+    }
+    if (gm > 0.0f) {
+        c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+        if (D == 3) c[2] = fdiv(c[2], gm);
+    }
+    return make_float4(c[0], c[1], c[2], gm);
+}
+
+template <int D>
+__device__ __forceinline__ void put_walk(Tree &t, uint32_t k, float4 cm, float size) {
+    const float s2 = fmul(size, size);
+    if (D == 2) t.walk[k] = make_float4(cm.x, cm.y, cm.w, s2);
+    else { t.walk[k] = make_float4(cm.x, cm.y, cm.z, cm.w); t.size2[k] = s2; }
+}
+
+// computeInternalMass / computeInternalMass3D: children read in the
+// reference's subGrids[x][y]([z]) order, x outermost
+template <int D>
+__device__ __forceinline__ float4 combine_children(const Tree &t, uint4 inf) {
+    constexpr int Q = 1 << D;
+    float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-                for (int q = 0; q < Q; q++) mask |= (bnd[q + 1] > bnd[q] ? 1u : 0u) << q;
-            } else if (valid && lane == 0) {
-                // computeLeafMass: sequential sums in the reference's order
+    for (int kk = 0; kk < Q; kk++) {
+        unsigned q;
+        if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
+        else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
+        if (!((inf.y >> q) & 1u)) continue;
+        const uint32_t ci = inf.x + __popc(inf.y & ((1u << q) - 1u));
+        const float4 cw = __ldcg(&t.walk[ci]);
+        const float cm = D == 2 ? cw.z : cw.w;
+        gm = fadd(gm, cm);
+        c[0] = fadd(c[0], fmul(cw.x, cm));
+        c[1] = fadd(c[1], fmul(cw.y, cm));
+        if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cm));
+    }
+    if (gm > 0.0f) {
+        c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+        if (D == 3) c[2] = fdiv(c[2], gm);
+    }
+    return make_float4(c[0], c[1], c[2], gm);
+}
+
+// Node k's mass is final: tell its parent.  The child that completes a
+// parent's set combines the parent (in the reference's child order, so the
+// result does not depend on which child came last) and carries on upward.
+template <int D>
+__device__ __forceinline__ void finish_upward(Tree &t, uint32_t k) {
+    __threadfence();
+    uint32_t par = __ldcg(&t.aux[k]).z;
+    while (par != kEmpty) {
+        if (atomicSub(&t.pend[par], 1u) != 1u) break;
+        __threadfence();
+        const uint4 inf = __ldcg(&t.info[par]);
+        put_walk<D>(t, par, combine_children<D>(t, inf), __ldcg(&t.cell[par]).w);
+        __threadfence();
+        par = __ldcg(&t.aux[par]).z;
+    }
+}
+
+// Corner of child slot q of a cell (Node::subGridMaker newPos).
+template <int D>
+__device__ __forceinline__ float4 child_cell(float4 cell, float half, unsigned q) {
+    float4 cc;
+    cc.x = fadd(cell.x, (q & 1u) ? half : 0.0f);
+    cc.y = fadd(cell.y, (q & 2u) ? half : 0.0f);
+    cc.z = D == 3 ? fadd(cell.z, (q & 4u) ? half : 0.0f) : 0.0f;
+    cc.w = half;
+    return cc;
+}
+
+// Write node k's children (slots in increasing q from `first`) and its own
+// child links; the pending count is set atomically before any child can finish.
+template <int D>
+__device__ __forceinline__ void emit_children(Tree &t, uint32_t k, uint32_t first, uint32_t mask,
+                                              const uint32_t *b, float4 cell, float half,
+                                              uint4 inf, uint4 ax) {
+    constexpr int Q = 1 << D;
+    uint32_t ci = first;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        if (!((mask >> q) & 1u)) continue;
+        t.cell[ci] = child_cell<D>(cell, half, (unsigned)q);
+        t.info[ci] = make_uint4(0u, 0u, b[q], b[q + 1]);
+        // same-end ancestors: the child ends where its parent ends
+        t.aux[ci] = make_uint4(ax.x + 1u, b[q + 1] == inf.w ? ax.y + 1u : 0u, k, 0u);
+        ci++;
+    }
+    t.info[k] = make_uint4(first, mask, inf.z, inf.w);
+    atomicExch(&t.pend[k], (uint32_t)__popc(mask));
+    __threadfence();
+}
+
+// Phase 1 work of one node per group of G lanes.
+template <int D, int G>
+__device__ __forceinline__ void split_level_node(const State &s, const StepParams &p, Tree &t,
+                                                 uint32_t k, bool valid, uint32_t level_end,
+                                                 uint32_t *lvl_alloc, uint32_t *err) {
+    constexpr int Q = 1 << D;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gl = lane & (G - 1u);
+    uint4 inf = make_uint4(0, 0, 0, 0), ax = make_uint4(0, 0, 0, 0);
+    float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        // written by other blocks during the previous level: read through L2
+        inf = __ldcg(&t.info[k]);
+        cell = __ldcg(&t.cell[k]);
+        ax = __ldcg(&t.aux[k]);
+    }
+    const uint32_t cnt = inf.w - inf.z;
+    const bool leaf = valid && is_leaf<D>(p, cnt, cell.w);
+    const bool small = valid && !leaf && cnt <= kSmallNode;
+    const bool split = valid && !leaf && !small;
+    const float half = fmul(cell.w, 0.5f);
+    const float mid[3] = {fadd(cell.x, half), fadd(cell.y, half), fadd(cell.z, half)};
+    uint32_t b[Q + 1];
+    cut_group<D, G>(s, split ? inf.z : 0u, split ? inf.w : 0u, mid, b);
+    uint32_t mask = 0;
+    if (split) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
+    }
+    const bool leader = gl == 0;
+    if (leader && leaf) {
+        put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), cell.w);
+        finish_upward<D>(t, k);
+    }
+    // queue the small subtrees (one atomic per warp)
+    {
+        const unsigned qb = __ballot_sync(0xffffffffu, leader && small);
+        uint32_t qbase = 0;
+        if (lane == 0 && qb) qbase = atomicAdd(&t.meta[kMetaSmall], (uint32_t)__popc(qb));
+        qbase = __shfl_sync(0xffffffffu, qbase, 0);
+        if (leader && small) t.small[qbase + __popc(qb & ((1u << lane) - 1u))] = k;
+    }
+    // children of the split nodes (one atomic per warp)
+    const uint32_t nch = (leader && split) ? (uint32_t)__popc(mask) : 0u;
+    uint32_t incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+    }
+    const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 0 && tot) base = atomicAdd(lvl_alloc, tot);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (nch) {
+        const uint32_t first = level_end + base + incl - nch;
+        if ((uint64_t)first + nch > (uint64_t)t.cap) set_err(err, kErrNodeCap);
+        else emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+    }
+}
+
+// Phase-2 node allocation per warp: slots come from the shared counter in
+// chunks of kChunk; the unused tail of a chunk becomes holes (empty range),
+// which the layout skips.  `real` counts the slots actually used.
+struct WarpAlloc {
+    uint32_t next, end, real;
+};
+
+__device__ __forceinline__ void mark_holes(Tree &t, uint32_t a, uint32_t b) {
+    const unsigned lane = threadIdx.x & 31u;
+    if (b > (uint32_t)t.cap) b = (uint32_t)t.cap;
+    for (uint32_t k = a + lane; k < b; k += 32) t.info[k] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// First of cnt consecutive node slots (warp-uniform; all lanes call), or
+// kEmpty when the node array is full.
+__device__ __forceinline__ uint32_t walloc(Tree &t, WarpAlloc &a, uint32_t cnt, uint32_t base,
+                                           uint32_t *err) {
+    if (a.next + cnt > a.end) {
+        mark_holes(t, a.next, a.end);
+        const uint32_t want = cnt > kChunk ? cnt : kChunk;
+        uint32_t g = 0;
+        if ((threadIdx.x & 31u) == 0) g = atomicAdd(&t.meta[kMetaP2Alloc], want);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        a.next = base + g;
+        a.end = a.next + want;
+        if ((uint64_t)a.end > (uint64_t)t.cap) {
+            if ((threadIdx.x & 31u) == 0) set_err(err, kErrNodeCap);
+            a.end = a.next;
+            return kEmpty;
+        }
+    }
+    const uint32_t r = a.next;
+    a.next += cnt;
+    a.real += cnt;
+    return r;
+}
+
+// Phase 2: the whole subtree of queued node R (2..kSmallNode particles) by one
+// warp.  Lane l holds particle start + l and follows the node containing it.
+template <int D>
+__device__ void build_small_subtree(const State &s, const StepParams &p, Tree &t, uint32_t R,
+                                    uint32_t node_base, WarpAlloc &wa, uint32_t *err) {
+    constexpr int Q = 1 << D;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint4 rinf = __ldcg(&t.info[R]);
+    const uint4 rax = __ldcg(&t.aux[R]);
+    const uint32_t st = rinf.z, en = rinf.w;
+    const uint32_t pidx = st + lane;
+    const bool act = pidx < en;
+    float pos[3] = {0.f, 0.f, 0.f}, pm = 0.f;
+    if (act) {
+        pos[0] = s.x[pidx]; pos[1] = s.y[pidx];
+        if (D == 3) pos[2] = s.z[pidx];
+        pm = s.m[pidx];
+    }
+    uint32_t nid = R, na = st, nb = en, lev = rax.x, same_end = rax.y;
+    float4 cell = __ldcg(&t.cell[R]);
+    bool done = !act;
+    uint32_t maxlev = 0;
+    for (int it = 0; __any_sync(0xffffffffu, !done); it++) {
+        if (it > kMaxLevels) { if (lane == 0) set_err(err, kErrDepth); break; }
+        const uint32_t cnt = nb - na;
+        const bool leader = !done && pidx == na;
+        const bool leaf = !done && is_leaf<D>(p, cnt, cell.w);
+        // leaves: sequential sums over the leaf's particles, in particle order
+        if (__any_sync(0xffffffffu, leaf)) {
+            float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+            for (int j = 0; j < 32; j++) {
+                const float xj = __shfl_sync(0xffffffffu, pos[0], j);
+                const float yj = __shfl_sync(0xffffffffu, pos[1], j);
+                const float zj = __shfl_sync(0xffffffffu, pos[2], j);
+                const float mj = __shfl_sync(0xffffffffu, pm, j);
+                const uint32_t pj = st + (uint32_t)j;
+                if (leaf && leader && pj >= na && pj < nb) {
+                    gm = fadd(gm, mj);
+                    c[0] = fadd(c[0], fmul(xj, mj));
+                    c[1] = fadd(c[1], fmul(yj, mj));
+                    if (D == 3) c[2] = fadd(c[2], fmul(zj, mj));
+                }
+            }
+            if (leaf && leader) {
+                if (gm > 0.0f) {
+                    c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+                    if (D == 3) c[2] = fdiv(c[2], gm);
+                }
+                put_walk<D>(t, nid, make_float4(c[0], c[1], c[2], gm), cell.w);
+                finish_upward<D>(t, nid);
+                maxlev = max(maxlev, lev);
+            }
+            done = done || leaf;
+        }
+        // the remaining nodes: predicates of every particle against its node's
+        // midpoint, one ballot per axis, then the searches on those bits
+        const float half = fmul(cell.w, 0.5f);
+        const bool live = !done;
+        const unsigned bx = __ballot_sync(0xffffffffu, live && pos[0] < fadd(cell.x, half));
+        const unsigned by = __ballot_sync(0xffffffffu, live && pos[1] < fadd(cell.y, half));
+        const unsigned bz = D == 3 ? __ballot_sync(0xffffffffu, live && pos[2] < fadd(cell.z, half)) : 0u;
+        uint32_t b[Q + 1];
+        const uint32_t r0 = na - st, len = nb - na;
+        b[0] = na; b[Q] = nb;
+        if (D == 2) {
+            const uint32_t r2 = bits_partition_point(by, r0, len);
+            b[2] = st + r2;
+            b[1] = st + bits_partition_point(bx, r0, r2 - r0);
+            b[3] = st + bits_partition_point(bx, r2, r0 + len - r2);
+        } else {
+            const uint32_t r4 = bits_partition_point(bz, r0, len);
+            const uint32_t r2 = bits_partition_point(by, r0, r4 - r0);
+            const uint32_t r6 = bits_partition_point(by, r4, r0 + len - r4);
+            b[4] = st + r4; b[2] = st + r2; b[6] = st + r6;
+            b[1] = st + bits_partition_point(bx, r0, r2 - r0);
+            b[3] = st + bits_partition_point(bx, r2, r4 - r2);
+            b[5] = st + bits_partition_point(bx, r4, r6 - r4);
+            b[7] = st + bits_partition_point(bx, r6, r0 + len - r6);
+        }
+        uint32_t mask = 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
+        // allocation: node leaders' child counts, one atomic per warp
+        const uint32_t nch = (live && leader) ? (uint32_t)__popc(mask) : 0u;
+        uint32_t incl = nch;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (tot == 0) continue;
+        const uint32_t base = walloc(t, wa, tot, node_base, err);
+        if (base == kEmpty) break;
+        const uint32_t myfirst = base + incl - nch;
+        if (live && leader) {
+            emit_children<D>(t, nid, myfirst, mask, b, cell, half, make_uint4(0, 0, na, nb),
+                             make_uint4(lev, same_end, 0, 0));
+        }
+        // every live lane moves to the child that holds its particle
+        const uint32_t first = __shfl_sync(0xffffffffu, myfirst, (int)((na - st) & 31u));
+        if (live) {
+            unsigned q = 0;
+#pragma unroll
+            for (int qq = 1; qq < Q; qq++) if (pidx >= b[qq]) q = (unsigned)qq;
+            const uint32_t cnb = b[q + 1];
+            nid = first + __popc(mask & ((1u << q) - 1u));
+            cell = child_cell<D>(cell, half, q);
+            same_end = cnb == nb ? same_end + 1u : 0u;
+            na = b[q];
+            nb = cnb;
+            lev++;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
+    if (lane == 0) atomicMax(&t.meta[kMetaLevels], maxlev + 1u);
+}
+
+// Phase 2, fast form: the subtree of queued node R is built in shared memory
+// (nodes, cells, masses), then allocated with one atomic and written out.
+// Lane l holds particle start + l; sm.p keeps them for the leaf sums.  Returns
+// false, with nothing written, when the subtree has more than kSubMax nodes
+// (long single-child chains of nearly coincident particles); the caller then
+// builds it with build_small_subtree.
+constexpr int kSubMax = 64;
+
+struct SubTreeSmem {
+    float4 p[32];            // particles {x, y, z, m}
+    float4 cell[kSubMax];
+    float4 cm[kSubMax];      // {com.x, com.y, com.z, mass}
+    uint4 node[kSubMax];     // {a | b << 8 | mask << 16, first child, parent, level | same_end << 16}
+    uint32_t lvl[kSubMax + 1];
+};
+
+template <int D>
+__device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tree &t,
+                                         uint32_t R, uint32_t node_base, SubTreeSmem &sm,
+                                         WarpAlloc &wa, uint32_t *err) {
+    constexpr int Q = 1 << D;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint4 rinf = __ldcg(&t.info[R]);
+    const uint4 rax = __ldcg(&t.aux[R]);
+    const float4 rcell = __ldcg(&t.cell[R]);
+    const uint32_t st = rinf.z, cnt = rinf.w - rinf.z;
+    const bool act = lane < cnt;
+    float pos[3] = {0.f, 0.f, 0.f};
+    if (act) {
+        pos[0] = s.x[st + lane]; pos[1] = s.y[st + lane];
+        if (D == 3) pos[2] = s.z[st + lane];
+        sm.p[lane] = make_float4(pos[0], pos[1], pos[2], s.m[st + lane]);
+    }
+    if (lane == 0) {
+        sm.cell[0] = rcell;
+        sm.node[0] = make_uint4(cnt << 8, 0u, kEmpty, rax.x | (rax.y << 16));
+        sm.cm[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        sm.lvl[0] = 0;
+        sm.lvl[1] = 1;
+    }
+    __syncwarp();
+    uint32_t loc = 0, na = 0, nb = cnt, lev = rax.x, se = rax.y, count = 1;
+    int nlv = 1;   // local levels made so far
+    float4 cell = rcell;
+    bool done = !act;
+    uint32_t maxlev = 0;
+    for (int it = 0; __any_sync(0xffffffffu, !done); it++) {
+        if (it > kMaxLevels) { if (lane == 0) set_err(err, kErrDepth); return true; }
+        const bool leader = !done && lane == na;
+        const bool leaf = !done && is_leaf<D>(p, nb - na, cell.w);
+        if (leaf && leader) {
+            // computeLeafMass: sequential sums in particle order
+            float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+            for (uint32_t j = na; j < nb; j++) {
+                const float4 q = sm.p[j];
+                gm = fadd(gm, q.w);
+                c[0] = fadd(c[0], fmul(q.x, q.w));
+                c[1] = fadd(c[1], fmul(q.y, q.w));
+                if (D == 3) c[2] = fadd(c[2], fmul(q.z, q.w));
+            }
+            if (gm > 0.0f) {
+                c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+                if (D == 3) c[2] = fdiv(c[2], gm);
+            }
+            sm.cm[loc] = make_float4(c[0], c[1], c[2], gm);
+            maxlev = max(maxlev, lev);
+        }
+        done = done || leaf;
+        const float half = fmul(cell.w, 0.5f);
+        const bool live = !done;
+        const unsigned bx = __ballot_sync(0xffffffffu, live && pos[0] < fadd(cell.x, half));
+        const unsigned by = __ballot_sync(0xffffffffu, live && pos[1] < fadd(cell.y, half));
+        const unsigned bz = D == 3 ? __ballot_sync(0xffffffffu, live && pos[2] < fadd(cell.z, half)) : 0u;
+        uint32_t b[Q + 1];
+        const uint32_t len = nb - na;
+        b[0] = na; b[Q] = nb;
+        if (D == 2) {
+            b[2] = bits_partition_point(by, na, len);
+            b[1] = bits_partition_point(bx, na, b[2] - na);
+            b[3] = bits_partition_point(bx, b[2], nb - b[2]);
+        } else {
+            b[4] = bits_partition_point(bz, na, len);
+            b[2] = bits_partition_point(by, na, b[4] - na);
+            b[6] = bits_partition_point(by, b[4], nb - b[4]);
+            b[1] = bits_partition_point(bx, na, b[2] - na);
+            b[3] = bits_partition_point(bx, b[2], b[4] - b[2]);
+            b[5] = bits_partition_point(bx, b[4], b[6] - b[4]);
+            b[7] = bits_partition_point(bx, b[6], nb - b[6]);
+        }
+        uint32_t mask = 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
+        const uint32_t nch = (live && leader) ? (uint32_t)__popc(mask) : 0u;
+        uint32_t incl = nch;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (tot == 0) break;
+        if (count + tot > (uint32_t)kSubMax || nlv + 1 > kSubMax) return false;
+        const uint32_t myfirst = count + incl - nch;
+        if (live && leader) {
+            uint4 nd = sm.node[loc];
+            nd.x |= mask << 16;
+            nd.y = myfirst;
+            sm.node[loc] = nd;
+            uint32_t ci = myfirst;
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                if (!((mask >> q) & 1u)) continue;
+                sm.cell[ci] = child_cell<D>(cell, half, (unsigned)q);
+                const uint32_t cse = b[q + 1] == nb ? se + 1u : 0u;
+                sm.node[ci] = make_uint4(b[q] | (b[q + 1] << 8), 0u, loc, (lev + 1u) | (cse << 16));
+                sm.cm[ci] = make_float4(0.f, 0.f, 0.f, 0.f);
+                ci++;
+            }
+        }
+        count += tot;
+        nlv++;
+        if (lane == 0) sm.lvl[nlv] = count;
+        __syncwarp();
+        const uint32_t first = __shfl_sync(0xffffffffu, myfirst, (int)(na & 31u));
+        if (live) {
+            unsigned q = 0;
+#pragma unroll
+            for (int qq = 1; qq < Q; qq++) if (lane >= b[qq]) q = (unsigned)qq;
+            const uint32_t cnb = b[q + 1];
+            loc = first + __popc(mask & ((1u << q) - 1u));
+            cell = child_cell<D>(cell, half, q);
+            se = cnb == nb ? se + 1u : 0u;
+            na = b[q];
+            nb = cnb;
+            lev++;
+        }
+    }
+    __syncwarp();
+    // computeInternalMass, deepest local level first, children in x-major order
+    for (int L = nlv - 1; L >= 0; --L) {
+        const uint32_t j = sm.lvl[L] + lane;
+        if (j < sm.lvl[L + 1]) {
+            const uint4 nd = sm.node[j];
+            const uint32_t mask = nd.x >> 16;
+            if (mask) {
                 float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
-                for (uint32_t i = st; i < en; i++) {
-                    const float mi = s.m[i];
-                    gm = fadd(gm, mi);
-                    c[0] = fadd(c[0], fmul(s.x[i], mi));
-                    c[1] = fadd(c[1], fmul(s.y[i], mi));
-                    if (D == 3) c[2] = fadd(c[2], fmul(s.z[i], mi));
+#pragma unroll
+                for (int kk = 0; kk < Q; kk++) {
+                    unsigned q;
+                    if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
+                    else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
+                    if (!((mask >> q) & 1u)) continue;
+                    const float4 cw = sm.cm[nd.y + __popc(mask & ((1u << q) - 1u))];
+                    gm = fadd(gm, cw.w);
+                    c[0] = fadd(c[0], fmul(cw.x, cw.w));
+                    c[1] = fadd(c[1], fmul(cw.y, cw.w));
+                    if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cw.w));
                 }
                 if (gm > 0.0f) {
                     c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
                     if (D == 3) c[2] = fdiv(c[2], gm);
                 }
-                const float s2 = fmul(cell.w, cell.w);
-                if (D == 2) t.walk[k] = make_float4(c[0], c[1], gm, s2);
-                else { t.walk[k] = make_float4(c[0], c[1], c[2], gm); t.size2[k] = s2; }
+                sm.cm[j] = make_float4(c[0], c[1], c[2], gm);
             }
-            const uint32_t nch = (uint32_t)__popc(mask);
-            if (lane == 0) s_cnt[warp] = valid ? nch : 0u;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t tot = 0;
-                for (int w = 0; w < kBuildWarps; w++) { s_off[w] = tot; tot += s_cnt[w]; }
-                s_base = tot ? atomicAdd(&t.lvl_alloc[L], tot) : 0u;
+        }
+        __syncwarp();
+    }
+    // allocate and write out: local node 0 is R itself
+    const uint32_t base = walloc(t, wa, count - 1u, node_base, err);
+    if (base == kEmpty) return true;
+    for (uint32_t j = lane; j < count; j += 32) {
+        const uint4 nd = sm.node[j];
+        const uint32_t a = nd.x & 0xFFu, bb = (nd.x >> 8) & 0xFFu, mask = nd.x >> 16;
+        const uint32_t gid = j == 0 ? R : base + j - 1u;
+        const uint32_t gfirst = mask ? base + nd.y - 1u : 0u;
+        t.info[gid] = make_uint4(gfirst, mask, st + a, st + bb);
+        const float4 cl = sm.cell[j];
+        if (j > 0) {
+            t.cell[gid] = cl;
+            const uint32_t gpar = nd.z == 0 ? R : base + nd.z - 1u;
+            t.aux[gid] = make_uint4(nd.w & 0xFFFFu, nd.w >> 16, gpar, 0u);
+        }
+        put_walk<D>(t, gid, sm.cm[j], cl.w);
+    }
+    for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
+    __syncwarp();
+    if (lane == 0) {
+        atomicMax(&t.meta[kMetaLevels], maxlev + 1u);
+        finish_upward<D>(t, R);
+    }
+    return true;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBuildThreads)
+k_build(State s, StepParams p, Tree t, uint32_t *err) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nthreads = gridDim.x * blockDim.x;
+    const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
+    const uint32_t n = (uint32_t)p.n;
+    uint32_t *bar_count = t.meta + kMetaBarCount, *bar_gen = t.meta + kMetaBarGen;
+
+    // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
+    uint32_t lb = 0, le = 1;
+    int L = 0;
+    if (gtid == 0) {
+        t.level[0] = 0;
+        t.aux[0] = make_uint4(0u, 0u, kEmpty, 0u);
+    }
+    grid_barrier(bar_count, bar_gen, err);
+    if (gtid == 0) stamp(t);
+    while (true) {
+        if (le - lb <= nwarps) {
+            for (uint32_t k = lb + gwarp; k < le; k += nwarps)
+                split_level_node<D, 32>(s, p, t, k, true, le, &t.lvl_alloc[L], err);
+        } else {
+            for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
+                const uint32_t k = kb + (lane >> 3);
+                split_level_node<D, 8>(s, p, t, k, k < le, le, &t.lvl_alloc[L], err);
             }
-            __syncthreads();
-            if (valid && nch) {
-                const uint32_t first = le + s_base + s_off[warp];
-                if ((uint64_t)first + nch > cap) {
-                    if (lane == 0) set_err(err, kErrNodeCap);
-                } else {
-                    if (lane < (unsigned)Q && ((mask >> lane) & 1u)) {
-                        const unsigned q = lane;
-                        const uint32_t ci = first + __popc(mask & ((1u << q) - 1u));
-                        float4 cc;
-                        cc.x = fadd(cell.x, (q & 1u) ? half : 0.0f);
-                        cc.y = fadd(cell.y, (q & 2u) ? half : 0.0f);
-                        cc.z = D == 3 ? fadd(cell.z, (q & 4u) ? half : 0.0f) : 0.0f;
-                        cc.w = half;
-                        t.cell[ci] = cc;
-                        t.info[ci] = make_uint4(0u, 0u, bnd[q], bnd[q + 1]);
-                    }
-                    if (lane == 0) t.info[k] = make_uint4(first, mask, st, en);
-                }
-            }
-            __syncthreads();
         }
         grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
         const uint32_t cnt = *(volatile uint32_t *)&t.lvl_alloc[L];
         const uint32_t e = *(volatile uint32_t *)err;
         if (cnt == 0 || (e & (kErrNodeCap | kErrSpin))) break;
@@ -226,71 +732,172 @@ k_build(State s, StepParams p, Tree t, uint32_t *err) {
         L++;
         if (gtid == 0) t.level[L] = lb;
     }
-    const int nlev = L + 1;
     if (gtid == 0) {
-        t.level[nlev] = le;
-        t.meta[0] = le;
-        t.meta[1] = (uint32_t)nlev;
+        t.level[L + 1] = le;
+        atomicMax(&t.meta[kMetaLevels], (uint32_t)(L + 1));
     }
-    // bottom-up: computeInternalMass[3D] with children read in subGrids[x][y]([z])
-    // order, x outermost
-    for (int lev = nlev - 2; lev >= 0; --lev) {
-        const uint32_t a = __ldcg(&t.level[lev]), b = __ldcg(&t.level[lev + 1]);
-        for (uint32_t k = a + gtid; k < b; k += gridDim.x * blockDim.x) {
-            const uint4 inf = __ldcg(&t.info[k]);
-            const uint32_t mask = inf.y;
-            if (!mask) continue;
-            float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-            for (int kk = 0; kk < Q; kk++) {
-                unsigned q;
-                if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
-                else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
-                if (!((mask >> q) & 1u)) continue;
-                const uint32_t ci = inf.x + __popc(mask & ((1u << q) - 1u));
-                const float4 cw = __ldcg(&t.walk[ci]);
-                const float cm = D == 2 ? cw.z : cw.w;
-                gm = fadd(gm, cm);
-                c[0] = fadd(c[0], fmul(cw.x, cm));
-                c[1] = fadd(c[1], fmul(cw.y, cm));
-                if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cm));
-            }
-            if (gm > 0.0f) {
-                c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
-                if (D == 3) c[2] = fdiv(c[2], gm);
-            }
-            const float size = __ldcg(&t.cell[k]).w;
-            const float s2 = fmul(size, size);
-            if (D == 2) t.walk[k] = make_float4(c[0], c[1], gm, s2);
-            else { t.walk[k] = make_float4(c[0], c[1], c[2], gm); t.size2[k] = s2; }
+    if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
+
+    // ---- phase 2: queued small subtrees, one warp each, no barriers --------
+    const uint32_t nsmall = *(volatile uint32_t *)&t.meta[kMetaSmall];
+    {
+        __shared__ SubTreeSmem s_sub[kBuildThreads / 32];
+        SubTreeSmem &sm = s_sub[threadIdx.x >> 5];
+        WarpAlloc wa{0u, 0u, 0u};
+        for (uint32_t task = gwarp; task < nsmall; task += nwarps) {
+            const uint32_t R = __ldcg(&t.small[task]);
+            if (!build_small_subtree_smem<D>(s, p, t, R, le, sm, wa, err))
+                build_small_subtree<D>(s, p, t, R, le, wa, err);
+            __syncwarp();
         }
+        mark_holes(t, wa.next, wa.end);
+        if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
+    }
+    grid_barrier(bar_count, bar_gen, err);
+    if (gtid == 0) stamp(t);
+    // slots in use (phase-2 holes included) and real nodes (the walk's extent)
+    uint32_t slots = le + *(volatile uint32_t *)&t.meta[kMetaP2Alloc];
+    if (slots > (uint32_t)t.cap) slots = (uint32_t)t.cap;
+    const uint32_t nodes = le + *(volatile uint32_t *)&t.meta[kMetaReal];
+    if (gtid == 0) {
+        t.meta[kMetaNodes] = nodes;
+        t.meta[kMetaSlots] = slots;
+    }
+    if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
+
+    // ---- phase 3: depth-first walk layout ------------------------------------
+    // histogram of range ends (endcnt was zeroed before the launch); holes have
+    // an empty range ending at 0 and are skipped
+    for (uint32_t k = gtid; k < slots; k += nthreads) {
+        const uint32_t e = __ldcg(&t.info[k]).w;
+        if (e) atomicAdd(&t.endcnt[e], 1u);
+    }
+    grid_barrier(bar_count, bar_gen, err);
+    if (gtid == 0) stamp(t);
+    // inclusive scan of endcnt[0..n] in place: block chunks, then block offsets
+    {
+        constexpr int W = kBuildThreads / 32;
+        __shared__ uint32_t s_w[W];
+        const uint32_t total = n + 1;
+        const uint32_t chunk = (total + gridDim.x - 1) / gridDim.x;
+        const uint32_t c0 = min(blockIdx.x * chunk, total);
+        const uint32_t c1 = min(c0 + chunk, total);
+        uint32_t carry = 0;
+        for (uint32_t base = c0; base < c1; base += blockDim.x) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t v = i < c1 ? __ldcg(&t.endcnt[i]) : 0u;
+            uint32_t incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (unsigned)o) incl += u;
+            }
+            if (lane == 31) s_w[threadIdx.x >> 5] = incl;
+            __syncthreads();
+            uint32_t wpre = 0, btot = 0;
+            for (int w = 0; w < W; w++) {
+                if (w < (int)(threadIdx.x >> 5)) wpre += s_w[w];
+                btot += s_w[w];
+            }
+            if (i < c1) t.endcnt[i] = carry + wpre + incl;
+            carry += btot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) t.blocksum[blockIdx.x] = carry;
         grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
+        uint32_t off = 0;
+        for (uint32_t b2 = threadIdx.x; b2 < blockIdx.x; b2 += blockDim.x)
+            off += __ldcg(&t.blocksum[b2]);
+        for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+        if (lane == 0) s_w[threadIdx.x >> 5] = off;
+        __syncthreads();
+        off = 0;
+        for (int w = 0; w < W; w++) off += s_w[w];
+        for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) t.endcnt[i] += off;
+        grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
+    }
+    // scatter nodes (and the particles of leaves) into the walk layout:
+    // pre(k) = C(start) + level, subtree successor = C(end) + level - same_end
+    for (uint32_t k = gtid; k < slots; k += nthreads) {
+        const uint4 inf = __ldcg(&t.info[k]);
+        if (inf.w == 0u) continue;   // hole
+        const uint4 ax = __ldcg(&t.aux[k]);
+        const float4 w = __ldcg(&t.walk[k]);
+        const uint32_t me = n + __ldcg(&t.endcnt[inf.z]) + ax.x;
+        const uint32_t skip = n + __ldcg(&t.endcnt[inf.w]) + ax.x - ax.y;
+        const uint32_t down = inf.y ? me + 1 : inf.z;
+        if (me >= n + nodes || skip > n + nodes) {   // cannot happen for a consistent tree
+            set_err(err, kErrDepth);
+            continue;
+        }
+        const float nm = D == 2 ? w.z : w.w;
+        if (nm <= 0.0f) {
+            // gridMass <= 0: the reference skips the whole subtree.  As a source
+            // it is accepted by every test (size^2 = -1), carries no mass (the
+            // walk makes no interaction with a massless source) and leads to
+            // its successor either way.
+            t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -1.0f) : make_float4(w.x, w.y, w.z, 0.0f);
+            if (D == 2) ((uint2 *)t.link)[me] = make_uint2(skip, skip);
+            else ((uint4 *)t.link)[me] = make_uint4(skip, skip, __float_as_uint(-1.0f), 0u);
+            continue;
+        }
+        t.src[me] = w;
+        if (D == 2) ((uint2 *)t.link)[me] = make_uint2(skip, down);
+        else ((uint4 *)t.link)[me] = make_uint4(skip, down, __float_as_uint(__ldcg(&t.size2[k])), 0u);
+        if (!inf.y) {
+            for (uint32_t j = inf.z; j < inf.w; j++) {
+                const uint32_t nx = j + 1 < inf.w ? j + 1 : skip;
+                if (D == 2) {
+                    t.src[j] = make_float4(s.x[j], s.y[j], s.m[j], -1.0f);
+                    ((uint2 *)t.link)[j] = make_uint2(nx, nx);
+                } else {
+                    t.src[j] = make_float4(s.x[j], s.y[j], s.z[j], s.m[j]);
+                    ((uint4 *)t.link)[j] = make_uint4(nx, nx, __float_as_uint(-1.0f), 0u);
+                }
+            }
+        }
     }
 }
 
 static int g_build_blocks[2] = {0, 0};
 
+int build_grid_blocks(int dims, int num_sms);
+
+// Node slots the build may leave unused: each warp's last phase-2 chunk.
+int64_t build_node_slack(int dims, int num_sms) {
+    return (int64_t)build_grid_blocks(dims, num_sms) * (kBuildThreads / 32) * kChunk;
+}
+
+int build_grid_blocks(int dims, int num_sms) {
+    const int di = dims == 2 ? 0 : 1;
+    if (g_build_blocks[di] == 0) {
+        int per_sm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
+            kBuildThreads, 0);
+        if (e != cudaSuccess || per_sm < 1) return 0;
+        // at most two blocks per SM: every block joins every grid barrier, so
+        // fewer, larger blocks make the barriers cheaper
+        g_build_blocks[di] = (per_sm < 2 ? per_sm : 2) * num_sms;
+    }
+    return g_build_blocks[di];
+}
+
 cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
                          int num_sms, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(t.lvl_alloc, 0, sizeof(uint32_t) * (kMaxLevels + 2), st);
     if (e != cudaSuccess) return e;
-    const int di = dims == 2 ? 0 : 1;
-    if (g_build_blocks[di] == 0) {
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
-            kBuildThreads, 0);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-        g_build_blocks[di] = per_sm * num_sms;
-    }
-    int blocks = g_build_blocks[di];
-    // every block takes part in each grid barrier: more blocks than the widest
-    // level needs only lengthen the barriers
-    int want = (p.n + 31) / 32;
-    if (want > num_sms * 4) want = num_sms * 4;
-    if (want < 1) want = 1;
-    if (blocks > want) blocks = want;
+    e = cudaMemsetAsync(t.endcnt, 0, sizeof(uint32_t) * ((size_t)p.n + 1), st);
+    if (e != cudaSuccess) return e;
+    // node count, level count, small-queue length, phase-2 allocation
+    e = cudaMemsetAsync(t.meta + kMetaNodes, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    // small-queue length, phase-2 slots, timeline count, real phase-2 nodes, slots
+    e = cudaMemsetAsync(t.meta + kMetaSmall, 0, 5 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const int blocks = build_grid_blocks(dims, num_sms);
+    if (blocks < 1) return cudaErrorLaunchOutOfResources;
     State sc = s;
     StepParams pc = p;
     Tree tc = t;

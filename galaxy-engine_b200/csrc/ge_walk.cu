@@ -7,16 +7,22 @@
 // a monopole when size^2 < theta^2 * r2; otherwise a leaf is summed directly
 // over its particles j != i; otherwise the walk descends.  acc_i = F_i / m_i.
 //
-// Warp-cooperative form: the 32 particles of a warp are consecutive in Morton
-// order and share one depth-first traversal stack in shared memory whose
-// entries carry the mask of lanes that still have to examine the node.  Every
-// lane applies the reference's own opening test (computed with the reference's
-// rounding, no contraction), so each particle's interaction set is exactly the
-// reference's; children are pushed in reverse slot order, so each lane also
-// meets its nodes in the reference's pre-order and accumulates in that order.
+// Here every particle walks the depth-first layout built with the tree
+// (ge_internal.h) with no stack: each step loads one source and its two
+// successor links, evaluates the reference's opening test with the
+// reference's rounding (so the interaction set is exactly the reference's),
+// interacts if accepted and follows `skip` or `descend`.  A leaf's particles
+// are sources of their own with size^2 = -1, which every test accepts, so the
+// direct sum over a leaf is the same loop body (the self term j == i is
+// skipped as in the reference); a node of zero mass is laid out as an accepted
+// source without mass, so its subtree is skipped as in the reference.
+// Sources are met in the reference's pre-order, so each particle accumulates
+// in the reference's order.
 //   GE_PREC_EXACT : every interaction with the reference's rounding
-//                   (1/sqrtf, three products, no FMA): bit-identical results.
-//   GE_PREC_FAST  : rsqrt and FMA for the force terms, G applied once.
+//                   (1/sqrtf, products in the reference's order, no FMA):
+//                   bit-identical accelerations.
+//   GE_PREC_FAST  : approximate reciprocal square root (MUFU, flush-to-zero)
+//                   and FMA for the force terms, G applied once.
 // integrateEnd (physics.cpp:1114-1125) is fused into the epilogue.
 #include "ge_bh.h"
 #include "ge_device.cuh"
@@ -24,11 +30,7 @@
 
 namespace ge {
 
-constexpr int kWalkThreads = 128;
-constexpr int kWalkWarps = kWalkThreads / 32;
-
-template <int D>
-struct WalkStack { static constexpr int size = D == 2 ? 512 : 1024; };
+constexpr int kWalkThreads = 256;
 
 __device__ __forceinline__ float wrap_d(float d, float dom, float hd) {
     // d -= domain * ((d > half) - (d < -half))   (physics.cpp:118-121)
@@ -36,173 +38,122 @@ __device__ __forceinline__ float wrap_d(float d, float dom, float hd) {
     return fsub(d, fmul(dom, (float)k));
 }
 
-template <int D, int MODE, bool COUNT>
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// size^2 of a source: in the float4 for 2D, in the link for 3D
+__device__ __forceinline__ float link_s2(const uint2 &, float in_src) { return in_src; }
+__device__ __forceinline__ float link_s2(const uint4 &l, float) { return __uint_as_float(l.z); }
+
+template <int D> struct LinkOf;
+template <> struct LinkOf<2> { using T = uint2; };
+template <> struct LinkOf<3> { using T = uint4; };
+
+template <int D, int MODE, bool COUNT, bool PER>
 __global__ void __launch_bounds__(kWalkThreads)
 k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
-    constexpr int SS = WalkStack<D>::size;
-    __shared__ uint2 stk_all[kWalkWarps][SS];
-    const int warp = threadIdx.x >> 5;
-    const unsigned lane = threadIdx.x & 31u;
-    uint2 *stk = stk_all[warp];
+    using LT = typename LinkOf<D>::T;
+    const LT *__restrict__ link = (const LT *)t.link;
+    const float4 *__restrict__ src = t.src;
     const int n = p.n;
+    const uint32_t end = (uint32_t)n + __ldg(&t.meta[0]);
+    const uint32_t limit = end + 1;   // every source is met at most once
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
-
-    for (int gw = blockIdx.x * kWalkWarps + warp; gw * 32 < n; gw += gridDim.x * kWalkWarps) {
-        const int i = gw * 32 + (int)lane;
-        const bool active = i < n;
-        float pi[3] = {0.f, 0.f, 0.f};
-        float mi = 1.0f;
-        if (active) {
-            pi[0] = s.x[i]; pi[1] = s.y[i];
-            if (D == 3) pi[2] = s.z[i];
-            mi = s.m[i];
-        }
-        const float gm_i = MODE == GE_PREC_EXACT ? fmul(G, mi) : 0.0f;   // Gf * pmass
+    if (i < n) {
+        float pi[3];
+        pi[0] = s.x[i]; pi[1] = s.y[i];
+        pi[2] = D == 3 ? s.z[i] : 0.0f;
+        const float mi = s.m[i];
+        const float gm_i = fmul(G, mi);   // Gf * pmass (exact mode)
         float f[3] = {0.f, 0.f, 0.f};
-        uint32_t cnt = 0;
-        int sp = 1;
-        const unsigned amask = __ballot_sync(0xffffffffu, active);
-        if (lane == 0) stk[0] = make_uint2(0u, amask);
-        __syncwarp();
-        while (sp > 0) {
-            --sp;
-            const uint2 e = stk[sp];
-            __syncwarp();
-            const uint32_t node = e.x;
-            const bool mine = (e.y >> lane) & 1u;
-            const float4 A = __ldg(&t.walk[node]);
-            const float nm = D == 2 ? A.z : A.w;
-            if (nm <= 0.0f) continue;   // gridMass <= 0: skip the subtree
-            const uint4 B = __ldg(&t.info[node]);
-            const float s2 = D == 2 ? A.w : __ldg(&t.size2[node]);
+        uint32_t k = (uint32_t)n, steps = 0, cnt = 0;
+        while (k < end) {
+            if (++steps > limit) { set_err(err, kErrStack); break; }
+            const float4 A = __ldg(&src[k]);
+            const LT L = __ldg(&link[k]);
+            const float m = D == 2 ? A.z : A.w;
+            const float s2 = link_s2(L, A.w);
             float d[3];
             d[0] = fsub(A.x, pi[0]);
             d[1] = fsub(A.y, pi[1]);
-            if (D == 3) d[2] = fsub(A.z, pi[2]);
-            if (p.periodic) {
+            d[2] = D == 3 ? fsub(A.z, pi[2]) : 0.0f;
+            if (PER) {
 #pragma unroll
                 for (int a = 0; a < D; a++) d[a] = wrap_d(d[a], p.domain[a], p.half_domain[a]);
             }
             float r2 = fadd(fmul(d[0], d[0]), fmul(d[1], d[1]));
             if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
             r2 = fadd(r2, eps2);
-            const bool accept = mine && (s2 < fmul(th2, r2));
-            if (accept) {
+            const bool acc = s2 < fmul(th2, r2);
+            if (acc && m != 0.0f && k != (uint32_t)i) {
                 if (MODE == GE_PREC_EXACT) {
                     const float inv = fdiv(1.0f, __fsqrt_rn(r2));
                     const float inv3 = fmul(fmul(inv, inv), inv);
-                    const float fm = fmul(fmul(gm_i, nm), inv3);
+                    const float fm = fmul(fmul(gm_i, m), inv3);
 #pragma unroll
                     for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(d[a], fm));
                 } else {
-                    const float inv = rsqrtf(r2);
-                    const float fm = nm * (inv * inv * inv);
+                    const float inv = rsqrt_approx(r2);
+                    const float fm = m * (inv * inv * inv);
 #pragma unroll
                     for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
                 }
                 if (COUNT) cnt++;
             }
-            const unsigned open = __ballot_sync(0xffffffffu, mine && !accept);
-            if (!open) continue;
-            if (B.y == 0u) {
-                // leaf: direct sum over its particles, j != i
-                const bool me = (open >> lane) & 1u;
-                for (uint32_t j = B.z; j < B.w; j++) {
-                    float pj[3];
-                    pj[0] = __ldg(&s.x[j]); pj[1] = __ldg(&s.y[j]);
-                    if (D == 3) pj[2] = __ldg(&s.z[j]);
-                    const float mj = __ldg(&s.m[j]);
-                    if (me && (int)j != i) {
-                        float q[3];
-#pragma unroll
-                        for (int a = 0; a < D; a++) q[a] = fsub(pj[a], pi[a]);
-                        if (p.periodic) {
-#pragma unroll
-                            for (int a = 0; a < D; a++)
-                                q[a] = wrap_d(q[a], p.domain[a], p.half_domain[a]);
-                        }
-                        float rr = fadd(fmul(q[0], q[0]), fmul(q[1], q[1]));
-                        if (D == 3) rr = fadd(rr, fmul(q[2], q[2]));
-                        rr = fadd(rr, eps2);
-                        if (MODE == GE_PREC_EXACT) {
-                            const float inv = fdiv(1.0f, __fsqrt_rn(rr));
-                            const float inv3 = fmul(fmul(inv, inv), inv);
-                            const float fm = fmul(fmul(gm_i, mj), inv3);
-#pragma unroll
-                            for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(q[a], fm));
-                        } else {
-                            const float inv = rsqrtf(rr);
-                            const float fm = mj * (inv * inv * inv);
-#pragma unroll
-                            for (int a = 0; a < D; a++) f[a] = fmaf(q[a], fm, f[a]);
-                        }
-                        if (COUNT) cnt++;
-                    }
-                }
-            } else {
-                // descend: push the children in reverse slot order (first child on top)
-                const int nc = __popc(B.y);
-                if (sp + nc > SS) {
-                    if (lane == 0) set_err(err, kErrStack);
-                    break;
-                }
-                if ((int)lane < nc) stk[sp + nc - 1 - (int)lane] = make_uint2(B.x + lane, open);
-                sp += nc;
-                __syncwarp();
-            }
+            k = acc ? L.x : L.y;
         }
-        if (active) {
-            float acc[3];
+        float a3[3];
 #pragma unroll
-            for (int a = 0; a < D; a++)
-                acc[a] = MODE == GE_PREC_EXACT ? fdiv(f[a], mi) : G * f[a];
-            s.ax[i] = acc[0]; s.ay[i] = acc[1];
-            if (D == 3) s.az[i] = acc[2];
-            if (integrate_end && !(s.pinned && s.pinned[i])) {
-                s.vx[i] = fadd(s.vx[i], fmul(acc[0], p.half_dt));
-                s.vy[i] = fadd(s.vy[i], fmul(acc[1], p.half_dt));
-                if (D == 3) s.vz[i] = fadd(s.vz[i], fmul(acc[2], p.half_dt));
-            }
+        for (int a = 0; a < D; a++) a3[a] = MODE == GE_PREC_EXACT ? fdiv(f[a], mi) : G * f[a];
+        s.ax[i] = a3[0]; s.ay[i] = a3[1];
+        if (D == 3) s.az[i] = a3[2];
+        if (integrate_end && !(s.pinned && s.pinned[i])) {
+            s.vx[i] = fadd(s.vx[i], fmul(a3[0], p.half_dt));
+            s.vy[i] = fadd(s.vy[i], fmul(a3[1], p.half_dt));
+            if (D == 3) s.vz[i] = fadd(s.vz[i], fmul(a3[2], p.half_dt));
         }
-        if (COUNT) my_count += cnt;
-        __syncwarp();
+        my_count = cnt;
     }
     if (COUNT) {
         for (int o = 16; o > 0; o >>= 1) my_count += __shfl_xor_sync(0xffffffffu, my_count, o);
-        if (lane == 0 && my_count) atomicAdd(inter, my_count);
+        if ((threadIdx.x & 31) == 0 && my_count) atomicAdd(inter, my_count);
     }
 }
 
-template <int D, int MODE, bool COUNT>
+template <int D, int MODE, bool COUNT, bool PER>
 static cudaError_t walk_one(const State &s, const StepParams &p, const Tree &t, int ie,
                             unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    int warps = (p.n + 31) / 32;
-    int blocks = (warps + kWalkWarps - 1) / kWalkWarps;
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    if (blocks < 1) blocks = 1;
-    k_walk<D, MODE, COUNT><<<blocks, kWalkThreads, 0, st>>>(s, p, t, ie, inter, err);
+    const int blocks = (p.n + kWalkThreads - 1) / kWalkThreads;
+    k_walk<D, MODE, COUNT, PER><<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, t, ie, inter, err);
     return cudaGetLastError();
+}
+
+template <int D, int MODE>
+static cudaError_t walk_mode(const State &s, const StepParams &p, const Tree &t, int ie,
+                             unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if (p.periodic)
+        return inter ? walk_one<D, MODE, true, true>(s, p, t, ie, inter, err, st)
+                     : walk_one<D, MODE, false, true>(s, p, t, ie, nullptr, err, st);
+    return inter ? walk_one<D, MODE, true, false>(s, p, t, ie, inter, err, st)
+                 : walk_one<D, MODE, false, false>(s, p, t, ie, nullptr, err, st);
 }
 
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
                         const Tree &t, bool integrate_end, unsigned long long *inter_count,
                         uint32_t *err, cudaStream_t st) {
     const int ie = integrate_end ? 1 : 0;
-    const bool cnt = inter_count != nullptr;
     const bool exact = precision == GE_PREC_EXACT;
-#define GE_WALK(Dv, Mv)                                                                   \
-    return cnt ? walk_one<Dv, Mv, true>(s, p, t, ie, inter_count, err, st)                \
-               : walk_one<Dv, Mv, false>(s, p, t, ie, nullptr, err, st)
-    if (dims == 2) {
-        if (exact) GE_WALK(2, GE_PREC_EXACT);
-        GE_WALK(2, GE_PREC_FAST);
-    } else {
-        if (exact) GE_WALK(3, GE_PREC_EXACT);
-        GE_WALK(3, GE_PREC_FAST);
-    }
-#undef GE_WALK
+    if (dims == 2)
+        return exact ? walk_mode<2, GE_PREC_EXACT>(s, p, t, ie, inter_count, err, st)
+                     : walk_mode<2, GE_PREC_FAST>(s, p, t, ie, inter_count, err, st);
+    return exact ? walk_mode<3, GE_PREC_EXACT>(s, p, t, ie, inter_count, err, st)
+                 : walk_mode<3, GE_PREC_FAST>(s, p, t, ie, inter_count, err, st);
 }
 
 }  // namespace ge

@@ -164,6 +164,11 @@ int ge_direct_sum_f64(ge_ctx *ctx, int64_t nt, const uint32_t *idx, double *ax, 
                       double *az);
 /* FP64 sums over the state: out = {kinetic energy, p_x, p_y, p_z, total mass} */
 int ge_sums_f64(ge_ctx *ctx, double *out);
+/* Timeline of the last tree build: device time (ns, from the first entry) at
+   each of its grid-wide barriers, in order (one per level of the large-node
+   phase, then the subtree phase, then the three layout steps).  Profiling aid
+   with no counterpart in the reference. */
+int ge_build_timeline(ge_ctx *ctx, int32_t cap, uint64_t *ns, int32_t *count);
 
 /* --- 2D Morton sort without device allocation --------------------------
  * No counterpart in the reference: an addition for callers that cannot
