@@ -179,16 +179,17 @@ int ensure_capacity(ge_ctx *c, int64_t n) {
     const int bblocks = build_grid_blocks(D, c->num_sms);
     if (bblocks < 1) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
     GE_CHECK(c, dalloc(c, &t.blocksum, (size_t)bblocks));
-    GE_CHECK(c, dalloc(c, &t.src, N + (size_t)node_cap));
+    GE_CHECK(c, dalloc(c, &t.src, N + (size_t)node_cap + 1));
     if (D == 2) {
-        uint2 *l = nullptr;
-        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap));
+        uint32_t *l = nullptr;
+        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap + 1));
         t.link = l;
     } else {
-        uint4 *l = nullptr;
-        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap));
+        uint2 *l = nullptr;
+        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap + 1));
         t.link = l;
     }
+    GE_CHECK(c, dalloc(c, &t.slot_of, N));
     GE_CHECK(c, dalloc(c, &t.level, kMaxLevels + 2));
     GE_CHECK(c, dalloc(c, &t.lvl_alloc, kMaxLevels + 2));
     GE_CHECK(c, dalloc(c, &t.meta, 16));

@@ -31,19 +31,20 @@ struct State {
 //   pend    uint32  children whose mass is not final yet (build only)
 //
 // Walk layout (written at the end of the build): one array of "sources" in
-// which particles come first (index j < n, in Morton order) and the nodes
-// follow in depth-first pre-order (index n + pre(k)):
+// depth-first pre-order in which every leaf is followed by its particles, so
+// opening any source leads to the next entry (first child, or the leaf's
+// first particle) and only the skip target has to be stored:
 //   src     float4  2D node {com.x, com.y, mass, size^2}; particle {x, y, m, -1}
 //                   3D node {com.x, com.y, com.z, mass};  particle {x, y, z, m}
-//   link    2D uint2 {skip, descend}; 3D uint4 {skip, descend, size^2 bits, 0}
-//                   (3D particles carry size^2 = -1).  skip is where the walk goes
-//                   after accepting the source (the subtree's successor in
-//                   pre-order, or the next particle of the same leaf), descend
-//                   where it goes when the source is opened (first child, or the
-//                   leaf's first particle).  The walk ends at n + node_count.
-// The pre-order position needs no top-down pass: with C(e) = #{nodes whose
-// range ends at or before e}, pre(k) = C(start_k) + level_k and the subtree
-// successor is C(end_k) + level_k - same_end_ancestors_k.
+//   link    2D uint32 skip; 3D uint2 {skip, size^2 bits} (particles: size^2 = -1,
+//                   which every opening test accepts).  skip is where the walk
+//                   goes after accepting the entry: the successor of the node's
+//                   subtree, or the next entry for a particle.
+//   slot_of uint32  entry index of each particle (for the self test)
+// The walk starts at entry 0 (the root) and ends at node_count + n.  The
+// positions need no top-down pass: with C(e) = #{nodes whose range ends at or
+// before e}, node k sits at C(start_k) + level_k + start_k and its subtree's
+// successor at C(end_k) + level_k - same_end_ancestors_k + end_k.
 struct Tree {
     float4 *walk;
     float *size2;
@@ -54,8 +55,9 @@ struct Tree {
     uint32_t *small;      // [n / 2] queued small subtrees (build only)
     uint32_t *endcnt;    // [n + 1] node-end histogram, scanned in place
     uint32_t *blocksum;   // [build grid] scan partials
-    float4 *src;          // [n + cap]
-    void *link;           // [n + cap] uint2 (2D) / uint4 (3D)
+    float4 *src;          // [n + cap + 1]
+    void *link;           // [n + cap + 1] uint32 (2D) / uint2 (3D)
+    uint32_t *slot_of;    // [n]
     uint32_t *level;      // [kMaxLevels + 2]
     uint32_t *lvl_alloc;  // [kMaxLevels + 2] per-level child allocation counters
     uint32_t *meta;       // [8] {node_count, levels, bar_count, bar_gen, err, small,

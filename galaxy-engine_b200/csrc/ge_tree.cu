@@ -31,6 +31,7 @@
 // reference's x-major subGrids order with the reference's rounding, so the
 // sums are bit-identical to the reference's whatever order nodes finish in.
 #include <cfloat>
+#include <cuda/atomic>
 
 #include "ge_device.cuh"
 #include "ge_internal.h"
@@ -234,14 +235,14 @@ __device__ __forceinline__ float4 combine_children(const Tree &t, uint4 inf) {
 // result does not depend on which child came last) and carries on upward.
 template <int D>
 __device__ __forceinline__ void finish_upward(Tree &t, uint32_t k) {
-    __threadfence();
+    // the decrement releases this node's mass to the parent's last child,
+    // whose decrement acquires every sibling's (one release sequence per counter)
     uint32_t par = __ldcg(&t.aux[k]).z;
     while (par != kEmpty) {
-        if (atomicSub(&t.pend[par], 1u) != 1u) break;
-        __threadfence();
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> pend(t.pend[par]);
+        if (pend.fetch_sub(1u, cuda::memory_order_acq_rel) != 1u) break;
         const uint4 inf = __ldcg(&t.info[par]);
         put_walk<D>(t, par, combine_children<D>(t, inf), __ldcg(&t.cell[par]).w);
-        __threadfence();
         par = __ldcg(&t.aux[par]).z;
     }
 }
@@ -690,7 +691,7 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
 }
 
 template <int D>
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kBuildThreads, D == 2 ? 3 : 2)
 k_build(State s, StepParams p, Tree t, uint32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -817,43 +818,50 @@ k_build(State s, StepParams p, Tree t, uint32_t *err) {
         grid_barrier(bar_count, bar_gen, err);
         if (gtid == 0) stamp(t);
     }
-    // scatter nodes (and the particles of leaves) into the walk layout:
-    // pre(k) = C(start) + level, subtree successor = C(end) + level - same_end
+    // scatter nodes and the particles of leaves into the walk layout, in which
+    // each leaf's particles follow the leaf: with C(e) the number of nodes
+    // whose range ends at or before e,
+    //   entry of node k      = C(start) + level + start
+    //   subtree successor    = C(end) + level - same_end + end
+    //   entry of particle j  = entry of its leaf + 1 + (j - start)
+    const uint32_t total = nodes + n;
     for (uint32_t k = gtid; k < slots; k += nthreads) {
         const uint4 inf = __ldcg(&t.info[k]);
         if (inf.w == 0u) continue;   // hole
         const uint4 ax = __ldcg(&t.aux[k]);
         const float4 w = __ldcg(&t.walk[k]);
-        const uint32_t me = n + __ldcg(&t.endcnt[inf.z]) + ax.x;
-        const uint32_t skip = n + __ldcg(&t.endcnt[inf.w]) + ax.x - ax.y;
-        const uint32_t down = inf.y ? me + 1 : inf.z;
-        if (me >= n + nodes || skip > n + nodes) {   // cannot happen for a consistent tree
+        const uint32_t me = __ldcg(&t.endcnt[inf.z]) + ax.x + inf.z;
+        const uint32_t skip = __ldcg(&t.endcnt[inf.w]) + ax.x - ax.y + inf.w;
+        if (me >= total || skip > total) {   // cannot happen for a consistent tree
             set_err(err, kErrDepth);
             continue;
         }
         const float nm = D == 2 ? w.z : w.w;
-        if (nm <= 0.0f) {
+        const bool massless = nm <= 0.0f;
+        if (massless) {
             // gridMass <= 0: the reference skips the whole subtree.  As a source
             // it is accepted by every test (size^2 = -1), carries no mass (the
             // walk makes no interaction with a massless source) and leads to
-            // its successor either way.
+            // its successor.
             t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -1.0f) : make_float4(w.x, w.y, w.z, 0.0f);
-            if (D == 2) ((uint2 *)t.link)[me] = make_uint2(skip, skip);
-            else ((uint4 *)t.link)[me] = make_uint4(skip, skip, __float_as_uint(-1.0f), 0u);
-            continue;
+            if (D == 2) ((uint32_t *)t.link)[me] = skip;
+            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-1.0f));
+        } else {
+            t.src[me] = w;
+            if (D == 2) ((uint32_t *)t.link)[me] = skip;
+            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(__ldcg(&t.size2[k])));
         }
-        t.src[me] = w;
-        if (D == 2) ((uint2 *)t.link)[me] = make_uint2(skip, down);
-        else ((uint4 *)t.link)[me] = make_uint4(skip, down, __float_as_uint(__ldcg(&t.size2[k])), 0u);
         if (!inf.y) {
             for (uint32_t j = inf.z; j < inf.w; j++) {
-                const uint32_t nx = j + 1 < inf.w ? j + 1 : skip;
+                const uint32_t e = me + 1 + (j - inf.z);
+                t.slot_of[j] = e;
+                if (massless) continue;   // never reached
                 if (D == 2) {
-                    t.src[j] = make_float4(s.x[j], s.y[j], s.m[j], -1.0f);
-                    ((uint2 *)t.link)[j] = make_uint2(nx, nx);
+                    t.src[e] = make_float4(s.x[j], s.y[j], s.m[j], -1.0f);
+                    ((uint32_t *)t.link)[e] = e + 1;
                 } else {
-                    t.src[j] = make_float4(s.x[j], s.y[j], s.z[j], s.m[j]);
-                    ((uint4 *)t.link)[j] = make_uint4(nx, nx, __float_as_uint(-1.0f), 0u);
+                    t.src[e] = make_float4(s.x[j], s.y[j], s.z[j], s.m[j]);
+                    ((uint2 *)t.link)[e] = make_uint2(e + 1, __float_as_uint(-1.0f));
                 }
             }
         }
@@ -877,9 +885,10 @@ int build_grid_blocks(int dims, int num_sms) {
             &per_sm, dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
             kBuildThreads, 0);
         if (e != cudaSuccess || per_sm < 1) return 0;
-        // at most two blocks per SM: every block joins every grid barrier, so
-        // fewer, larger blocks make the barriers cheaper
-        g_build_blocks[di] = (per_sm < 2 ? per_sm : 2) * num_sms;
+        // at most three blocks per SM: every block joins every grid barrier, so
+        // more blocks lengthen the barriers; more warps hide the latency of
+        // the subtree phase
+        g_build_blocks[di] = (per_sm < 3 ? per_sm : 3) * num_sms;
     }
     return g_build_blocks[di];
 }

@@ -8,14 +8,15 @@
 // over its particles j != i; otherwise the walk descends.  acc_i = F_i / m_i.
 //
 // Here every particle walks the depth-first layout built with the tree
-// (ge_internal.h) with no stack: each step loads one source and its two
-// successor links, evaluates the reference's opening test with the
-// reference's rounding (so the interaction set is exactly the reference's),
-// interacts if accepted and follows `skip` or `descend`.  A leaf's particles
-// are sources of their own with size^2 = -1, which every test accepts, so the
+// (ge_internal.h) with no stack: each step loads one entry and its skip
+// target, evaluates the reference's opening test with the reference's
+// rounding (so the interaction set is exactly the reference's), interacts if
+// accepted and goes to the skip target, else to the next entry (the first
+// child, or a leaf's first particle).  A leaf's particles follow the leaf as
+// entries of their own with size^2 = -1, which every test accepts, so the
 // direct sum over a leaf is the same loop body (the self term j == i is
 // skipped as in the reference); a node of zero mass is laid out as an accepted
-// source without mass, so its subtree is skipped as in the reference.
+// entry without mass, so its subtree is skipped as in the reference.
 // Sources are met in the reference's pre-order, so each particle accumulates
 // in the reference's order.
 //   GE_PREC_EXACT : every interaction with the reference's rounding
@@ -44,24 +45,28 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return r;
 }
 
-// size^2 of a source: in the float4 for 2D, in the link for 3D
-__device__ __forceinline__ float link_s2(const uint2 &, float in_src) { return in_src; }
-__device__ __forceinline__ float link_s2(const uint4 &l, float) { return __uint_as_float(l.z); }
+// skip target and size^2 of an entry: 2D link = skip (size^2 in the source),
+// 3D link = {skip, size^2 bits}
+__device__ __forceinline__ uint32_t link_skip(uint32_t l) { return l; }
+__device__ __forceinline__ uint32_t link_skip(const uint2 &l) { return l.x; }
+__device__ __forceinline__ float link_s2(uint32_t, float in_src) { return in_src; }
+__device__ __forceinline__ float link_s2(const uint2 &l, float) { return __uint_as_float(l.y); }
 
 template <int D> struct LinkOf;
-template <> struct LinkOf<2> { using T = uint2; };
-template <> struct LinkOf<3> { using T = uint4; };
+template <> struct LinkOf<2> { using T = uint32_t; };
+template <> struct LinkOf<3> { using T = uint2; };
 
-template <int D, int MODE, bool COUNT, bool PER>
+template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
 __global__ void __launch_bounds__(kWalkThreads)
 k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
     using LT = typename LinkOf<D>::T;
+    constexpr bool kSelfTest = MODE == GE_PREC_EXACT || COUNT || !POS_EPS;
     const LT *__restrict__ link = (const LT *)t.link;
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
     const uint32_t end = (uint32_t)n + __ldg(&t.meta[0]);
-    const uint32_t limit = end + 1;   // every source is met at most once
+    const uint32_t limit = end + 1;   // every entry is met at most once
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
@@ -71,8 +76,9 @@ k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *int
         pi[2] = D == 3 ? s.z[i] : 0.0f;
         const float mi = s.m[i];
         const float gm_i = fmul(G, mi);   // Gf * pmass (exact mode)
+        const uint32_t self = kSelfTest ? __ldg(&t.slot_of[i]) : kEmpty;
         float f[3] = {0.f, 0.f, 0.f};
-        uint32_t k = (uint32_t)n, steps = 0, cnt = 0;
+        uint32_t k = 0, steps = 0, cnt = 0;
         while (k < end) {
             if (++steps > limit) { set_err(err, kErrStack); break; }
             const float4 A = __ldg(&src[k]);
@@ -91,22 +97,31 @@ k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *int
             if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
             r2 = fadd(r2, eps2);
             const bool acc = s2 < fmul(th2, r2);
-            if (acc && m != 0.0f && k != (uint32_t)i) {
-                if (MODE == GE_PREC_EXACT) {
-                    const float inv = fdiv(1.0f, __fsqrt_rn(r2));
-                    const float inv3 = fmul(fmul(inv, inv), inv);
-                    const float fm = fmul(fmul(gm_i, m), inv3);
+            if (kSelfTest) {
+                if (acc && m != 0.0f && k != self) {
+                    if (MODE == GE_PREC_EXACT) {
+                        const float inv = fdiv(1.0f, __fsqrt_rn(r2));
+                        const float inv3 = fmul(fmul(inv, inv), inv);
+                        const float fm = fmul(fmul(gm_i, m), inv3);
 #pragma unroll
-                    for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(d[a], fm));
-                } else {
-                    const float inv = rsqrt_approx(r2);
-                    const float fm = m * (inv * inv * inv);
+                        for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(d[a], fm));
+                    } else {
+                        const float inv = rsqrt_approx(r2);
+                        const float fm = m * (inv * inv * inv);
 #pragma unroll
-                    for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
+                        for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
+                    }
+                    if (COUNT) cnt++;
                 }
-                if (COUNT) cnt++;
+            } else {
+                // eps2 > 0: the self term (d = 0) and massless sources add exactly
+                // zero, so no test is needed for them
+                const float inv = rsqrt_approx(r2);
+                const float fm = acc ? m * (inv * inv * inv) : 0.0f;
+#pragma unroll
+                for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
             }
-            k = acc ? L.x : L.y;
+            k = acc ? link_skip(L) : k + 1;
         }
         float a3[3];
 #pragma unroll
@@ -126,22 +141,28 @@ k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *int
     }
 }
 
-template <int D, int MODE, bool COUNT, bool PER>
+template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
 static cudaError_t walk_one(const State &s, const StepParams &p, const Tree &t, int ie,
                             unsigned long long *inter, uint32_t *err, cudaStream_t st) {
     const int blocks = (p.n + kWalkThreads - 1) / kWalkThreads;
-    k_walk<D, MODE, COUNT, PER><<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, t, ie, inter, err);
+    k_walk<D, MODE, COUNT, PER, POS_EPS>
+        <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, t, ie, inter, err);
     return cudaGetLastError();
+}
+
+template <int D, int MODE, bool PER>
+static cudaError_t walk_eps(const State &s, const StepParams &p, const Tree &t, int ie,
+                            unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if (inter) return walk_one<D, MODE, true, PER, false>(s, p, t, ie, inter, err, st);
+    if (p.eps2 > 0.0f) return walk_one<D, MODE, false, PER, true>(s, p, t, ie, nullptr, err, st);
+    return walk_one<D, MODE, false, PER, false>(s, p, t, ie, nullptr, err, st);
 }
 
 template <int D, int MODE>
 static cudaError_t walk_mode(const State &s, const StepParams &p, const Tree &t, int ie,
                              unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    if (p.periodic)
-        return inter ? walk_one<D, MODE, true, true>(s, p, t, ie, inter, err, st)
-                     : walk_one<D, MODE, false, true>(s, p, t, ie, nullptr, err, st);
-    return inter ? walk_one<D, MODE, true, false>(s, p, t, ie, inter, err, st)
-                 : walk_one<D, MODE, false, false>(s, p, t, ie, nullptr, err, st);
+    if (p.periodic) return walk_eps<D, MODE, true>(s, p, t, ie, inter, err, st);
+    return walk_eps<D, MODE, false>(s, p, t, ie, inter, err, st);
 }
 
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
