@@ -99,6 +99,13 @@ SIGNATURES = {
     "ge_sums_f64": ([_vp, _vp], C.c_int),
     "ge_build_timeline": ([_vp, C.c_int32, _vp, _vp], C.c_int),
     "ge_morton_sort_2d_noalloc": ([C.c_int64, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "ge_batch_create": ([C.POINTER(Params), C.POINTER(_vp)], C.c_int),
+    "ge_batch_step": ([_vp, C.c_int32], C.c_int),
+    "ge_batch_add_sim": ([_vp, C.c_int64] + [_vp] * 8 + [C.POINTER(C.c_int32)], C.c_int),
+    "ge_batch_remove_sim": ([_vp, C.c_int32], C.c_int),
+    "ge_batch_list": ([_vp, C.c_int32, _vp, C.POINTER(C.c_int32)], C.c_int),
+    "ge_batch_query": ([_vp, C.c_int32, _vp, _vp, _vp], C.c_int),
+    "ge_batch_download_sim": ([_vp, C.c_int32] + [_vp] * 11, C.c_int),
 }
 NOALLOC_MAX_N = 262144   # GE_NOALLOC_MAX_N
 
@@ -215,18 +222,59 @@ class Simulation:
         p = None if pinned is None else np.ascontiguousarray(pinned, np.uint8)
         self._check(lib().ge_upload_pinned(self._h, _ptr(p)))
 
-    def download(self):
-        n, d3 = self.n, self.dims == 3
+    def _host_state(self, n):
         out = {k: np.empty(n, np.float32) for k in ("x", "y", "vx", "vy", "ax", "ay", "m")}
-        if d3:
+        if self.dims == 3:
             for k in ("z", "vz", "az"):
                 out[k] = np.empty(n, np.float32)
         out["id"] = np.empty(n, np.uint32)
         g = out.get
-        self._check(lib().ge_download(self._h, _ptr(g("x")), _ptr(g("y")), _ptr(g("z")),
-                                      _ptr(g("vx")), _ptr(g("vy")), _ptr(g("vz")),
-                                      _ptr(g("ax")), _ptr(g("ay")), _ptr(g("az")),
-                                      _ptr(g("m")), _ptr(g("id"))))
+        ptrs = [_ptr(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m", "id")]
+        return out, ptrs
+
+    def download(self):
+        out, ptrs = self._host_state(self.n)
+        self._check(lib().ge_download(self._h, *ptrs))
+        return out
+
+    # -- batched simulations ------------------------------------------------
+    def add_sim(self, state):
+        """Append an independent simulation (same dict as upload, no ax/ay/az);
+        returns its handle.  Every later step advances all simulations."""
+        g = state.get
+        arrs = {k: _f32(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        ids = None if g("id") is None else np.ascontiguousarray(g("id"), np.uint32)
+        h = C.c_int32(0)
+        self._check(lib().ge_batch_add_sim(self._h, len(arrs["x"]), _ptr(arrs["x"]),
+                                           _ptr(arrs["y"]), _ptr(arrs["z"]), _ptr(arrs["vx"]),
+                                           _ptr(arrs["vy"]), _ptr(arrs["vz"]), _ptr(arrs["m"]),
+                                           _ptr(ids), C.byref(h)))
+        self.n = int(self.stats().n)
+        return h.value
+
+    def remove_sim(self, sim):
+        self._check(lib().ge_batch_remove_sim(self._h, int(sim)))
+        self.n = int(self.stats().n)
+
+    def sims(self):
+        """Handles of the simulations, in slot order."""
+        cnt = C.c_int32(0)
+        self._check(lib().ge_batch_list(self._h, 0, None, C.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1), np.int32)
+        self._check(lib().ge_batch_list(self._h, len(out), _ptr(out), C.byref(cnt)))
+        return [int(v) for v in out[: cnt.value]]
+
+    def query(self, sim):
+        """(particles, first slot, steps since added) of a simulation."""
+        n, off, steps = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        self._check(lib().ge_batch_query(self._h, int(sim), C.byref(n), C.byref(off),
+                                         C.byref(steps)))
+        return n.value, off.value, steps.value
+
+    def download_sim(self, sim):
+        n = self.query(sim)[0]
+        out, ptrs = self._host_state(n)
+        self._check(lib().ge_batch_download_sim(self._h, int(sim), *ptrs))
         return out
 
     def download_prev_vel(self):

@@ -1,18 +1,25 @@
 // ge_api.cu -- host side of the C ABI (include/ge_bh.h): context, resident
-// device state, the per-frame pipeline and the stage calls.
+// device state, the per-frame pipeline, the stage calls and the batch of
+// independent simulations.
 //
 // One frame (GalaxyEngine/src/globalLogic.cpp:1155-1370 in 2D, :1584-1719 in 3D):
-//   1. kick + drift fused with the bounding box          (integrateStart, boundingBox)
+//   1. kick + drift fused with the bounding boxes         (integrateStart, boundingBox)
 //   2. Morton keys + digit histograms                      (computeMortonKeys)
 //   3. stable radix sort passes                            (sortParticlesByMortonKey)
 //   4. gather of the state into Morton order
 //   5. tree build with mass / centre of mass               (Quadtree / Octree)
 //   6. tree walk with the second half kick fused           (calculateForceFromGrid, integrateEnd)
 // All of it is enqueued on the context's stream; nothing returns to the host
-// between stages.
+// between stages.  A context holds S >= 1 independent simulations back to
+// back in its arrays (segments, ge_internal.h); every stage runs once over
+// all of them, so a batch of many small simulations costs one launch per
+// stage instead of one per simulation.
+#include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ge_bh.h"
@@ -21,21 +28,75 @@
 
 using namespace ge;
 
+namespace gehost {
+
+// Device buffers sized for a particle capacity; replaced as a whole when the
+// capacity grows (the particle state is copied across).
+struct Buffers {
+    int64_t cap_n = 0;
+    State st[2]{};
+    SortScratch ss{};
+    Tree tree{};
+    unsigned long long *d_inter = nullptr;
+    bool prev = false;     // prevVel arrays allocated
+    bool pinned = false;   // pin flag arrays allocated
+    std::vector<void *> allocs;
+};
+
+// Segment tables, sized for a segment, tile and particle capacity.
+struct SegBuffers {
+    int64_t seg_cap = 0, tile_cap = 0, n_cap = 0;
+    uint32_t *off = nullptr, *tile_base = nullptr, *seg_of = nullptr, *tile_seg = nullptr;
+    float4 *box = nullptr;
+    uint32_t *boxmm = nullptr, *root_begin = nullptr, *root_end = nullptr;
+    uint32_t *hist = nullptr, *status = nullptr;
+    std::vector<void *> allocs;
+};
+
+struct SimRec {
+    int32_t handle;
+    int64_t n;
+    int64_t step0;   // context steps when the simulation was added
+};
+
+inline void free_all(std::vector<void *> &v) {
+    for (void *q : v) cudaFree(q);
+    v.clear();
+}
+
+template <typename T>
+cudaError_t dalloc(std::vector<void *> &list, T **p, size_t count) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+    if (e != cudaSuccess) return e;
+    list.push_back(q);
+    *p = (T *)q;
+    return cudaSuccess;
+}
+
+constexpr int kMaxPasses = 8;   // radix passes of the 3D keys (2D uses 5)
+
+}  // namespace gehost
+
+using namespace gehost;
+
 struct ge_ctx {
     ge_params p{};
     int dev = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    int64_t n = 0, cap_n = 0;
-    State st[2]{};
-    int cur = 0;
-    bool has_pinned = false;
-    bool has_prev = false;
-    SortScratch ss{};
-    Tree tree{};
+    int64_t n = 0;                // particles over all simulations
+    int cur = 0;                  // which of b.st[2] holds the state
+    bool has_pinned = false;      // pin flags uploaded and in effect
+    Buffers b;
+    SegBuffers sb;
+    Segs g{};
+    std::vector<SimRec> sims;     // in slot order
+    int32_t next_handle = 1;
+    int64_t total_steps = 0;
+    std::vector<uint32_t> h_off, h_tile_base;
     uint32_t *d_err = nullptr;
-    unsigned long long *d_inter = nullptr;
     uint32_t *h_meta = nullptr;   // pinned copy of the tree meta words
     int64_t slots = 0;            // node slots of the last build (holes included)
     bool count_inter = false;
@@ -44,7 +105,6 @@ struct ge_ctx {
     cudaEvent_t ev[8]{};
     ge_stats stats{};
     std::string err;
-    std::vector<void *> allocs;
 };
 
 namespace {
@@ -55,6 +115,8 @@ int fail(ge_ctx *c, int code, const std::string &msg) {
 }
 
 int cuda_fail(ge_ctx *c, cudaError_t e, const char *where) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(c, GE_ERR_OOM, std::string(where) + ": " + cudaGetErrorString(e));
     return fail(c, GE_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
@@ -64,28 +126,19 @@ int cuda_fail(ge_ctx *c, cudaError_t e, const char *where) {
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
     } while (0)
 
-template <typename T>
-cudaError_t dalloc(ge_ctx *c, T **p, size_t count) {
-    void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
-    if (e != cudaSuccess) return e;
-    c->allocs.push_back(q);
-    *p = (T *)q;
-    return cudaSuccess;
-}
-
 void free_buffers(ge_ctx *c) {
-    for (void *q : c->allocs) cudaFree(q);
-    c->allocs.clear();
-    c->st[0] = State{};
-    c->st[1] = State{};
-    c->ss = SortScratch{};
-    c->tree = Tree{};
+    free_all(c->b.allocs);
+    free_all(c->sb.allocs);
+    c->b = Buffers{};
+    c->sb = SegBuffers{};
+    c->g = Segs{};
     c->d_err = nullptr;
-    c->d_inter = nullptr;
-    c->cap_n = 0;
     c->has_pinned = false;
-    c->has_prev = false;
+    c->n = 0;
+    c->cur = 0;
+    c->sims.clear();
+    c->tree_valid = false;
+    c->keys_valid = false;
 }
 
 StepParams step_params(const ge_ctx *c) {
@@ -122,82 +175,218 @@ int validate(ge_ctx *c, const ge_params *p) {
     return GE_OK;
 }
 
-// (Re)allocate every device buffer for n particles.
-int ensure_capacity(ge_ctx *c, int64_t n) {
+// Allocates every per-particle and tree buffer of `nb` for cap particles.
+int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool prev, bool pinned) {
     const int D = c->p.dims;
-    const int64_t slack = build_node_slack(D, c->num_sms);
-    if (slack <= 0) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
-    const int64_t node_cap = (int64_t)(c->p.node_cap_factor * (double)n) + 1024 + slack;
-    if (n <= c->cap_n && node_cap <= c->tree.cap && c->has_prev == (bool)c->p.track_prev_vel)
-        return GE_OK;
-    if (D == 2 && n >= (1ll << 28)) return fail(c, GE_ERR_ARG, "2D supports N < 2^28");
-    if (node_cap >= (1ll << 32) - 1) return fail(c, GE_ERR_ARG, "node capacity exceeds 2^32");
-    free_buffers(c);
-    const size_t N = (size_t)n;
-    for (int b = 0; b < 2; b++) {
-        State &s = c->st[b];
-        GE_CHECK(c, dalloc(c, &s.x, N)); GE_CHECK(c, dalloc(c, &s.y, N));
-        GE_CHECK(c, dalloc(c, &s.vx, N)); GE_CHECK(c, dalloc(c, &s.vy, N));
-        GE_CHECK(c, dalloc(c, &s.ax, N)); GE_CHECK(c, dalloc(c, &s.ay, N));
+    const size_t N = (size_t)cap;
+    auto &L = nb.allocs;
+    nb.cap_n = cap;
+    nb.prev = prev;
+    nb.pinned = pinned;
+    for (int k = 0; k < 2; k++) {
+        State &s = nb.st[k];
+        GE_CHECK(c, dalloc(L, &s.x, N)); GE_CHECK(c, dalloc(L, &s.y, N));
+        GE_CHECK(c, dalloc(L, &s.vx, N)); GE_CHECK(c, dalloc(L, &s.vy, N));
+        GE_CHECK(c, dalloc(L, &s.ax, N)); GE_CHECK(c, dalloc(L, &s.ay, N));
         if (D == 3) {
-            GE_CHECK(c, dalloc(c, &s.z, N)); GE_CHECK(c, dalloc(c, &s.vz, N));
-            GE_CHECK(c, dalloc(c, &s.az, N));
+            GE_CHECK(c, dalloc(L, &s.z, N)); GE_CHECK(c, dalloc(L, &s.vz, N));
+            GE_CHECK(c, dalloc(L, &s.az, N));
         }
-        GE_CHECK(c, dalloc(c, &s.m, N));
-        GE_CHECK(c, dalloc(c, &s.id, N));
-        if (c->p.track_prev_vel) {
-            GE_CHECK(c, dalloc(c, &s.pvx, N)); GE_CHECK(c, dalloc(c, &s.pvy, N));
-            if (D == 3) GE_CHECK(c, dalloc(c, &s.pvz, N));
+        GE_CHECK(c, dalloc(L, &s.m, N));
+        GE_CHECK(c, dalloc(L, &s.id, N));
+        if (prev) {
+            GE_CHECK(c, dalloc(L, &s.pvx, N)); GE_CHECK(c, dalloc(L, &s.pvy, N));
+            if (D == 3) GE_CHECK(c, dalloc(L, &s.pvz, N));
         }
+        if (pinned) GE_CHECK(c, dalloc(L, &s.pinned, N));
     }
-    c->has_prev = c->p.track_prev_vel != 0;
-    SortScratch &ss = c->ss;
-    GE_CHECK(c, dalloc(c, &ss.keys[0], N)); GE_CHECK(c, dalloc(c, &ss.keys[1], N));
-    if (D == 3) { GE_CHECK(c, dalloc(c, &ss.vals[0], N)); GE_CHECK(c, dalloc(c, &ss.vals[1], N)); }
-    ss.tiles = (n + kSortTile - 1) / kSortTile;
-    GE_CHECK(c, dalloc(c, &ss.hist, 8 * 256));
-    GE_CHECK(c, dalloc(c, &ss.status, (size_t)8 * ss.tiles * 256));
-    GE_CHECK(c, dalloc(c, &ss.tile_ctr, 8));
-    int bb = (int)((n + kBBoxThreads - 1) / kBBoxThreads);
-    if (bb > c->num_sms * 4) bb = c->num_sms * 4;
-    if (bb < 1) bb = 1;
-    ss.bbox_blocks = bb;
-    GE_CHECK(c, dalloc(c, &ss.bbox_part, 2 * (size_t)bb));
-    GE_CHECK(c, dalloc(c, &ss.bbox_ctr, 1));
-    GE_CHECK(c, dalloc(c, &ss.bbox, 1));
-    GE_CHECK(c, cudaMemset(ss.bbox_ctr, 0, sizeof(uint32_t)));
-    Tree &t = c->tree;
+    SortScratch &ss = nb.ss;
+    GE_CHECK(c, dalloc(L, &ss.keys[0], N)); GE_CHECK(c, dalloc(L, &ss.keys[1], N));
+    if (D == 3) { GE_CHECK(c, dalloc(L, &ss.vals[0], N)); GE_CHECK(c, dalloc(L, &ss.vals[1], N)); }
+    GE_CHECK(c, dalloc(L, &ss.tile_ctr, 8));
+    Tree &t = nb.tree;
     t.cap = node_cap;
-    GE_CHECK(c, dalloc(c, &t.walk, (size_t)node_cap));
-    if (D == 3) GE_CHECK(c, dalloc(c, &t.size2, (size_t)node_cap));
-    GE_CHECK(c, dalloc(c, &t.info, (size_t)node_cap));
-    GE_CHECK(c, dalloc(c, &t.cell, (size_t)node_cap));
-    GE_CHECK(c, dalloc(c, &t.aux, (size_t)node_cap));
-    GE_CHECK(c, dalloc(c, &t.pend, (size_t)node_cap));
-    GE_CHECK(c, dalloc(c, &t.small, N / 2 + 1));
-    GE_CHECK(c, dalloc(c, &t.endcnt, N + 1));
+    GE_CHECK(c, dalloc(L, &t.walk, (size_t)node_cap));
+    if (D == 3) GE_CHECK(c, dalloc(L, &t.size2, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.info, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.cell, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.aux, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.pend, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.small, N / 2 + 1));
+    GE_CHECK(c, dalloc(L, &t.endcnt, N + 1));
     const int bblocks = build_grid_blocks(D, c->num_sms);
     if (bblocks < 1) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
-    GE_CHECK(c, dalloc(c, &t.blocksum, (size_t)bblocks));
-    GE_CHECK(c, dalloc(c, &t.src, N + (size_t)node_cap + 1));
+    GE_CHECK(c, dalloc(L, &t.blocksum, (size_t)bblocks));
+    GE_CHECK(c, dalloc(L, &t.src, N + (size_t)node_cap + 1));
     if (D == 2) {
         uint32_t *l = nullptr;
-        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap + 1));
+        GE_CHECK(c, dalloc(L, &l, N + (size_t)node_cap + 1));
         t.link = l;
     } else {
         uint2 *l = nullptr;
-        GE_CHECK(c, dalloc(c, &l, N + (size_t)node_cap + 1));
+        GE_CHECK(c, dalloc(L, &l, N + (size_t)node_cap + 1));
         t.link = l;
     }
-    GE_CHECK(c, dalloc(c, &t.slot_of, N));
-    GE_CHECK(c, dalloc(c, &t.level, kMaxLevels + 2));
-    GE_CHECK(c, dalloc(c, &t.lvl_alloc, kMaxLevels + 2));
-    GE_CHECK(c, dalloc(c, &t.meta, 16));
-    GE_CHECK(c, dalloc(c, &t.tl, kTimeline));
-    GE_CHECK(c, cudaMemset(t.meta, 0, 16 * sizeof(uint32_t)));
-    c->d_err = t.meta + 4;
-    GE_CHECK(c, dalloc(c, &c->d_inter, 1));
-    c->cap_n = n;
+    GE_CHECK(c, dalloc(L, &t.slot_of, N));
+    GE_CHECK(c, dalloc(L, &t.level, kMaxLevels + 2));
+    GE_CHECK(c, dalloc(L, &t.lvl_alloc, kMaxLevels + 2));
+    GE_CHECK(c, dalloc(L, &t.meta, 16));
+    GE_CHECK(c, dalloc(L, &t.tl, kTimeline));
+    GE_CHECK(c, cudaMemsetAsync(t.meta, 0, 16 * sizeof(uint32_t), c->stream));
+    GE_CHECK(c, dalloc(L, &nb.d_inter, 1));
+    return GE_OK;
+}
+
+// Copies particles [soff, soff + cnt) of src to [doff, doff + cnt) of dst
+// (device to device, on the context's stream).
+int copy_range(ge_ctx *c, const State &dst, int64_t doff, const State &src, int64_t soff,
+               int64_t cnt, bool prev, bool pinned) {
+    if (cnt <= 0) return GE_OK;
+    const bool d3 = c->p.dims == 3;
+    const size_t B = sizeof(float) * (size_t)cnt;
+    float *const fd[] = {dst.x, dst.y, d3 ? dst.z : nullptr, dst.vx, dst.vy, d3 ? dst.vz : nullptr,
+                         dst.ax, dst.ay, d3 ? dst.az : nullptr, dst.m,
+                         prev ? dst.pvx : nullptr, prev ? dst.pvy : nullptr,
+                         prev && d3 ? dst.pvz : nullptr};
+    const float *const fs[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.ax, src.ay,
+                               src.az, src.m, src.pvx, src.pvy, src.pvz};
+    for (size_t k = 0; k < sizeof(fd) / sizeof(fd[0]); k++)
+        if (fd[k])
+            GE_CHECK(c, cudaMemcpyAsync(fd[k] + doff, fs[k] + soff, B, cudaMemcpyDeviceToDevice,
+                                        c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(dst.id + doff, src.id + soff, sizeof(uint32_t) * (size_t)cnt,
+                                cudaMemcpyDeviceToDevice, c->stream));
+    if (pinned)
+        GE_CHECK(c, cudaMemcpyAsync(dst.pinned + doff, src.pinned + soff, (size_t)cnt,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    return GE_OK;
+}
+
+int64_t node_cap_for(const ge_ctx *c, int64_t n, int64_t S, int64_t slack) {
+    return (int64_t)(c->p.node_cap_factor * (double)n) + 1024 + slack + S;
+}
+
+// Makes the buffers hold n particles in S simulations.  With `keep` the
+// current c->n particles survive a reallocation (they move to st[0]).
+int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep) {
+    const int D = c->p.dims;
+    const int64_t slack = build_node_slack(D, c->num_sms);
+    if (slack <= 0) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
+    if (D == 2 && n >= (1ll << 28)) return fail(c, GE_ERR_ARG, "2D supports N < 2^28 per context");
+    if (n >= (1ll << 31)) return fail(c, GE_ERR_ARG, "N must be < 2^31 per context");
+    const bool want_prev = c->p.track_prev_vel != 0;
+    Buffers &ob = c->b;
+    if (n <= ob.cap_n && node_cap_for(c, n, S, slack) <= ob.tree.cap && ob.prev == want_prev)
+        return GE_OK;
+    // a live context grows by half again at least, so adding simulations one
+    // by one reallocates O(log) times
+    int64_t cap = n, scap = S;
+    if (keep && ob.cap_n > 0) {
+        cap = std::max(n, ob.cap_n + ob.cap_n / 2);
+        scap = S + S / 2;
+        const int64_t lim = D == 2 ? (1ll << 28) - 1 : (1ll << 31) - 1;
+        if (cap > lim) cap = lim;
+    }
+    const int64_t node_cap = node_cap_for(c, cap, scap, slack);
+    if (node_cap >= (1ll << 32) - 1) return fail(c, GE_ERR_ARG, "node capacity exceeds 2^32");
+    Buffers nb;
+    int rc = alloc_buffers(c, nb, cap, node_cap, want_prev, ob.pinned);
+    if (rc) {
+        cudaStreamSynchronize(c->stream);
+        free_all(nb.allocs);
+        return rc;
+    }
+    if (keep && c->n > 0) {
+        rc = copy_range(c, nb.st[0], 0, ob.st[c->cur], 0, c->n, ob.prev && want_prev, ob.pinned);
+        if (rc) {
+            cudaStreamSynchronize(c->stream);
+            free_all(nb.allocs);
+            return rc;
+        }
+    }
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    free_all(ob.allocs);
+    c->b = std::move(nb);
+    c->cur = 0;
+    c->d_err = c->b.tree.meta + 4;
+    c->tree_valid = false;
+    c->keys_valid = false;
+    return GE_OK;
+}
+
+// Rebuilds the segment tables from c->sims (after any change of the
+// simulations or of the capacity) and binds them to the sort scratch.
+int sync_segments(ge_ctx *c) {
+    const int64_t S = (int64_t)c->sims.size();
+    c->h_off.assign((size_t)S + 1, 0u);
+    c->h_tile_base.assign((size_t)S + 1, 0u);
+    for (int64_t s = 0; s < S; s++) {
+        c->h_off[s + 1] = c->h_off[s] + (uint32_t)c->sims[s].n;
+        c->h_tile_base[s + 1] =
+            c->h_tile_base[s] + (uint32_t)((c->sims[s].n + kSortTile - 1) / kSortTile);
+    }
+    const int64_t tiles = c->h_tile_base[S];
+    SegBuffers &sb = c->sb;
+    if (S > sb.seg_cap || tiles > sb.tile_cap || c->b.cap_n > sb.n_cap) {
+        SegBuffers nb;
+        nb.seg_cap = std::max<int64_t>(std::max<int64_t>(S, 1), sb.seg_cap + sb.seg_cap / 2);
+        nb.n_cap = c->b.cap_n;
+        nb.tile_cap = std::max<int64_t>(tiles, nb.n_cap / kSortTile + nb.seg_cap + 1);
+        const size_t SC = (size_t)nb.seg_cap, TC = (size_t)nb.tile_cap;
+        auto &L = nb.allocs;
+        cudaError_t e = cudaSuccess;
+        if (e == cudaSuccess) e = dalloc(L, &nb.off, SC + 1);
+        if (e == cudaSuccess) e = dalloc(L, &nb.tile_base, SC + 1);
+        if (e == cudaSuccess) e = dalloc(L, &nb.seg_of, (size_t)nb.n_cap);
+        if (e == cudaSuccess) e = dalloc(L, &nb.tile_seg, TC);
+        if (e == cudaSuccess) e = dalloc(L, &nb.box, SC);
+        if (e == cudaSuccess) e = dalloc(L, &nb.boxmm, 6 * SC);
+        if (e == cudaSuccess) e = dalloc(L, &nb.root_begin, SC);
+        if (e == cudaSuccess) e = dalloc(L, &nb.root_end, SC);
+        if (e == cudaSuccess) e = dalloc(L, &nb.hist, (size_t)kMaxPasses * SC * 256);
+        if (e == cudaSuccess) e = dalloc(L, &nb.status, (size_t)kMaxPasses * TC * 256);
+        if (e == cudaSuccess) {
+            Segs all{};
+            all.S = (int)nb.seg_cap;
+            all.boxmm = nb.boxmm;
+            e = launch_reset_boxes(all, c->stream);
+        }
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(c->stream);
+            free_all(L);
+            return cuda_fail(c, e, "segment tables");
+        }
+        GE_CHECK(c, cudaStreamSynchronize(c->stream));
+        free_all(sb.allocs);
+        sb = std::move(nb);
+    }
+    Segs &g = c->g;
+    g = Segs{};
+    g.S = (int)S;
+    g.tiles = tiles;
+    g.box = sb.box;
+    g.boxmm = sb.boxmm;
+    g.root_begin = sb.root_begin;
+    g.root_end = sb.root_end;
+    if (S > 1) {
+        GE_CHECK(c, cudaMemcpyAsync(sb.off, c->h_off.data(), sizeof(uint32_t) * (S + 1),
+                                    cudaMemcpyHostToDevice, c->stream));
+        GE_CHECK(c, cudaMemcpyAsync(sb.tile_base, c->h_tile_base.data(), sizeof(uint32_t) * (S + 1),
+                                    cudaMemcpyHostToDevice, c->stream));
+        GE_CHECK(c, launch_seg_tables(sb.off, sb.tile_base, (int)S, (int)c->n, tiles, sb.seg_of,
+                                      sb.tile_seg, c->stream));
+        GE_CHECK(c, cudaStreamSynchronize(c->stream));   // the host tables are reused
+        g.off = sb.off;
+        g.seg_of = sb.seg_of;
+        g.tile_base = sb.tile_base;
+        g.tile_seg = sb.tile_seg;
+    }
+    c->b.ss.hist = sb.hist;
+    c->b.ss.status = sb.status;
+    int64_t bb = (c->n + kBBoxThreads * 16 - 1) / (kBBoxThreads * 16);
+    if (bb > (int64_t)c->num_sms * 4) bb = (int64_t)c->num_sms * 4;
+    if (bb < 1) bb = 1;
+    c->b.ss.box_blocks = (int)bb;
     c->tree_valid = false;
     c->keys_valid = false;
     return GE_OK;
@@ -205,7 +394,7 @@ int ensure_capacity(ge_ctx *c, int64_t n) {
 
 // Reads back the error word and tree size; clears the error word.
 int check_device(ge_ctx *c) {
-    GE_CHECK(c, cudaMemcpyAsync(c->h_meta, c->tree.meta, 10 * sizeof(uint32_t),
+    GE_CHECK(c, cudaMemcpyAsync(c->h_meta, c->b.tree.meta, 10 * sizeof(uint32_t),
                                 cudaMemcpyDeviceToHost, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     const uint32_t e = c->h_meta[4];
@@ -227,7 +416,13 @@ int check_device(ge_ctx *c) {
 }
 
 State cur_state(ge_ctx *c) {
-    State s = c->st[c->cur];
+    State s = c->b.st[c->cur];
+    if (!c->has_pinned) s.pinned = nullptr;
+    return s;
+}
+
+State other_state(ge_ctx *c) {
+    State s = c->b.st[c->cur ^ 1];
     if (!c->has_pinned) s.pinned = nullptr;
     return s;
 }
@@ -235,28 +430,31 @@ State cur_state(ge_ctx *c) {
 int enqueue_bbox(ge_ctx *c, bool kick) {
     StepParams p = step_params(c);
     State s = cur_state(c);
-    GE_CHECK(c, launch_kick_drift_bbox(c->p.dims, s, p, kick, c->ss, c->tree, c->d_err, c->stream));
+    GE_CHECK(c, launch_kick_drift_bbox(c->p.dims, s, p, kick, c->g, c->b.ss, c->b.tree, c->stream));
     return GE_OK;
 }
 
 int enqueue_keys(ge_ctx *c) {
-    GE_CHECK(c, launch_keys(c->p.dims, cur_state(c), (int)c->n, c->ss, c->stream));
+    GE_CHECK(c, launch_keys(c->p.dims, cur_state(c), (int)c->n, c->g, c->b.ss, c->stream));
     return GE_OK;
 }
 
-int enqueue_sort_permute(ge_ctx *c, bool with_acc) {
-    GE_CHECK(c, launch_sort(c->p.dims, (int)c->n, c->ss, c->d_err, c->stream));
-    State in = cur_state(c);
-    State out = c->st[c->cur ^ 1];
-    if (!c->has_pinned) out.pinned = nullptr;
-    GE_CHECK(c, launch_permute(c->p.dims, (int)c->n, c->ss, in, out, with_acc, c->stream));
+int enqueue_sort(ge_ctx *c) {
+    GE_CHECK(c, launch_sort(c->p.dims, (int)c->n, c->g, c->b.ss, c->d_err, c->stream));
+    return GE_OK;
+}
+
+int enqueue_permute(ge_ctx *c, bool with_acc) {
+    GE_CHECK(c, launch_permute(c->p.dims, (int)c->n, c->b.ss, cur_state(c), other_state(c),
+                               with_acc, c->stream));
     c->cur ^= 1;
     return GE_OK;
 }
 
 int enqueue_build(ge_ctx *c) {
     StepParams p = step_params(c);
-    GE_CHECK(c, launch_build(c->p.dims, cur_state(c), p, c->tree, c->d_err, c->num_sms, c->stream));
+    GE_CHECK(c, launch_build(c->p.dims, cur_state(c), p, c->g, c->b.tree, c->d_err, c->num_sms,
+                             c->stream));
     return GE_OK;
 }
 
@@ -264,11 +462,11 @@ int enqueue_walk(ge_ctx *c, bool integrate_end) {
     StepParams p = step_params(c);
     unsigned long long *cnt = nullptr;
     if (c->count_inter) {
-        GE_CHECK(c, cudaMemsetAsync(c->d_inter, 0, sizeof(unsigned long long), c->stream));
-        cnt = c->d_inter;
+        GE_CHECK(c, cudaMemsetAsync(c->b.d_inter, 0, sizeof(unsigned long long), c->stream));
+        cnt = c->b.d_inter;
     }
-    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, cur_state(c), p, c->tree, integrate_end,
-                            cnt, c->d_err, c->stream));
+    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, cur_state(c), p, c->g, c->b.tree,
+                            integrate_end, cnt, c->d_err, c->stream));
     return GE_OK;
 }
 
@@ -279,15 +477,9 @@ int enqueue_frame(ge_ctx *c, cudaEvent_t *ev) {
     if (ev) GE_CHECK(c, cudaEventRecord(ev[1], c->stream));
     if ((rc = enqueue_keys(c))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[2], c->stream));
-    GE_CHECK(c, launch_sort(c->p.dims, (int)c->n, c->ss, c->d_err, c->stream));
+    if ((rc = enqueue_sort(c))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[3], c->stream));
-    {
-        State in = cur_state(c);
-        State out = c->st[c->cur ^ 1];
-        if (!c->has_pinned) out.pinned = nullptr;
-        GE_CHECK(c, launch_permute(c->p.dims, (int)c->n, c->ss, in, out, false, c->stream));
-        c->cur ^= 1;
-    }
+    if ((rc = enqueue_permute(c, false))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[4], c->stream));
     if ((rc = enqueue_build(c))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[5], c->stream));
@@ -300,6 +492,83 @@ int require_state(ge_ctx *c) {
     if (!c) return GE_ERR_ARG;
     if (c->n <= 0) return fail(c, GE_ERR_STATE, "no particles uploaded");
     return GE_OK;
+}
+
+int check_host_arrays(ge_ctx *c, int64_t n, const float *x, const float *y, const float *z,
+                      const float *vx, const float *vy, const float *vz, const float *m) {
+    if (n < 1) return fail(c, GE_ERR_ARG, "n must be >= 1");
+    if (!x || !y || !vx || !vy || !m || (c->p.dims == 3 && (!z || !vz)))
+        return fail(c, GE_ERR_ARG, "positions, velocities and masses are required");
+    return GE_OK;
+}
+
+// Host arrays into particles [off, off + n) of the current state.
+int put_host(ge_ctx *c, int64_t off, int64_t n, const float *x, const float *y, const float *z,
+             const float *vx, const float *vy, const float *vz, const float *m,
+             const uint32_t *id, const float *ax, const float *ay, const float *az) {
+    const int D = c->p.dims;
+    const State &s = c->b.st[c->cur];
+    const size_t B = sizeof(float) * (size_t)n;
+    cudaStream_t st = c->stream;
+    GE_CHECK(c, cudaMemcpyAsync(s.x + off, x, B, cudaMemcpyHostToDevice, st));
+    GE_CHECK(c, cudaMemcpyAsync(s.y + off, y, B, cudaMemcpyHostToDevice, st));
+    GE_CHECK(c, cudaMemcpyAsync(s.vx + off, vx, B, cudaMemcpyHostToDevice, st));
+    GE_CHECK(c, cudaMemcpyAsync(s.vy + off, vy, B, cudaMemcpyHostToDevice, st));
+    GE_CHECK(c, cudaMemcpyAsync(s.m + off, m, B, cudaMemcpyHostToDevice, st));
+    if (D == 3) {
+        GE_CHECK(c, cudaMemcpyAsync(s.z + off, z, B, cudaMemcpyHostToDevice, st));
+        GE_CHECK(c, cudaMemcpyAsync(s.vz + off, vz, B, cudaMemcpyHostToDevice, st));
+    }
+    if (ax) GE_CHECK(c, cudaMemcpyAsync(s.ax + off, ax, B, cudaMemcpyHostToDevice, st));
+    else GE_CHECK(c, cudaMemsetAsync(s.ax + off, 0, B, st));
+    if (ay) GE_CHECK(c, cudaMemcpyAsync(s.ay + off, ay, B, cudaMemcpyHostToDevice, st));
+    else GE_CHECK(c, cudaMemsetAsync(s.ay + off, 0, B, st));
+    if (D == 3) {
+        if (az) GE_CHECK(c, cudaMemcpyAsync(s.az + off, az, B, cudaMemcpyHostToDevice, st));
+        else GE_CHECK(c, cudaMemsetAsync(s.az + off, 0, B, st));
+    }
+    if (id) {
+        GE_CHECK(c, cudaMemcpyAsync(s.id + off, id, sizeof(uint32_t) * (size_t)n,
+                                    cudaMemcpyHostToDevice, st));
+        GE_CHECK(c, cudaStreamSynchronize(st));
+    } else {
+        std::vector<uint32_t> iota((size_t)n);
+        for (int64_t i = 0; i < n; i++) iota[(size_t)i] = (uint32_t)i;
+        GE_CHECK(c, cudaMemcpyAsync(s.id + off, iota.data(), sizeof(uint32_t) * (size_t)n,
+                                    cudaMemcpyHostToDevice, st));
+        GE_CHECK(c, cudaStreamSynchronize(st));
+    }
+    if (c->b.prev) {
+        GE_CHECK(c, cudaMemcpyAsync(s.pvx + off, s.vx + off, B, cudaMemcpyDeviceToDevice, st));
+        GE_CHECK(c, cudaMemcpyAsync(s.pvy + off, s.vy + off, B, cudaMemcpyDeviceToDevice, st));
+        if (D == 3)
+            GE_CHECK(c, cudaMemcpyAsync(s.pvz + off, s.vz + off, B, cudaMemcpyDeviceToDevice, st));
+    }
+    if (c->b.pinned) GE_CHECK(c, cudaMemsetAsync(s.pinned + off, 0, (size_t)n, st));
+    return GE_OK;
+}
+
+// Particles [off, off + n) of the current state into host arrays.
+int get_host(ge_ctx *c, int64_t off, int64_t n, float *x, float *y, float *z, float *vx,
+             float *vy, float *vz, float *ax, float *ay, float *az, float *m, uint32_t *id) {
+    const State &s = c->b.st[c->cur];
+    const size_t B = sizeof(float) * (size_t)n;
+    const bool d3 = c->p.dims == 3;
+    struct { void *h; const void *d; size_t b; } cp[] = {
+        {x, s.x + off, B}, {y, s.y + off, B}, {d3 ? z : nullptr, d3 ? s.z + off : nullptr, B},
+        {vx, s.vx + off, B}, {vy, s.vy + off, B}, {d3 ? vz : nullptr, d3 ? s.vz + off : nullptr, B},
+        {ax, s.ax + off, B}, {ay, s.ay + off, B}, {d3 ? az : nullptr, d3 ? s.az + off : nullptr, B},
+        {m, s.m + off, B}, {id, s.id + off, sizeof(uint32_t) * (size_t)n}};
+    for (auto &q : cp)
+        if (q.h) GE_CHECK(c, cudaMemcpyAsync(q.h, q.d, q.b, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    return GE_OK;
+}
+
+int find_sim(ge_ctx *c, int32_t handle) {
+    for (size_t k = 0; k < c->sims.size(); k++)
+        if (c->sims[k].handle == handle) return (int)k;
+    return -1;
 }
 
 }  // namespace
@@ -358,6 +627,8 @@ int ge_create(const ge_params *p, ge_ctx **out) {
     return GE_OK;
 }
 
+int ge_batch_create(const ge_params *p, ge_ctx **out) { return ge_create(p, out); }
+
 int ge_destroy(ge_ctx *c) {
     if (!c) return GE_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -375,13 +646,12 @@ int ge_set_params(ge_ctx *c, const ge_params *p) {
     if (!c) return GE_ERR_ARG;
     int rc = validate(c, p);
     if (rc) return rc;
-    if (p->dims != c->p.dims && c->cap_n) {
+    if (p->dims != c->p.dims && c->b.cap_n) {
         GE_CHECK(c, cudaStreamSynchronize(c->stream));
         free_buffers(c);
-        c->n = 0;
     }
-    const bool realloc = c->cap_n && (p->node_cap_factor != c->p.node_cap_factor ||
-                                      (p->track_prev_vel != 0) != c->has_prev);
+    const bool realloc = c->b.cap_n && (p->node_cap_factor != c->p.node_cap_factor ||
+                                        (p->track_prev_vel != 0) != c->b.prev);
     if (realloc) return fail(c, GE_ERR_STATE, "node_cap_factor / track_prev_vel change needs a new upload");
     c->p = *p;
     return GE_OK;
@@ -424,52 +694,15 @@ int ge_upload(ge_ctx *c, int64_t n, const float *x, const float *y, const float 
               const float *vx, const float *vy, const float *vz, const float *m,
               const uint32_t *id, const float *ax, const float *ay, const float *az) {
     if (!c) return GE_ERR_ARG;
-    const int D = c->p.dims;
-    if (n < 1) return fail(c, GE_ERR_ARG, "n must be >= 1");
-    if (!x || !y || !vx || !vy || !m || (D == 3 && (!z || !vz)))
-        return fail(c, GE_ERR_ARG, "positions, velocities and masses are required");
-    int rc = ensure_capacity(c, n);
+    int rc = check_host_arrays(c, n, x, y, z, vx, vy, vz, m);
     if (rc) return rc;
-    c->n = n;
+    if ((rc = ensure_capacity(c, n, 1, false))) return rc;
     c->cur = 0;
     c->has_pinned = false;
-    State &s = c->st[0];
-    const size_t B = sizeof(float) * (size_t)n;
-    cudaStream_t st = c->stream;
-    GE_CHECK(c, cudaMemcpyAsync(s.x, x, B, cudaMemcpyHostToDevice, st));
-    GE_CHECK(c, cudaMemcpyAsync(s.y, y, B, cudaMemcpyHostToDevice, st));
-    GE_CHECK(c, cudaMemcpyAsync(s.vx, vx, B, cudaMemcpyHostToDevice, st));
-    GE_CHECK(c, cudaMemcpyAsync(s.vy, vy, B, cudaMemcpyHostToDevice, st));
-    GE_CHECK(c, cudaMemcpyAsync(s.m, m, B, cudaMemcpyHostToDevice, st));
-    if (D == 3) {
-        GE_CHECK(c, cudaMemcpyAsync(s.z, z, B, cudaMemcpyHostToDevice, st));
-        GE_CHECK(c, cudaMemcpyAsync(s.vz, vz, B, cudaMemcpyHostToDevice, st));
-    }
-    if (ax) GE_CHECK(c, cudaMemcpyAsync(s.ax, ax, B, cudaMemcpyHostToDevice, st));
-    else GE_CHECK(c, cudaMemsetAsync(s.ax, 0, B, st));
-    if (ay) GE_CHECK(c, cudaMemcpyAsync(s.ay, ay, B, cudaMemcpyHostToDevice, st));
-    else GE_CHECK(c, cudaMemsetAsync(s.ay, 0, B, st));
-    if (D == 3) {
-        if (az) GE_CHECK(c, cudaMemcpyAsync(s.az, az, B, cudaMemcpyHostToDevice, st));
-        else GE_CHECK(c, cudaMemsetAsync(s.az, 0, B, st));
-    }
-    if (id) {
-        GE_CHECK(c, cudaMemcpyAsync(s.id, id, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
-    } else {
-        std::vector<uint32_t> iota((size_t)n);
-        for (int64_t i = 0; i < n; i++) iota[(size_t)i] = (uint32_t)i;
-        GE_CHECK(c, cudaMemcpyAsync(s.id, iota.data(), sizeof(uint32_t) * (size_t)n,
-                                    cudaMemcpyHostToDevice, st));
-        GE_CHECK(c, cudaStreamSynchronize(st));
-    }
-    if (c->has_prev) {
-        GE_CHECK(c, cudaMemcpyAsync(s.pvx, s.vx, B, cudaMemcpyDeviceToDevice, st));
-        GE_CHECK(c, cudaMemcpyAsync(s.pvy, s.vy, B, cudaMemcpyDeviceToDevice, st));
-        if (D == 3) GE_CHECK(c, cudaMemcpyAsync(s.pvz, s.vz, B, cudaMemcpyDeviceToDevice, st));
-    }
-    c->tree_valid = false;
-    c->keys_valid = false;
-    return GE_OK;
+    if ((rc = put_host(c, 0, n, x, y, z, vx, vy, vz, m, id, ax, ay, az))) return rc;
+    c->n = n;
+    c->sims.assign(1, SimRec{c->next_handle++, n, c->total_steps});
+    return sync_segments(c);
 }
 
 int ge_upload_pinned(ge_ctx *c, const uint8_t *pinned) {
@@ -479,12 +712,14 @@ int ge_upload_pinned(ge_ctx *c, const uint8_t *pinned) {
         c->has_pinned = false;
         return GE_OK;
     }
-    if (!c->st[0].pinned) {
-        GE_CHECK(c, dalloc(c, &c->st[0].pinned, (size_t)c->cap_n));
-        GE_CHECK(c, dalloc(c, &c->st[1].pinned, (size_t)c->cap_n));
+    if (!c->b.pinned) {
+        for (int k = 0; k < 2; k++)
+            GE_CHECK(c, dalloc(c->b.allocs, &c->b.st[k].pinned, (size_t)c->b.cap_n));
+        c->b.pinned = true;
     }
-    GE_CHECK(c, cudaMemcpyAsync(c->st[c->cur].pinned, pinned, (size_t)c->n, cudaMemcpyHostToDevice,
-                                c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(c->b.st[c->cur].pinned, pinned, (size_t)c->n,
+                                cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
     c->has_pinned = true;
     return GE_OK;
 }
@@ -493,25 +728,14 @@ int ge_download(ge_ctx *c, float *x, float *y, float *z, float *vx, float *vy, f
                 float *ax, float *ay, float *az, float *m, uint32_t *id) {
     int rc = require_state(c);
     if (rc) return rc;
-    const State &s = c->st[c->cur];
-    const size_t B = sizeof(float) * (size_t)c->n;
-    cudaStream_t st = c->stream;
-    const bool d3 = c->p.dims == 3;
-    struct { void *h; const void *d; size_t b; } cp[] = {
-        {x, s.x, B}, {y, s.y, B}, {d3 ? z : nullptr, s.z, B}, {vx, s.vx, B}, {vy, s.vy, B},
-        {d3 ? vz : nullptr, s.vz, B}, {ax, s.ax, B}, {ay, s.ay, B}, {d3 ? az : nullptr, s.az, B},
-        {m, s.m, B}, {id, s.id, sizeof(uint32_t) * (size_t)c->n}};
-    for (auto &q : cp)
-        if (q.h) GE_CHECK(c, cudaMemcpyAsync(q.h, q.d, q.b, cudaMemcpyDeviceToHost, st));
-    GE_CHECK(c, cudaStreamSynchronize(st));
-    return GE_OK;
+    return get_host(c, 0, c->n, x, y, z, vx, vy, vz, ax, ay, az, m, id);
 }
 
 int ge_download_prev_vel(ge_ctx *c, float *pvx, float *pvy, float *pvz) {
     int rc = require_state(c);
     if (rc) return rc;
-    if (!c->has_prev) return fail(c, GE_ERR_STATE, "track_prev_vel is off");
-    const State &s = c->st[c->cur];
+    if (!c->b.prev) return fail(c, GE_ERR_STATE, "track_prev_vel is off");
+    const State &s = c->b.st[c->cur];
     const size_t B = sizeof(float) * (size_t)c->n;
     if (pvx) GE_CHECK(c, cudaMemcpyAsync(pvx, s.pvx, B, cudaMemcpyDeviceToHost, c->stream));
     if (pvy) GE_CHECK(c, cudaMemcpyAsync(pvy, s.pvy, B, cudaMemcpyDeviceToHost, c->stream));
@@ -535,14 +759,17 @@ int ge_step(ge_ctx *c, int32_t nsteps) {
     cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
     c->stats.ms_last_step = ms / (float)nsteps;
     c->stats.steps += nsteps;
+    c->total_steps += nsteps;
     c->tree_valid = rc == GE_OK;
     if (rc == GE_OK && c->count_inter) {
         unsigned long long v = 0;
-        GE_CHECK(c, cudaMemcpy(&v, c->d_inter, sizeof(v), cudaMemcpyDeviceToHost));
+        GE_CHECK(c, cudaMemcpy(&v, c->b.d_inter, sizeof(v), cudaMemcpyDeviceToHost));
         c->stats.interactions = v;
     }
     return rc;
 }
+
+int ge_batch_step(ge_ctx *c, int32_t nsteps) { return ge_step(c, nsteps); }
 
 int ge_profile_step(ge_ctx *c) {
     int rc = require_state(c);
@@ -553,6 +780,7 @@ int ge_profile_step(ge_ctx *c) {
         cudaEventElapsedTime(&c->stats.stage_ms[k], c->ev[k], c->ev[k + 1]);
     cudaEventElapsedTime(&c->stats.stage_ms[6], c->ev[0], c->ev[6]);
     c->stats.steps += 1;
+    c->total_steps += 1;
     c->tree_valid = true;
     return GE_OK;
 }
@@ -581,7 +809,7 @@ int ge_bounding_box(ge_ctx *c, float *out) {
     if (rc) return rc;
     if ((rc = enqueue_bbox(c, false))) return rc;
     float4 bb;
-    GE_CHECK(c, cudaMemcpyAsync(&bb, c->ss.bbox, sizeof(bb), cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(&bb, c->g.box, sizeof(bb), cudaMemcpyDeviceToHost, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     float v[4] = {bb.x, bb.y, bb.z, bb.w};
     if (c->p.dims == 2) { v[2] = bb.w; v[3] = 0.0f; }
@@ -600,7 +828,7 @@ int ge_compute_morton_keys(ge_ctx *c, uint64_t *keys_out) {
         uint64_t *tmp = nullptr;
         GE_CHECK(c, cudaMallocAsync((void **)&tmp, sizeof(uint64_t) * (size_t)c->n, c->stream));
         // keys of the current order: the packed words hold them above bit 28 in 2D
-        GE_CHECK(c, launch_keys_out(c->p.dims, (int)c->n, c->ss, tmp, c->stream));
+        GE_CHECK(c, launch_keys_out(c->p.dims, (int)c->n, c->b.ss, tmp, c->stream));
         GE_CHECK(c, cudaMemcpyAsync(keys_out, tmp, sizeof(uint64_t) * (size_t)c->n,
                                     cudaMemcpyDeviceToHost, c->stream));
         GE_CHECK(c, cudaFreeAsync(tmp, c->stream));
@@ -613,13 +841,14 @@ int ge_sort_by_morton_key(ge_ctx *c, uint32_t *perm_out) {
     int rc = require_state(c);
     if (rc) return rc;
     if (!c->keys_valid) return fail(c, GE_ERR_STATE, "compute the Morton keys first");
-    if ((rc = enqueue_sort_permute(c, true))) return rc;
+    if ((rc = enqueue_sort(c))) return rc;
+    if ((rc = enqueue_permute(c, true))) return rc;
     c->keys_valid = false;
     c->tree_valid = false;
     if (perm_out) {
         uint32_t *tmp = nullptr;
         GE_CHECK(c, cudaMallocAsync((void **)&tmp, sizeof(uint32_t) * (size_t)c->n, c->stream));
-        GE_CHECK(c, launch_perm_out(c->p.dims, (int)c->n, c->ss, tmp, c->stream));
+        GE_CHECK(c, launch_perm_out(c->p.dims, (int)c->n, c->b.ss, tmp, c->stream));
         GE_CHECK(c, cudaMemcpyAsync(perm_out, tmp, sizeof(uint32_t) * (size_t)c->n,
                                     cudaMemcpyDeviceToHost, c->stream));
         GE_CHECK(c, cudaFreeAsync(tmp, c->stream));
@@ -630,7 +859,7 @@ int ge_sort_by_morton_key(ge_ctx *c, uint32_t *perm_out) {
 int ge_build_tree(ge_ctx *c) {
     int rc = require_state(c);
     if (rc) return rc;
-    if ((rc = enqueue_bbox(c, false))) return rc;   // seeds the root cell
+    if ((rc = enqueue_bbox(c, false))) return rc;   // seeds the root cells
     if ((rc = enqueue_build(c))) return rc;
     rc = check_device(c);
     c->tree_valid = rc == GE_OK;
@@ -645,7 +874,7 @@ int ge_compute_forces(ge_ctx *c) {
     rc = check_device(c);
     if (rc == GE_OK && c->count_inter) {
         unsigned long long v = 0;
-        GE_CHECK(c, cudaMemcpy(&v, c->d_inter, sizeof(v), cudaMemcpyDeviceToHost));
+        GE_CHECK(c, cudaMemcpy(&v, c->b.d_inter, sizeof(v), cudaMemcpyDeviceToHost));
         c->stats.interactions = v;
     }
     return rc;
@@ -669,23 +898,32 @@ int ge_direct_sum_f64(ge_ctx *c, int64_t nt, const uint32_t *idx, double *ax, do
     for (int64_t k = 0; k < nt; k++)
         if ((int64_t)idx[k] >= c->n) return fail(c, GE_ERR_ARG, "sample index out of range");
     const int D = c->p.dims;
+    // targets in ascending slot order, so each block's targets share a segment
+    std::vector<int64_t> ord((size_t)nt);
+    for (int64_t k = 0; k < nt; k++) ord[(size_t)k] = k;
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](int64_t a, int64_t b) { return idx[a] < idx[b]; });
+    std::vector<uint32_t> sidx((size_t)nt);
+    for (int64_t k = 0; k < nt; k++) sidx[(size_t)k] = idx[ord[(size_t)k]];
     uint32_t *d_idx = nullptr;
     double *d_out = nullptr;
     GE_CHECK(c, cudaMallocAsync((void **)&d_idx, sizeof(uint32_t) * nt, c->stream));
     GE_CHECK(c, cudaMallocAsync((void **)&d_out, sizeof(double) * nt * D, c->stream));
-    GE_CHECK(c, cudaMemcpyAsync(d_idx, idx, sizeof(uint32_t) * nt, cudaMemcpyHostToDevice, c->stream));
-    GE_CHECK(c, launch_direct_f64(D, cur_state(c), (int)c->n, d_idx, (int)nt, (double)c->p.G,
-                                  (double)c->p.eps2, d_out, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(d_idx, sidx.data(), sizeof(uint32_t) * nt, cudaMemcpyHostToDevice,
+                                c->stream));
+    GE_CHECK(c, launch_direct_f64(D, cur_state(c), (int)c->n, c->g, d_idx, (int)nt,
+                                  (double)c->p.G, (double)c->p.eps2, d_out, c->stream));
     std::vector<double> h((size_t)(nt * D));
     GE_CHECK(c, cudaMemcpyAsync(h.data(), d_out, sizeof(double) * nt * D, cudaMemcpyDeviceToHost,
                                 c->stream));
     GE_CHECK(c, cudaFreeAsync(d_idx, c->stream));
     GE_CHECK(c, cudaFreeAsync(d_out, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
-    for (int64_t k = 0; k < nt; k++) {
-        ax[k] = h[(size_t)(k * D)];
-        ay[k] = h[(size_t)(k * D + 1)];
-        if (D == 3 && az) az[k] = h[(size_t)(k * D + 2)];
+    for (int64_t r = 0; r < nt; r++) {
+        const int64_t k = ord[(size_t)r];
+        ax[k] = h[(size_t)(r * D)];
+        ay[k] = h[(size_t)(r * D + 1)];
+        if (D == 3 && az) az[k] = h[(size_t)(r * D + 2)];
     }
     return GE_OK;
 }
@@ -695,9 +933,9 @@ int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
     if (rc) return rc;
     if (!count || (cap > 0 && !ns)) return fail(c, GE_ERR_ARG, "bad timeline buffers");
     uint32_t m[8];
-    GE_CHECK(c, cudaMemcpyAsync(m, c->tree.meta, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(m, c->b.tree.meta, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
     unsigned long long tl[kTimeline];
-    GE_CHECK(c, cudaMemcpyAsync(tl, c->tree.tl, sizeof(tl), cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(tl, c->b.tree.tl, sizeof(tl), cudaMemcpyDeviceToHost, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     const int32_t k = (int32_t)(m[7] < (uint32_t)kTimeline ? m[7] : kTimeline);
     *count = k;
@@ -718,6 +956,81 @@ int ge_sums_f64(ge_ctx *c, double *out) {
     return GE_OK;
 }
 
+// --- batched simulations ------------------------------------------------
+
+int ge_batch_add_sim(ge_ctx *c, int64_t n, const float *x, const float *y, const float *z,
+                     const float *vx, const float *vy, const float *vz, const float *m,
+                     const uint32_t *id, int32_t *sim) {
+    if (!c) return GE_ERR_ARG;
+    int rc = check_host_arrays(c, n, x, y, z, vx, vy, vz, m);
+    if (rc) return rc;
+    if (c->next_handle == INT32_MAX) return fail(c, GE_ERR_CAPACITY, "simulation handles exhausted");
+    const int64_t old_n = c->n;
+    if ((rc = ensure_capacity(c, old_n + n, (int64_t)c->sims.size() + 1, true))) return rc;
+    if ((rc = put_host(c, old_n, n, x, y, z, vx, vy, vz, m, id, nullptr, nullptr, nullptr)))
+        return rc;
+    const int32_t h = c->next_handle++;
+    c->sims.push_back(SimRec{h, n, c->total_steps});
+    c->n = old_n + n;
+    if ((rc = sync_segments(c))) {
+        c->sims.pop_back();
+        c->n = old_n;
+        sync_segments(c);
+        return rc;
+    }
+    if (sim) *sim = h;
+    return GE_OK;
+}
+
+int ge_batch_remove_sim(ge_ctx *c, int32_t sim) {
+    if (!c) return GE_ERR_ARG;
+    const int r = find_sim(c, sim);
+    if (r < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    const int64_t lo = c->h_off[(size_t)r], hi = c->h_off[(size_t)r + 1];
+    const int64_t n = c->n;
+    if (hi - lo < n) {
+        // the simulations after it move down by its size (through the other
+        // state buffer, so no copy overlaps itself)
+        const State &src = c->b.st[c->cur];
+        const State &dst = c->b.st[c->cur ^ 1];
+        int rc = copy_range(c, dst, 0, src, 0, lo, c->b.prev, c->b.pinned);
+        if (!rc) rc = copy_range(c, dst, lo, src, hi, n - hi, c->b.prev, c->b.pinned);
+        if (rc) return rc;
+        c->cur ^= 1;
+    }
+    c->sims.erase(c->sims.begin() + r);
+    c->n = n - (hi - lo);
+    return sync_segments(c);
+}
+
+int ge_batch_list(ge_ctx *c, int32_t cap, int32_t *sims, int32_t *count) {
+    if (!c || !count) return GE_ERR_ARG;
+    *count = (int32_t)c->sims.size();
+    if (sims)
+        for (int32_t k = 0; k < cap && k < *count; k++) sims[k] = c->sims[(size_t)k].handle;
+    return GE_OK;
+}
+
+int ge_batch_query(ge_ctx *c, int32_t sim, int64_t *n, int64_t *offset, int64_t *steps) {
+    if (!c) return GE_ERR_ARG;
+    const int r = find_sim(c, sim);
+    if (r < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    if (n) *n = c->sims[(size_t)r].n;
+    if (offset) *offset = c->h_off[(size_t)r];
+    if (steps) *steps = c->total_steps - c->sims[(size_t)r].step0;
+    return GE_OK;
+}
+
+int ge_batch_download_sim(ge_ctx *c, int32_t sim, float *x, float *y, float *z, float *vx,
+                          float *vy, float *vz, float *ax, float *ay, float *az, float *m,
+                          uint32_t *id) {
+    if (!c) return GE_ERR_ARG;
+    const int r = find_sim(c, sim);
+    if (r < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    return get_host(c, c->h_off[(size_t)r], c->sims[(size_t)r].n, x, y, z, vx, vy, vz, ax, ay, az,
+                    m, id);
+}
+
 int ge_export_tree(ge_ctx *c, int64_t cap, int64_t *count, float *pos, float *size, float *com,
                    float *mass, uint32_t *start, uint32_t *end, uint32_t *next,
                    uint32_t *child) {
@@ -733,18 +1046,23 @@ int ge_export_tree(ge_ctx *c, int64_t cap, int64_t *count, float *pos, float *si
     const int64_t ns = c->slots > nn ? c->slots : nn;
     std::vector<float4> w((size_t)ns), cell((size_t)ns);
     std::vector<uint4> inf((size_t)ns);
-    GE_CHECK(c, cudaMemcpy(w.data(), c->tree.walk, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
-    GE_CHECK(c, cudaMemcpy(cell.data(), c->tree.cell, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
-    GE_CHECK(c, cudaMemcpy(inf.data(), c->tree.info, sizeof(uint4) * ns, cudaMemcpyDeviceToHost));
+    const Tree &t = c->b.tree;
+    GE_CHECK(c, cudaMemcpy(w.data(), t.walk, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
+    GE_CHECK(c, cudaMemcpy(cell.data(), t.cell, sizeof(float4) * ns, cudaMemcpyDeviceToHost));
+    GE_CHECK(c, cudaMemcpy(inf.data(), t.info, sizeof(uint4) * ns, cudaMemcpyDeviceToHost));
     // depth-first pre-order numbering, children in slot order (the reference's
-    // emission order, quadtree.cpp:67-87); next = number of descendants
+    // emission order, quadtree.cpp:67-87), the simulations' roots (slots
+    // 0..S-1) one after another; next = number of descendants
     std::vector<uint32_t> order;
     order.reserve((size_t)nn);
-    std::vector<uint32_t> stack{0u};
+    std::vector<uint32_t> stack;
+    for (int r = c->g.S - 1; r >= 0; --r) stack.push_back((uint32_t)r);
     std::vector<uint32_t> newid((size_t)ns, kEmpty);
     while (!stack.empty()) {
         uint32_t k = stack.back();
         stack.pop_back();
+        if ((int64_t)order.size() >= nn || k >= (uint32_t)ns)
+            return fail(c, GE_ERR_STATE, "tree is not consistent");
         newid[k] = (uint32_t)order.size();
         order.push_back(k);
         const uint32_t mask = inf[k].y;

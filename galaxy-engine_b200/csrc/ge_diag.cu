@@ -14,23 +14,34 @@ constexpr int kDiagThreads = 256;
 
 template <int D>
 __global__ void __launch_bounds__(kDiagThreads)
-k_direct_f64(State s, int n, const uint32_t *__restrict__ idx, int nt, double G, double eps2,
-             double *__restrict__ out) {
+k_direct_f64(State s, int n, Segs g, const uint32_t *__restrict__ idx, int nt, double G,
+             double eps2, double *__restrict__ out) {
     __shared__ float4 tile[kDiagThreads];
+    __shared__ uint32_t s_lo, s_hi;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const bool ok = t < nt;
     uint32_t i = ok ? idx[t] : 0u;
     if (i >= (uint32_t)n) i = 0u;
+    // sources: the target's own segment; the block walks the union of its
+    // targets' segments
+    const uint32_t sg = g.seg_of ? g.seg_of[i] : 0u;
+    const uint32_t lo = seg_lo(g, sg), hi = seg_hi(g, sg, (uint32_t)n);
+    if (threadIdx.x == 0) { s_lo = 0xFFFFFFFFu; s_hi = 0u; }
+    __syncthreads();
+    if (ok) { atomicMin(&s_lo, lo); atomicMax(&s_hi, hi); }
+    __syncthreads();
+    const int blo = (int)s_lo, bhi = (int)s_hi;
     const double xi = s.x[i], yi = s.y[i], zi = D == 3 ? (double)s.z[i] : 0.0;
     double a[3] = {0.0, 0.0, 0.0};
-    for (int base = 0; base < n; base += kDiagThreads) {
+    for (int base = blo; base < bhi; base += kDiagThreads) {
         const int j = base + threadIdx.x;
         __syncthreads();
-        if (j < n) tile[threadIdx.x] = make_float4(s.x[j], s.y[j], D == 3 ? s.z[j] : 0.0f, s.m[j]);
+        if (j < bhi) tile[threadIdx.x] = make_float4(s.x[j], s.y[j], D == 3 ? s.z[j] : 0.0f, s.m[j]);
         __syncthreads();
-        const int cnt = min(kDiagThreads, n - base);
+        const int cnt = min(kDiagThreads, bhi - base);
         for (int k = 0; k < cnt; k++) {
-            if ((uint32_t)(base + k) == i) continue;
+            const uint32_t jj = (uint32_t)(base + k);
+            if (jj == i || jj < lo || jj >= hi) continue;
             const float4 q = tile[k];
             const double dx = (double)q.x - xi, dy = (double)q.y - yi;
             const double dz = D == 3 ? (double)q.z - zi : 0.0;
@@ -49,12 +60,13 @@ k_direct_f64(State s, int n, const uint32_t *__restrict__ idx, int nt, double G,
     }
 }
 
-cudaError_t launch_direct_f64(int dims, const State &s, int n, const uint32_t *idx, int nt,
-                              double G, double eps2, double *out, cudaStream_t st) {
+cudaError_t launch_direct_f64(int dims, const State &s, int n, const Segs &g, const uint32_t *idx,
+                              int nt, double G, double eps2, double *out, cudaStream_t st) {
     const int blocks = (nt + kDiagThreads - 1) / kDiagThreads;
     if (blocks < 1) return cudaSuccess;
-    if (dims == 2) k_direct_f64<2><<<blocks, kDiagThreads, 0, st>>>(s, n, idx, nt, G, eps2, out);
-    else k_direct_f64<3><<<blocks, kDiagThreads, 0, st>>>(s, n, idx, nt, G, eps2, out);
+    if (dims == 2)
+        k_direct_f64<2><<<blocks, kDiagThreads, 0, st>>>(s, n, g, idx, nt, G, eps2, out);
+    else k_direct_f64<3><<<blocks, kDiagThreads, 0, st>>>(s, n, g, idx, nt, G, eps2, out);
     return cudaGetLastError();
 }
 

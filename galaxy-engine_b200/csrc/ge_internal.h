@@ -66,18 +66,38 @@ struct Tree {
     int64_t cap;
 };
 
-// Scratch for bounding box, keys and sort.
+// Independent simulations ("segments") stepped together: the particles of
+// segment s occupy [off[s], off[s+1]) of the state arrays and never leave it;
+// boxes, keys, the sort, the trees and the walks never mix segments.  With a
+// single segment the arrays may be null (segment 0 = all particles).
+struct Segs {
+    int S;
+    const uint32_t *off;        // [S + 1]
+    const uint32_t *seg_of;     // [n] segment of each particle slot
+    const uint32_t *tile_base;  // [S + 1] first sort tile of each segment
+    const uint32_t *tile_seg;   // [tiles] segment of each sort tile
+    int64_t tiles;              // sort tiles over all segments
+    float4 *box;                // [S] root boxes {x, y, z, size}
+    uint32_t *boxmm;            // [S * 6] order-preserving min/max words
+    uint32_t *root_begin;       // [S] walk entry of each root
+    uint32_t *root_end;         // [S] end of each root's walk
+};
+
+__host__ __device__ __forceinline__ uint32_t seg_lo(const Segs &g, uint32_t s) {
+    return g.off ? g.off[s] : 0u;
+}
+__host__ __device__ __forceinline__ uint32_t seg_hi(const Segs &g, uint32_t s, uint32_t n) {
+    return g.off ? g.off[s + 1] : n;
+}
+
+// Scratch for keys and sort.
 struct SortScratch {
     uint64_t *keys[2];     // 2D: (key << 28 | index) packed; 3D: keys
     uint32_t *vals[2];     // 3D: indices
-    uint32_t *hist;        // [8][256] per-pass digit counts
-    uint32_t *status;      // [8][tiles][256] decoupled look-back words
+    uint32_t *hist;        // [passes][S][256] per-segment digit counts
+    uint32_t *status;      // [passes][tiles][256] decoupled look-back words
     uint32_t *tile_ctr;    // [8]
-    int64_t tiles;
-    float4 *bbox_part;     // per-block min/max partials (2 float4 per block)
-    uint32_t *bbox_ctr;    // [1]
-    float4 *bbox;          // [1] {x, y, z, size}
-    int bbox_blocks;
+    int box_blocks;        // grid of the kick/box kernel
 };
 
 struct StepParams {
@@ -95,14 +115,27 @@ constexpr int kSortTile = 4096;   // keys per look-back tile (256 threads x 16)
 constexpr int kTimeline = 256;    // build timeline entries
 
 // --- launchers (each runs on `st`) ----------------------------------------
-// integrateStart (kick + drift) fused with the bounding-box reduction; the
-// last block finalises the root box and seeds the root node.
+// integrateStart (kick + drift) fused with the per-segment bounding-box
+// reduction; a second small kernel applies the reference's box formula per
+// segment and seeds each segment's root node.
 cudaError_t launch_kick_drift_bbox(int dims, const State &s, const StepParams &p, bool kick_drift,
-                                   SortScratch &ss, Tree &t, uint32_t *err, cudaStream_t st);
-// Morton keys from the root box plus the digit histograms of every pass
-cudaError_t launch_keys(int dims, const State &s, int n, SortScratch &ss, cudaStream_t st);
-// all radix passes; leaves the sorted keys in ss.keys[0] (and vals[0])
-cudaError_t launch_sort(int dims, int n, SortScratch &ss, uint32_t *err, cudaStream_t st);
+                                   const Segs &g, SortScratch &ss, Tree &t, cudaStream_t st);
+// sets every segment's min/max words to their identities (needed once after
+// the words are allocated; the box kernel leaves them reset)
+cudaError_t launch_reset_boxes(const Segs &g, cudaStream_t st);
+// segment of every particle slot and of every sort tile, from the segment
+// offsets off [S + 1] and first tiles tile_base [S + 1]
+cudaError_t launch_seg_tables(const uint32_t *off, const uint32_t *tile_base, int S, int n,
+                              int64_t tiles, uint32_t *seg_of, uint32_t *tile_seg,
+                              cudaStream_t st);
+// Morton keys from each segment's root box plus the per-segment digit
+// histograms of every pass
+cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScratch &ss,
+                        cudaStream_t st);
+// all radix passes (stable within each segment); leaves the sorted keys in
+// ss.keys[0] (and vals[0])
+cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_t *err,
+                        cudaStream_t st);
 // gather of the state into `out` by the sorted order
 cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
                            const State &out, bool with_acc, cudaStream_t st);
@@ -114,16 +147,18 @@ cudaError_t launch_keys_out(int dims, int n, const SortScratch &ss, uint64_t *ke
 // tree build + mass/centre of mass + walk layout (one cooperative launch)
 int build_grid_blocks(int dims, int num_sms);
 int64_t build_node_slack(int dims, int num_sms);
-cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
-                         int num_sms, cudaStream_t st);
+cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Segs &g, Tree &t,
+                         uint32_t *err, int num_sms, cudaStream_t st);
 // tree walk; integrate_end fuses integrateEnd (v += a*dt/2)
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
-                        const Tree &t, bool integrate_end, unsigned long long *inter_count,
-                        uint32_t *err, cudaStream_t st);
+                        const Segs &g, const Tree &t, bool integrate_end,
+                        unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
 // FP64 diagnostics
-cudaError_t launch_direct_f64(int dims, const State &s, int n, const uint32_t *idx, int nt,
-                              double G, double eps2, double *out, cudaStream_t st);
+// (each target sums over its own segment only; idx sorted ascending keeps a
+// block's targets inside one or two segments)
+cudaError_t launch_direct_f64(int dims, const State &s, int n, const Segs &g, const uint32_t *idx,
+                              int nt, double G, double eps2, double *out, cudaStream_t st);
 cudaError_t launch_sums_f64(int dims, const State &s, int n, double *out, cudaStream_t st);
 
 }  // namespace ge

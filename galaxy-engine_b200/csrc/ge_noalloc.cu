@@ -5,7 +5,7 @@
 // fixed arena under its own accounting, or a frame loop that must not call
 // cudaMalloc / cudaFree (both can synchronise the whole device and stall
 // the frame).  They pass device buffers for the inputs and outputs; every
-// temporary the sort needs (box partials, packed keys in two ping-pong
+// temporary the sort needs (box min/max words, packed keys in two ping-pong
 // buffers, digit histograms, look-back words) lives in one file-scope
 // __device__ array of fixed size, which each GPU that loads the library
 // holds until the process exits.
@@ -24,7 +24,7 @@ namespace {
 
 constexpr int64_t kNoAllocMaxN = GE_NOALLOC_MAX_N;
 constexpr int64_t kNoAllocTiles = (kNoAllocMaxN + kSortTile - 1) / kSortTile;
-constexpr int kNoAllocBBoxBlocks = 256;
+constexpr int kNoAllocBoxBlocks = 148 * 4;
 
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // byte offsets inside the scratch array
@@ -33,10 +33,9 @@ constexpr size_t kOffKeys1 = kOffKeys0 + align256(sizeof(uint64_t) * kNoAllocMax
 constexpr size_t kOffHist = kOffKeys1 + align256(sizeof(uint64_t) * kNoAllocMaxN);
 constexpr size_t kOffStatus = kOffHist + align256(sizeof(uint32_t) * 8 * 256);
 constexpr size_t kOffTileCtr = kOffStatus + align256(sizeof(uint32_t) * 8 * kNoAllocTiles * 256);
-constexpr size_t kOffBBoxPart = kOffTileCtr + align256(sizeof(uint32_t) * 8);
-constexpr size_t kOffBBoxCtr = kOffBBoxPart + align256(sizeof(float4) * 2 * kNoAllocBBoxBlocks);
-constexpr size_t kOffBBox = kOffBBoxCtr + align256(sizeof(uint32_t));
-constexpr size_t kOffRootCell = kOffBBox + align256(sizeof(float4));
+constexpr size_t kOffBox = kOffTileCtr + align256(sizeof(uint32_t) * 8);
+constexpr size_t kOffBoxMM = kOffBox + align256(sizeof(float4));
+constexpr size_t kOffRootCell = kOffBoxMM + align256(sizeof(uint32_t) * 6);
 constexpr size_t kOffRootInfo = kOffRootCell + align256(sizeof(float4));
 constexpr size_t kOffErr = kOffRootInfo + align256(sizeof(uint4));
 constexpr size_t kScratchBytes = kOffErr + align256(sizeof(uint32_t));
@@ -87,13 +86,17 @@ extern "C" int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const floa
     ss.hist = (uint32_t *)(base + kOffHist);
     ss.status = (uint32_t *)(base + kOffStatus);
     ss.tile_ctr = (uint32_t *)(base + kOffTileCtr);
-    ss.tiles = kNoAllocTiles;
-    ss.bbox_part = (float4 *)(base + kOffBBoxPart);
-    ss.bbox_ctr = (uint32_t *)(base + kOffBBoxCtr);
-    ss.bbox = (float4 *)(base + kOffBBox);
-    int blocks = (int)((n + kBBoxThreads - 1) / kBBoxThreads);
-    ss.bbox_blocks = blocks < kNoAllocBBoxBlocks ? blocks : kNoAllocBBoxBlocks;
+    const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+    const int64_t blocks = tiles < kNoAllocBoxBlocks ? tiles : kNoAllocBoxBlocks;
+    ss.box_blocks = (int)blocks;
     uint32_t *err = (uint32_t *)(base + kOffErr);
+
+    // one segment: every particle belongs to it, so no segment tables
+    Segs g{};
+    g.S = 1;
+    g.tiles = tiles;
+    g.box = (float4 *)(base + kOffBox);
+    g.boxmm = (uint32_t *)(base + kOffBoxMM);
 
     Tree t{};
     t.cell = (float4 *)(base + kOffRootCell);   // the box kernel seeds a root node here
@@ -106,14 +109,15 @@ extern "C" int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const floa
     StepParams p{};
     p.n = (int)n;
 
-    // the array keeps the previous call's contents: zero what must start at zero
-    // (the key kernel clears the histograms' users, the look-back words and the
-    // tile counters itself)
-    if (cudaMemsetAsync(ss.bbox_ctr, 0, sizeof(uint32_t), st) != cudaSuccess) return GE_ERR_CUDA;
+    // the array keeps the previous call's contents (zero before the first):
+    // set what must start at a known value -- the min/max words and the error
+    // word; the key launch clears the histograms, look-back words and tile
+    // counters itself
+    if (launch_reset_boxes(g, st) != cudaSuccess) return GE_ERR_CUDA;
     if (cudaMemsetAsync(err, 0, sizeof(uint32_t), st) != cudaSuccess) return GE_ERR_CUDA;
-    if (launch_kick_drift_bbox(2, s, p, false, ss, t, err, st) != cudaSuccess) return GE_ERR_CUDA;
-    if (launch_keys(2, s, (int)n, ss, st) != cudaSuccess) return GE_ERR_CUDA;
-    if (launch_sort(2, (int)n, ss, err, st) != cudaSuccess) return GE_ERR_CUDA;
+    if (launch_kick_drift_bbox(2, s, p, false, g, ss, t, st) != cudaSuccess) return GE_ERR_CUDA;
+    if (launch_keys(2, s, (int)n, g, ss, st) != cudaSuccess) return GE_ERR_CUDA;
+    if (launch_sort(2, (int)n, g, ss, err, st) != cudaSuccess) return GE_ERR_CUDA;
     if (launch_perm_out(2, (int)n, ss, d_perm, st) != cudaSuccess) return GE_ERR_CUDA;
     if (d_keys && launch_keys_out(2, (int)n, ss, d_keys, st) != cudaSuccess) return GE_ERR_CUDA;
     uint32_t h_err = 0;

@@ -32,12 +32,19 @@ constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 3
 __host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 5 : 8; }
 __host__ __device__ constexpr int key_shift0(int dims) { return dims == 2 ? 28 : 0; }
 
+// Morton keys of every particle from its segment's root box, and the digit
+// histograms of every pass per segment.  Each block covers a contiguous chunk
+// of particles and accumulates in shared memory while its particles stay in
+// one segment (one flush per segment change); a warp that straddles segments
+// counts with global atomics instead.
 template <int D>
 __global__ void __launch_bounds__(256)
-k_keys(State s, int n, const float4 *bbox, uint64_t *keys, uint32_t *vals, uint32_t *hist,
+k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
        uint32_t *status, int64_t status_words, uint32_t *tile_ctr) {
     constexpr int P = key_passes(D), S0 = key_shift0(D);
     __shared__ uint32_t sh[P][kRadix];
+    const int lane = threadIdx.x & 31;
+    const size_t SH = (size_t)g.S * kRadix;   // stride of one pass in hist
     for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
     // clear the look-back status words for this step's passes
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < status_words;
@@ -45,31 +52,50 @@ k_keys(State s, int n, const float4 *bbox, uint64_t *keys, uint32_t *vals, uint3
         status[i] = 0u;
     if (blockIdx.x == 0 && threadIdx.x < 8) tile_ctr[threadIdx.x] = 0u;
     __syncthreads();
-    const float4 bb = *bbox;
-    float hx, hy, hz;
-    if (D == 2) {
-        float ext = bb.w > 1e-6f ? bb.w : 1e-6f;   // std::max(posSize.z, 1e-6f)
-        hx = fadd(bb.x, ext); hy = fadd(bb.y, ext); hz = 0.0f;
-    } else {
-        hx = fadd(bb.x, bb.w); hy = fadd(bb.y, bb.w); hz = fadd(bb.z, bb.w);
-    }
-    const int stride = gridDim.x * blockDim.x;
-    // iterate whole warps so that __match_any_sync sees full warps
-    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-        int i = base + threadIdx.x;
-        bool ok = i < n;
+    const int chunk = ((n + gridDim.x - 1) / gridDim.x + 255) & ~255;
+    const int c0 = blockIdx.x * chunk, c1 = min(c0 + chunk, n);
+    int cur = -1;   // segment the shared histogram belongs to (block-uniform)
+    for (int base = c0; base < c1; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const bool ok = i < c1;
+        const uint32_t sg = ok && g.seg_of ? g.seg_of[i] : 0u;
+        // one segment for the whole block tile?
+        const int tlast = min(base + (int)blockDim.x, c1) - 1;
+        const uint32_t s_first = g.seg_of ? g.seg_of[base] : 0u;
+        const uint32_t s_last = g.seg_of ? g.seg_of[tlast] : 0u;
+        const bool uni = s_first == s_last;
+        if (uni && (int)s_first != cur) {
+            __syncthreads();
+            if (cur >= 0)
+                for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) {
+                    const uint32_t c = (&sh[0][0])[k];
+                    if (c) atomicAdd(&hist[(k / kRadix) * SH + (size_t)cur * kRadix + (k % kRadix)], c);
+                }
+            __syncthreads();
+            for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) (&sh[0][0])[k] = 0;
+            __syncthreads();
+            cur = (int)s_first;
+        }
         uint64_t word = 0;
         if (ok) {
+            const float4 bb = g.box[sg];
+            float hx, hy, hz;
             if (D == 2) {
-                uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 262144.0f, 262143ull);
-                uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 262144.0f, 262143ull);
-                uint64_t key = spread2(ix) | (spread2(iy) << 1);
+                const float ext = bb.w > 1e-6f ? bb.w : 1e-6f;   // std::max(posSize.z, 1e-6f)
+                hx = fadd(bb.x, ext); hy = fadd(bb.y, ext); hz = 0.0f;
+            } else {
+                hx = fadd(bb.x, bb.w); hy = fadd(bb.y, bb.w); hz = fadd(bb.z, bb.w);
+            }
+            if (D == 2) {
+                const uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 262144.0f, 262143ull);
+                const uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 262144.0f, 262143ull);
+                const uint64_t key = spread2(ix) | (spread2(iy) << 1);
                 word = (key << 28) | (uint64_t)i;
                 keys[i] = word;
             } else {
-                uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 2097151.0f, 2097151ull);
-                uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 2097151.0f, 2097151ull);
-                uint64_t iz = scale_to_grid(s.z[i], bb.z, hz, 2097151.0f, 2097151ull);
+                const uint64_t ix = scale_to_grid(s.x[i], bb.x, hx, 2097151.0f, 2097151ull);
+                const uint64_t iy = scale_to_grid(s.y[i], bb.y, hy, 2097151.0f, 2097151ull);
+                const uint64_t iz = scale_to_grid(s.z[i], bb.z, hz, 2097151.0f, 2097151ull);
                 word = spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2);
                 keys[i] = word;
                 vals[i] = (uint32_t)i;
@@ -77,25 +103,33 @@ k_keys(State s, int n, const float4 *bbox, uint64_t *keys, uint32_t *vals, uint3
         }
 #pragma unroll
         for (int ps = 0; ps < P; ps++) {
-            uint32_t d = ok ? (uint32_t)((word >> (S0 + 8 * ps)) & 0xFFu) : 0x100u;
-            unsigned peers = __match_any_sync(0xffffffffu, d);
-            if (ok && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1))
-                atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
+            const uint32_t d = ok ? (uint32_t)((word >> (S0 + 8 * ps)) & 0xFFu) : 0x100u;
+            if (uni) {
+                const unsigned peers = __match_any_sync(0xffffffffu, d);
+                if (ok && lane == __ffs(peers) - 1) atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
+            } else {
+                const unsigned peers = __match_any_sync(0xffffffffu, ok ? (sg << 8) | d : 0xFFFFFFFFu);
+                if (ok && lane == __ffs(peers) - 1)
+                    atomicAdd(&hist[ps * SH + (size_t)sg * kRadix + d], (uint32_t)__popc(peers));
+            }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) {
-        uint32_t c = (&sh[0][0])[i];
-        if (c) atomicAdd(&hist[i], c);
-    }
+    if (cur >= 0)
+        for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) {
+            const uint32_t c = (&sh[0][0])[k];
+            if (c) atomicAdd(&hist[(k / kRadix) * SH + (size_t)cur * kRadix + (k % kRadix)], c);
+        }
 }
 
-// One stable counting pass over digit (word >> shift) & 255.
+// One stable counting pass over digit (word >> shift) & 255, segment by
+// segment: a tile belongs to one segment, its digit offsets start at the
+// segment's first slot, and look-back stops at the segment's first tile.
 template <bool PAIRS>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
              const uint32_t *__restrict__ vin, uint32_t *__restrict__ vout, int n, int shift,
-             const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
+             Segs g, const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
              uint32_t *err) {
     __shared__ uint32_t s_whist[kSortWarps][kRadix];
     __shared__ uint32_t s_off[kRadix];
@@ -104,38 +138,43 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
     for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&s_whist[0][0])[i] = 0u;
-    // exclusive scan of this pass's global digit counts (thread = digit)
-    uint32_t g = hist[tid];
-    uint32_t incl = g;
+    __syncthreads();
+    const int tile = (int)s_tile;
+    const uint32_t sg = g.tile_seg ? g.tile_seg[tile] : 0u;
+    const int tile0 = g.tile_base ? (int)g.tile_base[sg] : 0;
+    const uint32_t lo = seg_lo(g, sg), hi = seg_hi(g, sg, (uint32_t)n);
+    // exclusive scan of this segment's digit counts (thread = digit)
+    const uint32_t gcount = hist[(size_t)sg * kRadix + tid];
+    uint32_t incl = gcount;
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
     if (lane == 31) s_scan[w] = incl;
     __syncthreads();
     uint32_t wbase = 0;
     for (int ww = 0; ww < w; ww++) wbase += s_scan[ww];
-    const uint32_t gexcl = wbase + incl - g;
-    const int tile = (int)s_tile;
-    const int base = tile * kSortTile + w * 32 * kItems;
+    const uint32_t gexcl = lo + wbase + incl - gcount;
+    const uint32_t tstart = lo + (uint32_t)(tile - tile0) * kSortTile;
+    const int base = (int)tstart + w * 32 * kItems;
 
     uint64_t k[kItems];
     uint32_t v[kItems], rk[kItems], dg[kItems];
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
-        int idx = base + it * 32 + lane;
-        bool ok = idx < n;
+        const int idx = base + it * 32 + lane;
+        const bool ok = idx < (int)hi;
         k[it] = ok ? kin[idx] : 0ull;
         if (PAIRS) v[it] = ok ? vin[idx] : 0u;
         dg[it] = ok ? (uint32_t)((k[it] >> shift) & 0xFFu) : 0x100u;
     }
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
-        uint32_t d = dg[it];
-        unsigned peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t d = dg[it];
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
         uint32_t prev = 0;
-        int leader = __ffs(peers) - 1;
+        const int leader = __ffs(peers) - 1;
         if (d < 0x100u && lane == leader) {
             prev = s_whist[w][d];
             s_whist[w][d] = prev + (uint32_t)__popc(peers);
@@ -151,20 +190,20 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
         uint32_t sum = 0;
 #pragma unroll
         for (int ww = 0; ww < kSortWarps; ww++) {
-            uint32_t c = s_whist[ww][d];
+            const uint32_t c = s_whist[ww][d];
             s_whist[ww][d] = sum;
             sum += c;
         }
         volatile uint32_t *st = status;
         uint32_t excl = 0;
-        if (tile == 0) {
-            st[d] = kFlagInc | sum;
+        if (tile == tile0) {
+            st[(int64_t)tile * kRadix + d] = kFlagInc | sum;
         } else {
             st[(int64_t)tile * kRadix + d] = kFlagAgg | sum;
             int t = tile - 1;
             uint32_t spins = 0;
-            while (t >= 0) {
-                uint32_t word = st[(int64_t)t * kRadix + d];
+            while (t >= tile0) {
+                const uint32_t word = st[(int64_t)t * kRadix + d];
                 if ((word & ~kValMask) == 0u) {
                     if (++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
                     continue;
@@ -180,10 +219,10 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
-        uint32_t d = dg[it];
+        const uint32_t d = dg[it];
         if (d < 0x100u) {
-            uint32_t pos = s_off[d] + s_whist[w][d] + rk[it];
-            if (pos < (uint32_t)n) {   // always true unless a look-back wait gave up
+            const uint32_t pos = s_off[d] + s_whist[w][d] + rk[it];
+            if (pos < hi) {   // always true unless a look-back wait gave up
                 kout[pos] = k[it];
                 if (PAIRS) vout[pos] = v[it];
             }
@@ -229,35 +268,38 @@ static int grid_for(int n, int threads, int cap) {
     return b < 1 ? 1 : b;
 }
 
-cudaError_t launch_keys(int dims, const State &s, int n, SortScratch &ss, cudaStream_t st) {
-    int blocks = grid_for(n, 256, 148 * 8);
-    int64_t words = (int64_t)key_passes(dims) * ss.tiles * kRadix;
-    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * 8 * kRadix, st);
+cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScratch &ss,
+                        cudaStream_t st) {
+    const int blocks = grid_for(n, 256, 148 * 8);
+    const int64_t words = (int64_t)key_passes(dims) * g.tiles * kRadix;
+    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kRadix, st);
     if (e != cudaSuccess) return e;
     if (dims == 2)
-        k_keys<2><<<blocks, 256, 0, st>>>(s, n, ss.bbox, ss.keys[0], ss.vals[0], ss.hist,
-                                          ss.status, words, ss.tile_ctr);
+        k_keys<2><<<blocks, 256, 0, st>>>(s, n, g, ss.keys[0], ss.vals[0], ss.hist, ss.status,
+                                          words, ss.tile_ctr);
     else
-        k_keys<3><<<blocks, 256, 0, st>>>(s, n, ss.bbox, ss.keys[0], ss.vals[0], ss.hist,
-                                          ss.status, words, ss.tile_ctr);
+        k_keys<3><<<blocks, 256, 0, st>>>(s, n, g, ss.keys[0], ss.vals[0], ss.hist, ss.status,
+                                          words, ss.tile_ctr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sort(int dims, int n, SortScratch &ss, uint32_t *err, cudaStream_t st) {
+cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_t *err,
+                        cudaStream_t st) {
     const int P = key_passes(dims), S0 = key_shift0(dims);
-    const int tiles = (n + kSortTile - 1) / kSortTile;
+    const int tiles = (int)g.tiles;
     int cur = 0;
     for (int ps = 0; ps < P; ps++) {
-        uint32_t *status = ss.status + (int64_t)ps * ss.tiles * kRadix;
+        uint32_t *status = ss.status + (int64_t)ps * g.tiles * kRadix;
+        const uint32_t *hist = ss.hist + (size_t)ps * g.S * kRadix;
         if (dims == 2)
             k_radix_pass<false><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, S0 + 8 * ps,
-                ss.hist + ps * kRadix, status, ss.tile_ctr + ps, err);
+                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, S0 + 8 * ps, g, hist,
+                status, ss.tile_ctr + ps, err);
         else
             k_radix_pass<true><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, S0 + 8 * ps,
-                ss.hist + ps * kRadix, status, ss.tile_ctr + ps, err);
-        cudaError_t e = cudaGetLastError();
+                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, S0 + 8 * ps, g,
+                hist, status, ss.tile_ctr + ps, err);
+        const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         cur ^= 1;
     }

@@ -692,7 +692,7 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
 
 template <int D>
 __global__ void __launch_bounds__(kBuildThreads, D == 2 ? 3 : 2)
-k_build(State s, StepParams p, Tree t, uint32_t *err) {
+k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthreads = gridDim.x * blockDim.x;
@@ -701,12 +701,12 @@ k_build(State s, StepParams p, Tree t, uint32_t *err) {
     uint32_t *bar_count = t.meta + kMetaBarCount, *bar_gen = t.meta + kMetaBarGen;
 
     // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
-    uint32_t lb = 0, le = 1;
+    // one root per segment (seeded by the box kernel): nodes 0 .. S-1
+    uint32_t lb = 0, le = (uint32_t)g.S;
     int L = 0;
-    if (gtid == 0) {
-        t.level[0] = 0;
-        t.aux[0] = make_uint4(0u, 0u, kEmpty, 0u);
-    }
+    for (uint32_t r = gtid; r < (uint32_t)g.S; r += nthreads)
+        t.aux[r] = make_uint4(0u, 0u, kEmpty, 0u);
+    if (gtid == 0) t.level[0] = 0;
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
     while (true) {
@@ -836,6 +836,10 @@ k_build(State s, StepParams p, Tree t, uint32_t *err) {
             set_err(err, kErrDepth);
             continue;
         }
+        if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
+            g.root_begin[k] = me;
+            g.root_end[k] = skip;
+        }
         const float nm = D == 2 ? w.z : w.w;
         const bool massless = nm <= 0.0f;
         if (massless) {
@@ -893,8 +897,8 @@ int build_grid_blocks(int dims, int num_sms) {
     return g_build_blocks[di];
 }
 
-cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
-                         int num_sms, cudaStream_t st) {
+cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Segs &g, Tree &t,
+                         uint32_t *err, int num_sms, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(t.lvl_alloc, 0, sizeof(uint32_t) * (kMaxLevels + 2), st);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(t.endcnt, 0, sizeof(uint32_t) * ((size_t)p.n + 1), st);
@@ -909,9 +913,10 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, Tree &t,
     if (blocks < 1) return cudaErrorLaunchOutOfResources;
     State sc = s;
     StepParams pc = p;
+    Segs gc = g;
     Tree tc = t;
     uint32_t *ec = err;
-    void *args[] = {&sc, &pc, &tc, &ec};
+    void *args[] = {&sc, &pc, &gc, &tc, &ec};
     return cudaLaunchCooperativeKernel(dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
                                        dim3(blocks), dim3(kBuildThreads), args, 0, st);
 }

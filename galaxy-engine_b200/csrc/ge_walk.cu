@@ -58,15 +58,14 @@ template <> struct LinkOf<3> { using T = uint2; };
 
 template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
 __global__ void __launch_bounds__(kWalkThreads)
-k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *inter,
+k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
     using LT = typename LinkOf<D>::T;
     constexpr bool kSelfTest = MODE == GE_PREC_EXACT || COUNT || !POS_EPS;
     const LT *__restrict__ link = (const LT *)t.link;
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
-    const uint32_t end = (uint32_t)n + __ldg(&t.meta[0]);
-    const uint32_t limit = end + 1;   // every entry is met at most once
+    const uint32_t limit = (uint32_t)n + __ldg(&t.meta[0]) + 1;   // every entry is met at most once
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
@@ -78,7 +77,11 @@ k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *int
         const float gm_i = fmul(G, mi);   // Gf * pmass (exact mode)
         const uint32_t self = kSelfTest ? __ldg(&t.slot_of[i]) : kEmpty;
         float f[3] = {0.f, 0.f, 0.f};
-        uint32_t k = 0, steps = 0, cnt = 0;
+        // the walk of the particle's own segment: its root to the root's successor
+        const uint32_t sg = g.seg_of ? __ldg(&g.seg_of[i]) : 0u;
+        uint32_t k = __ldg(&g.root_begin[sg]);
+        const uint32_t end = __ldg(&g.root_end[sg]);
+        uint32_t steps = 0, cnt = 0;
         while (k < end) {
             if (++steps > limit) { set_err(err, kErrStack); break; }
             const float4 A = __ldg(&src[k]);
@@ -142,39 +145,39 @@ k_walk(State s, StepParams p, Tree t, int integrate_end, unsigned long long *int
 }
 
 template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
-static cudaError_t walk_one(const State &s, const StepParams &p, const Tree &t, int ie,
-                            unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+static cudaError_t walk_one(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                            int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
     const int blocks = (p.n + kWalkThreads - 1) / kWalkThreads;
     k_walk<D, MODE, COUNT, PER, POS_EPS>
-        <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, t, ie, inter, err);
+        <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, g, t, ie, inter, err);
     return cudaGetLastError();
 }
 
 template <int D, int MODE, bool PER>
-static cudaError_t walk_eps(const State &s, const StepParams &p, const Tree &t, int ie,
-                            unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    if (inter) return walk_one<D, MODE, true, PER, false>(s, p, t, ie, inter, err, st);
-    if (p.eps2 > 0.0f) return walk_one<D, MODE, false, PER, true>(s, p, t, ie, nullptr, err, st);
-    return walk_one<D, MODE, false, PER, false>(s, p, t, ie, nullptr, err, st);
+static cudaError_t walk_eps(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                            int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if (inter) return walk_one<D, MODE, true, PER, false>(s, p, g, t, ie, inter, err, st);
+    if (p.eps2 > 0.0f) return walk_one<D, MODE, false, PER, true>(s, p, g, t, ie, nullptr, err, st);
+    return walk_one<D, MODE, false, PER, false>(s, p, g, t, ie, nullptr, err, st);
 }
 
 template <int D, int MODE>
-static cudaError_t walk_mode(const State &s, const StepParams &p, const Tree &t, int ie,
-                             unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    if (p.periodic) return walk_eps<D, MODE, true>(s, p, t, ie, inter, err, st);
-    return walk_eps<D, MODE, false>(s, p, t, ie, inter, err, st);
+static cudaError_t walk_mode(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if (p.periodic) return walk_eps<D, MODE, true>(s, p, g, t, ie, inter, err, st);
+    return walk_eps<D, MODE, false>(s, p, g, t, ie, inter, err, st);
 }
 
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
-                        const Tree &t, bool integrate_end, unsigned long long *inter_count,
-                        uint32_t *err, cudaStream_t st) {
+                        const Segs &g, const Tree &t, bool integrate_end,
+                        unsigned long long *inter_count, uint32_t *err, cudaStream_t st) {
     const int ie = integrate_end ? 1 : 0;
     const bool exact = precision == GE_PREC_EXACT;
     if (dims == 2)
-        return exact ? walk_mode<2, GE_PREC_EXACT>(s, p, t, ie, inter_count, err, st)
-                     : walk_mode<2, GE_PREC_FAST>(s, p, t, ie, inter_count, err, st);
-    return exact ? walk_mode<3, GE_PREC_EXACT>(s, p, t, ie, inter_count, err, st)
-                 : walk_mode<3, GE_PREC_FAST>(s, p, t, ie, inter_count, err, st);
+        return exact ? walk_mode<2, GE_PREC_EXACT>(s, p, g, t, ie, inter_count, err, st)
+                     : walk_mode<2, GE_PREC_FAST>(s, p, g, t, ie, inter_count, err, st);
+    return exact ? walk_mode<3, GE_PREC_EXACT>(s, p, g, t, ie, inter_count, err, st)
+                 : walk_mode<3, GE_PREC_FAST>(s, p, g, t, ie, inter_count, err, st);
 }
 
 }  // namespace ge

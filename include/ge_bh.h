@@ -158,7 +158,8 @@ int ge_set_count_interactions(ge_ctx *ctx, int32_t enable);
 
 /* --- FP64 diagnostics (accuracy reference; not on the step path) ------- */
 /* Direct-sum accelerations in FP64 of the particles at indices idx[0..nt) of
-   the current order: sum over j != i of G m_j d / (|d|^2 + eps2)^(3/2).
+   the current order: sum over j != i of G m_j d / (|d|^2 + eps2)^(3/2), j over
+   the particle's own sim.
    ax/ay/az (host, nt doubles each; az ignored in 2D). */
 int ge_direct_sum_f64(ge_ctx *ctx, int64_t nt, const uint32_t *idx, double *ax, double *ay,
                       double *az);
@@ -197,8 +198,39 @@ int ge_build_timeline(ge_ctx *ctx, int32_t cap, uint64_t *ns, int32_t *count);
 int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const float *d_y, uint32_t *d_perm,
                               uint64_t *d_keys, void *stream);
 
+/* --- batched simulations -----------------------------------------------
+ * No counterpart in the reference (one particle system per process).  A
+ * context holds any number of independent simulations ("sims") of its dims
+ * and parameters; every ge_step / ge_batch_step advances all of them with
+ * one launch per stage.  Each sim keeps its own particle range, root box,
+ * Morton order and tree; no sim sees another's particles, so every sim's
+ * result is the same as stepping it alone in its own context.
+ * ge_upload replaces all sims by a single one.  Handles are positive and
+ * never reused within a context.  Adding or removing a sim waits for the
+ * context's stream and may reallocate (existing state is kept). */
+/* same as ge_create / ge_step */
+int ge_batch_create(const ge_params *p, ge_ctx **out);
+int ge_batch_step(ge_ctx *ctx, int32_t nsteps);
+/* appends a sim of n >= 1 particles (host SoA, as ge_upload; id NULL =
+   0..n-1); *sim receives its handle */
+int ge_batch_add_sim(ge_ctx *ctx, int64_t n, const float *x, const float *y, const float *z,
+                     const float *vx, const float *vy, const float *vz, const float *m,
+                     const uint32_t *id, int32_t *sim);
+/* removes a sim; the others keep their state */
+int ge_batch_remove_sim(ge_ctx *ctx, int32_t sim);
+/* number of sims and, when sims != NULL, up to cap handles in slot order */
+int ge_batch_list(ge_ctx *ctx, int32_t cap, int32_t *sims, int32_t *count);
+/* a sim's particle count, first slot in the context's arrays, and steps taken
+   since it was added (any pointer may be NULL) */
+int ge_batch_query(ge_ctx *ctx, int32_t sim, int64_t *n, int64_t *offset, int64_t *steps);
+/* one sim's state (its particles in its Morton order), as ge_download */
+int ge_batch_download_sim(ge_ctx *ctx, int32_t sim, float *x, float *y, float *z, float *vx,
+                          float *vy, float *vz, float *ax, float *ay, float *az, float *m,
+                          uint32_t *id);
+
 /* --- tree export: the reference's globalNodes in DFS pre-order --------- */
-/* Returns the node count in *count.  Arrays (capacity cap nodes; any may be
+/* Returns the node count in *count (with several sims: every sim's tree, one
+   after another in slot order).  Arrays (capacity cap nodes; any may be
    NULL): pos/com [cap*dims], size, mass [cap], start, end, next [cap],
    child [cap * 2^dims] with child[q], q = xbit | ybit<<1 (| zbit<<2), the
    reference's subGrids[x][y]([z]); 0xFFFFFFFF marks an empty slot. */
