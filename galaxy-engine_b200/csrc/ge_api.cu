@@ -40,6 +40,7 @@ struct Buffers {
     unsigned long long *d_inter = nullptr;
     bool prev = false;     // prevVel arrays allocated
     bool pinned = false;   // pin flag arrays allocated
+    bool mixed = false;    // GE_PREC_MIXED arrays allocated
     std::vector<void *> allocs;
 };
 
@@ -147,6 +148,7 @@ StepParams step_params(const ge_ctx *c) {
     s.dt = c->p.dt;
     s.half_dt = c->p.dt * 0.5f;
     s.G = c->p.G;
+    s.theta = c->p.theta;
     s.theta2 = c->p.theta * c->p.theta;
     s.eps2 = c->p.eps2;
     s.leaf_cap = c->p.leaf_cap;
@@ -163,8 +165,9 @@ StepParams step_params(const ge_ctx *c) {
 int validate(ge_ctx *c, const ge_params *p) {
     if (!p) return fail(c, GE_ERR_ARG, "params is NULL");
     if (p->dims != 2 && p->dims != 3) return fail(c, GE_ERR_ARG, "dims must be 2 or 3");
-    if (p->precision != GE_PREC_FAST && p->precision != GE_PREC_EXACT)
-        return fail(c, GE_ERR_UNSUPPORTED, "precision mode not supported by this build");
+    if (p->precision != GE_PREC_FAST && p->precision != GE_PREC_EXACT &&
+        p->precision != GE_PREC_MIXED)
+        return fail(c, GE_ERR_ARG, "unknown precision mode");
     if (!(p->theta >= 0.0f)) return fail(c, GE_ERR_ARG, "theta must be >= 0");
     if (!(p->eps2 >= 0.0f)) return fail(c, GE_ERR_ARG, "eps2 must be >= 0");
     if (p->leaf_cap < 1) return fail(c, GE_ERR_ARG, "leaf_cap must be >= 1");
@@ -237,19 +240,48 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     return GE_OK;
 }
 
+// GE_PREC_MIXED arrays: Kahan terms of both state buffers (zeroed) and the
+// node moments.
+int alloc_mixed(ge_ctx *c, Buffers &nb) {
+    const int D = c->p.dims;
+    const size_t N = (size_t)nb.cap_n, E = N + (size_t)nb.tree.cap + 1;
+    auto &L = nb.allocs;
+    for (int k = 0; k < 2; k++) {
+        State &s = nb.st[k];
+        float **kp[6] = {&s.kx, &s.ky, &s.kz, &s.kvx, &s.kvy, &s.kvz};
+        for (int a = 0; a < 6; a++) {
+            if (D == 2 && (a == 2 || a == 5)) continue;
+            GE_CHECK(c, dalloc(L, kp[a], N));
+            GE_CHECK(c, cudaMemsetAsync(*kp[a], 0, sizeof(float) * N, c->stream));
+        }
+    }
+    Tree &t = nb.tree;
+    GE_CHECK(c, dalloc(L, &t.mom, (size_t)t.cap * (D == 2 ? MomWords<2>::value : MomWords<3>::value)));
+    GE_CHECK(c, dalloc(L, &t.mq0, E));
+    if (D == 3) GE_CHECK(c, dalloc(L, &t.mq1, E));
+    GE_CHECK(c, dalloc(L, &t.mq2, E));
+    nb.mixed = true;
+    return GE_OK;
+}
+
 // Copies particles [soff, soff + cnt) of src to [doff, doff + cnt) of dst
 // (device to device, on the context's stream).
 int copy_range(ge_ctx *c, const State &dst, int64_t doff, const State &src, int64_t soff,
                int64_t cnt, bool prev, bool pinned) {
     if (cnt <= 0) return GE_OK;
     const bool d3 = c->p.dims == 3;
+    const bool kah = dst.kx && src.kx;
     const size_t B = sizeof(float) * (size_t)cnt;
     float *const fd[] = {dst.x, dst.y, d3 ? dst.z : nullptr, dst.vx, dst.vy, d3 ? dst.vz : nullptr,
                          dst.ax, dst.ay, d3 ? dst.az : nullptr, dst.m,
                          prev ? dst.pvx : nullptr, prev ? dst.pvy : nullptr,
-                         prev && d3 ? dst.pvz : nullptr};
+                         prev && d3 ? dst.pvz : nullptr,
+                         kah ? dst.kx : nullptr, kah ? dst.ky : nullptr,
+                         kah && d3 ? dst.kz : nullptr, kah ? dst.kvx : nullptr,
+                         kah ? dst.kvy : nullptr, kah && d3 ? dst.kvz : nullptr};
     const float *const fs[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.ax, src.ay,
-                               src.az, src.m, src.pvx, src.pvy, src.pvz};
+                               src.az, src.m, src.pvx, src.pvy, src.pvz,
+                               src.kx, src.ky, src.kz, src.kvx, src.kvy, src.kvz};
     for (size_t k = 0; k < sizeof(fd) / sizeof(fd[0]); k++)
         if (fd[k])
             GE_CHECK(c, cudaMemcpyAsync(fd[k] + doff, fs[k] + soff, B, cudaMemcpyDeviceToDevice,
@@ -291,6 +323,7 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep) {
     if (node_cap >= (1ll << 32) - 1) return fail(c, GE_ERR_ARG, "node capacity exceeds 2^32");
     Buffers nb;
     int rc = alloc_buffers(c, nb, cap, node_cap, want_prev, ob.pinned);
+    if (!rc && (ob.mixed || c->p.precision == GE_PREC_MIXED)) rc = alloc_mixed(c, nb);
     if (rc) {
         cudaStreamSynchronize(c->stream);
         free_all(nb.allocs);
@@ -415,17 +448,17 @@ int check_device(ge_ctx *c) {
     return GE_OK;
 }
 
-State cur_state(ge_ctx *c) {
-    State s = c->b.st[c->cur];
+// The state as the kernels see it: pin flags only when uploaded, Kahan terms
+// only in the mixed mode.
+State view(ge_ctx *c, int which) {
+    State s = c->b.st[which];
     if (!c->has_pinned) s.pinned = nullptr;
+    if (c->p.precision != GE_PREC_MIXED) s.kx = s.ky = s.kz = s.kvx = s.kvy = s.kvz = nullptr;
     return s;
 }
 
-State other_state(ge_ctx *c) {
-    State s = c->b.st[c->cur ^ 1];
-    if (!c->has_pinned) s.pinned = nullptr;
-    return s;
-}
+State cur_state(ge_ctx *c) { return view(c, c->cur); }
+State other_state(ge_ctx *c) { return view(c, c->cur ^ 1); }
 
 int enqueue_bbox(ge_ctx *c, bool kick) {
     StepParams p = step_params(c);
@@ -455,6 +488,18 @@ int enqueue_build(ge_ctx *c) {
     StepParams p = step_params(c);
     GE_CHECK(c, launch_build(c->p.dims, cur_state(c), p, c->g, c->b.tree, c->d_err, c->num_sms,
                              c->stream));
+    if (c->p.precision == GE_PREC_MIXED)
+        GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, c->b.tree, c->d_err, c->num_sms,
+                                   c->stream));
+    return GE_OK;
+}
+
+// The mixed-precision arrays, when the mode was switched on after the upload.
+int ensure_mode(ge_ctx *c) {
+    if (c->p.precision != GE_PREC_MIXED || c->b.mixed) return GE_OK;
+    int rc = alloc_mixed(c, c->b);
+    if (rc) return rc;
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
     return GE_OK;
 }
 
@@ -491,7 +536,7 @@ int enqueue_frame(ge_ctx *c, cudaEvent_t *ev) {
 int require_state(ge_ctx *c) {
     if (!c) return GE_ERR_ARG;
     if (c->n <= 0) return fail(c, GE_ERR_STATE, "no particles uploaded");
-    return GE_OK;
+    return ensure_mode(c);
 }
 
 int check_host_arrays(ge_ctx *c, int64_t n, const float *x, const float *y, const float *z,
@@ -545,6 +590,11 @@ int put_host(ge_ctx *c, int64_t off, int64_t n, const float *x, const float *y, 
             GE_CHECK(c, cudaMemcpyAsync(s.pvz + off, s.vz + off, B, cudaMemcpyDeviceToDevice, st));
     }
     if (c->b.pinned) GE_CHECK(c, cudaMemsetAsync(s.pinned + off, 0, (size_t)n, st));
+    if (s.kx) {
+        float *kp[6] = {s.kx, s.ky, s.kz, s.kvx, s.kvy, s.kvz};
+        for (float *q : kp)
+            if (q) GE_CHECK(c, cudaMemsetAsync(q + off, 0, B, st));
+    }
     return GE_OK;
 }
 
@@ -653,7 +703,18 @@ int ge_set_params(ge_ctx *c, const ge_params *p) {
     const bool realloc = c->b.cap_n && (p->node_cap_factor != c->p.node_cap_factor ||
                                         (p->track_prev_vel != 0) != c->b.prev);
     if (realloc) return fail(c, GE_ERR_STATE, "node_cap_factor / track_prev_vel change needs a new upload");
+    const bool to_mixed = p->precision == GE_PREC_MIXED && c->p.precision != GE_PREC_MIXED;
     c->p = *p;
+    if (to_mixed && c->b.mixed) {
+        // the compensation terms were not carried in the other modes: restart them
+        for (int k = 0; k < 2; k++) {
+            const State &s = c->b.st[k];
+            float *kp[6] = {s.kx, s.ky, s.kz, s.kvx, s.kvy, s.kvz};
+            for (float *q : kp)
+                if (q) GE_CHECK(c, cudaMemsetAsync(q, 0, sizeof(float) * (size_t)c->b.cap_n, c->stream));
+        }
+    }
+    c->tree_valid = false;
     return GE_OK;
 }
 

@@ -28,6 +28,15 @@ __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b)
 __device__ __forceinline__ float ref_min(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float ref_max(float a, float b) { return (a < b) ? b : a; }
 
+// v += t with Kahan compensation c (the running error of v, subtracted from
+// the next addend)
+__device__ __forceinline__ void kahan_add(float &v, float &c, float t) {
+    const float y = fsub(t, c);
+    const float s = fadd(v, y);
+    c = fsub(fsub(s, v), y);
+    v = s;
+}
+
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ void set_err(uint32_t *err, uint32_t bit) {

@@ -38,10 +38,23 @@ __device__ __forceinline__ void kick_drift(const State &s, const StepParams &p, 
         s.pvx[i] = vel[0]; s.pvy[i] = vel[1];
         if (D == 3) s.pvz[i] = vel[2];
     }
+    if (s.kx) {
+        // GE_PREC_MIXED: both updates Kahan-compensated
+        float *kp[3] = {s.kx, s.ky, s.kz}, *kv[3] = {s.kvx, s.kvy, s.kvz};
 #pragma unroll
-    for (int a = 0; a < D; a++) {
-        vel[a] = fadd(vel[a], fmul(acc[a], p.half_dt));   // vel += acc * halfDt
-        pos[a] = fadd(pos[a], fmul(vel[a], p.dt));         // pos += vel * dt
+        for (int a = 0; a < D; a++) {
+            float cv = kv[a][i], cp = kp[a][i];
+            kahan_add(vel[a], cv, fmul(acc[a], p.half_dt));
+            kahan_add(pos[a], cp, fmul(vel[a], p.dt));
+            kv[a][i] = cv;
+            kp[a][i] = cp;
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            vel[a] = fadd(vel[a], fmul(acc[a], p.half_dt));   // vel += acc * halfDt
+            pos[a] = fadd(pos[a], fmul(vel[a], p.dt));         // pos += vel * dt
+        }
     }
     if (p.periodic) {
         if (D == 2) {
@@ -164,6 +177,12 @@ template <int D>
 __global__ void k_integrate_end(State s, StepParams p) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x) {
         if (s.pinned && s.pinned[i]) continue;
+        if (s.kvx) {
+            kahan_add(s.vx[i], s.kvx[i], fmul(s.ax[i], p.half_dt));
+            kahan_add(s.vy[i], s.kvy[i], fmul(s.ay[i], p.half_dt));
+            if (D == 3) kahan_add(s.vz[i], s.kvz[i], fmul(s.az[i], p.half_dt));
+            continue;
+        }
         s.vx[i] = fadd(s.vx[i], fmul(s.ax[i], p.half_dt));
         s.vy[i] = fadd(s.vy[i], fmul(s.ay[i], p.half_dt));
         if (D == 3) s.vz[i] = fadd(s.vz[i], fmul(s.az[i], p.half_dt));

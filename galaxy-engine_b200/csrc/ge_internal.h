@@ -16,6 +16,10 @@ struct State {
     uint32_t *id;
     float *pvx, *pvy, *pvz;
     uint8_t *pinned;
+    // GE_PREC_MIXED: Kahan compensation terms of positions and velocities
+    // (nullptr in the other modes)
+    float *kx, *ky, *kz;
+    float *kvx, *kvy, *kvz;
 };
 
 // Tree nodes, structure-of-arrays.
@@ -27,7 +31,7 @@ struct State {
 //   cell    float4  {corner.x, corner.y, corner.z, size} (build only)
 //   level   uint32  first node of each level (nodes are stored level by level)
 //   aux     uint4   {level, number of proper ancestors whose range ends where this
-//                   node's range ends, parent, 0} (build only)
+//                   node's range ends, parent, walk entry (set by the layout)}
 //   pend    uint32  children whose mass is not final yet (build only)
 //
 // Walk layout (written at the end of the build): one array of "sources" in
@@ -63,8 +67,23 @@ struct Tree {
     uint32_t *meta;       // [8] {node_count, levels, bar_count, bar_gen, err, small,
                           //      phase-2 nodes, timeline entries}
     unsigned long long *tl;   // [kTimeline] build timeline (globaltimer ns)
+    // GE_PREC_MIXED node moments (nullptr in the other modes):
+    //   mom   double [cap * kMomWords]  {mass, com (D), second moments about the
+    //                                   com (xx, xy, yy | xx, yy, zz, xy, xz, yz)}
+    //   mq0   float4 per walk entry     2D {com_lo.x, com_lo.y, Ixx, Ixy}
+    //                                   3D {com_lo.x, com_lo.y, com_lo.z, Ixx}
+    //   mq1   float4 per walk entry     3D {Iyy, Izz, Ixy, Ixz}
+    //   mq2   float  per walk entry     2D Iyy, 3D Iyz
+    // (com = src com + com_lo as a double-float pair)
+    double *mom;
+    float4 *mq0, *mq1;
+    float *mq2;
     int64_t cap;
 };
+
+template <int D> struct MomWords;
+template <> struct MomWords<2> { static constexpr int value = 6; };
+template <> struct MomWords<3> { static constexpr int value = 10; };
 
 // Independent simulations ("segments") stepped together: the particles of
 // segment s occupy [off[s], off[s+1]) of the state arrays and never leave it;
@@ -103,7 +122,7 @@ struct SortScratch {
 struct StepParams {
     int n;
     float dt, half_dt;
-    float G, theta2, eps2;
+    float G, theta, theta2, eps2;
     uint32_t leaf_cap;
     float size_gate, min_size;
     int periodic;
@@ -154,6 +173,11 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         const Segs &g, const Tree &t, bool integrate_end,
                         unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+// GE_PREC_MIXED: FP64 mass, centre of mass and second moments of every node,
+// bottom-up from the particles, written into the walk entries with the
+// offset-corrected opening radius (after launch_build)
+cudaError_t launch_moments(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
+                           int num_sms, cudaStream_t st);
 // FP64 diagnostics
 // (each target sums over its own segment only; idx sorted ascending keeps a
 // block's targets inside one or two segments)

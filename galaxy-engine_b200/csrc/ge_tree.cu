@@ -836,6 +836,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
             set_err(err, kErrDepth);
             continue;
         }
+        t.aux[k].w = me;   // the node's entry (read by the moment pass)
         if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
             g.root_begin[k] = me;
             g.root_end[k] = skip;

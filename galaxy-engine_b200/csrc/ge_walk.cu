@@ -24,6 +24,10 @@
 //                   bit-identical accelerations.
 //   GE_PREC_FAST  : approximate reciprocal square root (MUFU, flush-to-zero)
 //                   and FMA for the force terms, G applied once.
+//   GE_PREC_MIXED : the node entries written by the moment pass
+//                   (ge_moments.cu): opening radius instead of size, the
+//                   double-float centre of mass, a quadrupole term, and
+//                   Kahan-compensated sums of the acceleration terms.
 // integrateEnd (physics.cpp:1114-1125) is fused into the epilogue.
 #include "ge_bh.h"
 #include "ge_device.cuh"
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(kWalkThreads)
 k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
     using LT = typename LinkOf<D>::T;
-    constexpr bool kSelfTest = MODE == GE_PREC_EXACT || COUNT || !POS_EPS;
+    constexpr bool kSelfTest = MODE != GE_PREC_FAST || COUNT || !POS_EPS;
     const LT *__restrict__ link = (const LT *)t.link;
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
@@ -77,6 +81,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         const float gm_i = fmul(G, mi);   // Gf * pmass (exact mode)
         const uint32_t self = kSelfTest ? __ldg(&t.slot_of[i]) : kEmpty;
         float f[3] = {0.f, 0.f, 0.f};
+        float fc[3] = {0.f, 0.f, 0.f};   // Kahan compensation (MIXED)
         // the walk of the particle's own segment: its root to the root's successor
         const uint32_t sg = g.seg_of ? __ldg(&g.seg_of[i]) : 0u;
         uint32_t k = __ldg(&g.root_begin[sg]);
@@ -99,10 +104,61 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
             float r2 = fadd(fmul(d[0], d[0]), fmul(d[1], d[1]));
             if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
             r2 = fadd(r2, eps2);
-            const bool acc = s2 < fmul(th2, r2);
+            // MIXED entries hold the squared opening radius, which already
+            // includes 1 / theta
+            const bool acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
             if (kSelfTest) {
                 if (acc && m != 0.0f && k != self) {
-                    if (MODE == GE_PREC_EXACT) {
+                    if (MODE == GE_PREC_MIXED) {
+                        float term[3];
+                        if (s2 >= 0.0f) {
+                            // node: centre of mass = hi + lo, then monopole +
+                            // quadrupole of the softened kernel:
+                            //   m d / r^3 - 3 I d / r^5 - 1.5 tr(I) d / r^5
+                            //   + 7.5 (d.I.d) d / r^7,   r^2 = |d|^2 + eps2
+                            const float4 B = __ldg(&t.mq0[k]);
+                            d[0] += B.x; d[1] += B.y;
+                            if (D == 3) d[2] += B.z;
+                            float rr = d[0] * d[0] + d[1] * d[1] + eps2;
+                            if (D == 3) rr += d[2] * d[2];
+                            const float inv = rsqrt_approx(rr);
+                            const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
+                            const float inv7 = inv5 * inv2;
+                            float Id[3], tr;
+                            if (D == 2) {
+                                const float ixx = B.z, ixy = B.w, iyy = __ldg(&t.mq2[k]);
+                                Id[0] = ixx * d[0] + ixy * d[1];
+                                Id[1] = ixy * d[0] + iyy * d[1];
+                                Id[2] = 0.0f;
+                                tr = ixx + iyy;
+                            } else {
+                                const float4 C = __ldg(&t.mq1[k]);   // {Iyy, Izz, Ixy, Ixz}
+                                const float ixx = B.w, iyz = __ldg(&t.mq2[k]);
+                                Id[0] = ixx * d[0] + C.z * d[1] + C.w * d[2];
+                                Id[1] = C.z * d[0] + C.x * d[1] + iyz * d[2];
+                                Id[2] = C.w * d[0] + iyz * d[1] + C.y * d[2];
+                                tr = ixx + C.x + C.y;
+                            }
+                            float dId = d[0] * Id[0] + d[1] * Id[1];
+                            if (D == 3) dId += d[2] * Id[2];
+                            const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
+                            const float ci = -3.0f * inv5;
+#pragma unroll
+                            for (int a = 0; a < D; a++) term[a] = cm * d[a] + ci * Id[a];
+                        } else {
+                            const float inv = rsqrt_approx(r2);
+                            const float fm = m * (inv * inv * inv);
+#pragma unroll
+                            for (int a = 0; a < D; a++) term[a] = d[a] * fm;
+                        }
+#pragma unroll
+                        for (int a = 0; a < D; a++) {   // Kahan summation
+                            const float y = fsub(term[a], fc[a]);
+                            const float tt = fadd(f[a], y);
+                            fc[a] = fsub(fsub(tt, f[a]), y);
+                            f[a] = tt;
+                        }
+                    } else if (MODE == GE_PREC_EXACT) {
                         const float inv = fdiv(1.0f, __fsqrt_rn(r2));
                         const float inv3 = fmul(fmul(inv, inv), inv);
                         const float fm = fmul(fmul(gm_i, m), inv3);
@@ -128,13 +184,21 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         }
         float a3[3];
 #pragma unroll
-        for (int a = 0; a < D; a++) a3[a] = MODE == GE_PREC_EXACT ? fdiv(f[a], mi) : G * f[a];
+        for (int a = 0; a < D; a++)
+            a3[a] = MODE == GE_PREC_EXACT ? fdiv(f[a], mi)
+                  : MODE == GE_PREC_MIXED ? G * fsub(f[a], fc[a]) : G * f[a];
         s.ax[i] = a3[0]; s.ay[i] = a3[1];
         if (D == 3) s.az[i] = a3[2];
         if (integrate_end && !(s.pinned && s.pinned[i])) {
-            s.vx[i] = fadd(s.vx[i], fmul(a3[0], p.half_dt));
-            s.vy[i] = fadd(s.vy[i], fmul(a3[1], p.half_dt));
-            if (D == 3) s.vz[i] = fadd(s.vz[i], fmul(a3[2], p.half_dt));
+            if (MODE == GE_PREC_MIXED && s.kvx) {
+                float *vel[3] = {s.vx, s.vy, s.vz}, *kv[3] = {s.kvx, s.kvy, s.kvz};
+#pragma unroll
+                for (int a = 0; a < D; a++) kahan_add(vel[a][i], kv[a][i], fmul(a3[a], p.half_dt));
+            } else {
+                s.vx[i] = fadd(s.vx[i], fmul(a3[0], p.half_dt));
+                s.vy[i] = fadd(s.vy[i], fmul(a3[1], p.half_dt));
+                if (D == 3) s.vz[i] = fadd(s.vz[i], fmul(a3[2], p.half_dt));
+            }
         }
         my_count = cnt;
     }
@@ -157,7 +221,9 @@ template <int D, int MODE, bool PER>
 static cudaError_t walk_eps(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
     if (inter) return walk_one<D, MODE, true, PER, false>(s, p, g, t, ie, inter, err, st);
-    if (p.eps2 > 0.0f) return walk_one<D, MODE, false, PER, true>(s, p, g, t, ie, nullptr, err, st);
+    if constexpr (MODE != GE_PREC_MIXED)   // MIXED always tests for the particle itself
+        if (p.eps2 > 0.0f)
+            return walk_one<D, MODE, false, PER, true>(s, p, g, t, ie, nullptr, err, st);
     return walk_one<D, MODE, false, PER, false>(s, p, g, t, ie, nullptr, err, st);
 }
 
@@ -173,6 +239,9 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         unsigned long long *inter_count, uint32_t *err, cudaStream_t st) {
     const int ie = integrate_end ? 1 : 0;
     const bool exact = precision == GE_PREC_EXACT;
+    if (precision == GE_PREC_MIXED)
+        return dims == 2 ? walk_mode<2, GE_PREC_MIXED>(s, p, g, t, ie, inter_count, err, st)
+                         : walk_mode<3, GE_PREC_MIXED>(s, p, g, t, ie, inter_count, err, st);
     if (dims == 2)
         return exact ? walk_mode<2, GE_PREC_EXACT>(s, p, g, t, ie, inter_count, err, st)
                      : walk_mode<2, GE_PREC_FAST>(s, p, g, t, ie, inter_count, err, st);

@@ -124,6 +124,17 @@ void or_direct_f64(int dims, int64_t n, const float *x, const float *y, const fl
                    const float *m, double G, double eps2, int64_t nt, const int64_t *idx,
                    double *ax, double *ay, double *az, int nthreads);
 
+/* --- mixed-precision walk (checker of GE_PREC_MIXED; ge_oracle_mixed.c) --
+ * FP64 node moments (mom: [count * (6 | 10)] = mass, com, second moments
+ * about the com: 2D xx xy yy, 3D xx yy zz xy xz yz), then the walk with the
+ * offset-corrected opening test and the softened quadrupole, accelerations
+ * in FP64.  inter (optional, [n]) receives the interaction counts. */
+int or_moments_mixed(const or_tree *t, const float *x, const float *y, const float *z,
+                     const float *m, double *mom);
+void or_walk_mixed(int64_t n, const float *x, const float *y, const float *z, const float *m,
+                   const or_tree *t, const or_params *p, double *ax, double *ay, double *az,
+                   uint32_t *inter, int nthreads);
+
 /* --- leapfrog --------------------------------------------------------- */
 void or_integrate_start(int dims, int64_t n, float *x, float *y, float *z,
                         float *vx, float *vy, float *vz, const float *ax, const float *ay,

@@ -1,0 +1,198 @@
+/*
+ * ge_oracle_mixed.c -- CPU statement of the mixed-precision tree walk.
+ * TEST INFRASTRUCTURE ONLY (the checker of GE_PREC_MIXED).
+ *
+ * The mixed mode has no counterpart in the reference: it keeps the
+ * reference's tree (quadtree.cpp:5-292, the same nodes and particle ranges as
+ * or_build_quadtree / or_build_octree) and its pre-order walk
+ * (physics.cpp:91-205, physics3D.cpp:131-253), and changes what a node
+ * contributes:
+ *   - mass, centre of mass and second moments about it, in FP64: a leaf sums
+ *     its particles in index order, an internal node combines its children in
+ *     child-slot order with the parallel-axis rule (the same operations, each
+ *     product-sum a correctly rounded fma, as the device pass);
+ *   - opening test b^2 < |d|^2 + eps2 in FP32 with b = size / theta +
+ *     |com - cell centre| (b^2 rounded to FP32 from FP64), d = FP32(com) - x;
+ *   - an accepted node adds the monopole and quadrupole of the softened
+ *     kernel:  G [ M d / r^3 - 3 I d / r^5 - 1.5 tr(I) d / r^5
+ *                  + 7.5 (d.I.d) d / r^7 ],  r^2 = |d|^2 + eps2,
+ *     here evaluated in FP64 with d = com - x in FP64;
+ *   - a leaf that is opened adds G m_j d / r^3 for its particles j != i
+ *     with m_j != 0, in FP64.
+ * The device evaluates the same interaction list in FP32 with a Kahan sum.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ge_oracle.h"
+
+#define EMPTY UINT32_MAX
+
+static int is_leaf(const or_tree *t, int64_t k) {
+    const int nq = 1 << t->dims;
+    for (int q = 0; q < nq; q++)
+        if (t->child[k * nq + q] != EMPTY) return 0;
+    return 1;
+}
+
+/* second-moment slot of (a, b): 2D xx xy yy; 3D xx yy zz xy xz yz */
+static int mom_index(int D, int a, int b) {
+    if (D == 2) return 1 + D + a + b;
+    if (a == b) return 1 + D + a;
+    return 1 + D + 2 + a + b;
+}
+
+int or_moments_mixed(const or_tree *t, const float *x, const float *y, const float *z,
+                     const float *m, double *mom) {
+    const int D = t->dims, R = D == 2 ? 6 : 10, nq = 1 << D;
+    const float *pos[3] = {x, y, z};
+    for (int64_t k = t->count - 1; k >= 0; k--) {   /* children follow parents in pre-order */
+        double *r = mom + k * R;
+        for (int w = 0; w < R; w++) r[w] = 0.0;
+        if (is_leaf(t, k)) {
+            for (uint32_t j = t->start[k]; j < t->end[k]; j++) {
+                const double mj = m[j];
+                r[0] += mj;
+                for (int a = 0; a < D; a++) r[1 + a] = fma(mj, (double)pos[a][j], r[1 + a]);
+            }
+            if (r[0] > 0.0) {
+                for (int a = 0; a < D; a++) r[1 + a] /= r[0];
+                for (uint32_t j = t->start[k]; j < t->end[k]; j++) {
+                    const double mj = m[j];
+                    double d[3];
+                    for (int a = 0; a < D; a++) d[a] = (double)pos[a][j] - r[1 + a];
+                    for (int a = 0; a < D; a++)
+                        for (int b = a; b < D; b++) {
+                            const int w = mom_index(D, a, b);
+                            r[w] = fma(mj * d[a], d[b], r[w]);
+                        }
+                }
+            }
+        } else {
+            for (int q = 0; q < nq; q++) {
+                const uint32_t c = t->child[k * nq + q];
+                if (c == EMPTY) continue;
+                const double *cr = mom + (int64_t)c * R;
+                r[0] += cr[0];
+                for (int a = 0; a < D; a++) r[1 + a] = fma(cr[0], cr[1 + a], r[1 + a]);
+            }
+            if (r[0] > 0.0) {
+                for (int a = 0; a < D; a++) r[1 + a] /= r[0];
+                for (int q = 0; q < nq; q++) {
+                    const uint32_t c = t->child[k * nq + q];
+                    if (c == EMPTY) continue;
+                    const double *cr = mom + (int64_t)c * R;
+                    if (!(cr[0] > 0.0)) continue;
+                    double d[3];
+                    for (int a = 0; a < D; a++) d[a] = cr[1 + a] - r[1 + a];
+                    for (int a = 0; a < D; a++)
+                        for (int b = a; b < D; b++) {
+                            const int w = mom_index(D, a, b);
+                            r[w] += fma(cr[0] * d[a], d[b], cr[w]);
+                        }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+/* periodic image shift of one FP32 offset: physics.cpp:118-121 */
+static float wrap_k(float d, float half) { return (float)((d > half) - (d < -half)); }
+
+void or_walk_mixed(int64_t n, const float *x, const float *y, const float *z, const float *m,
+                   const or_tree *t, const or_params *p, double *ax, double *ay, double *az,
+                   uint32_t *inter, int nthreads) {
+    const int D = t->dims, R = D == 2 ? 6 : 10;
+    double *mom = (double *)malloc(sizeof(double) * (size_t)(t->count > 0 ? t->count : 1) * R);
+    float *b2 = (float *)malloc(sizeof(float) * (size_t)(t->count > 0 ? t->count : 1));
+    float *hi = (float *)malloc(sizeof(float) * (size_t)(t->count > 0 ? t->count : 1) * 3);
+    if (!mom || !b2 || !hi) { free(mom); free(b2); free(hi); return; }
+    or_moments_mixed(t, x, y, z, m, mom);
+    const double inv_theta = 1.0 / (double)p->theta;
+    for (int64_t k = 0; k < t->count; k++) {
+        const double *r = mom + k * R;
+        const double half = 0.5 * (double)t->size[k];
+        double del2 = 0.0;
+        for (int a = 0; a < D; a++) {
+            hi[k * 3 + a] = (float)r[1 + a];
+            const double dc = r[1 + a] - ((double)t->pos[k * D + a] + half);
+            del2 = fma(dc, dc, del2);
+        }
+        const double b = fma((double)t->size[k], inv_theta, sqrt(del2));
+        b2[k] = (float)(b * b);
+    }
+    const float *pos[3] = {x, y, z};
+    const double G = p->G, eps2d = p->eps2;
+    const float eps2 = p->eps2;
+    const uint32_t count = (uint32_t)t->count;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+    for (int64_t i = 0; i < n; i++) {
+        double f[3] = {0, 0, 0};
+        uint32_t cnt = 0;
+        float xi[3] = {x[i], y[i], D == 3 ? z[i] : 0.0f};
+        uint32_t k = 0;
+        while (k < count) {
+            const double *r = mom + (int64_t)k * R;
+            if (!(r[0] > 0.0)) { k += t->next[k] + 1; continue; }
+            float df[3], sh[3] = {0, 0, 0};
+            float r2 = 0.0f;
+            for (int a = 0; a < D; a++) {
+                df[a] = hi[(int64_t)k * 3 + a] - xi[a];
+                if (p->periodic) {
+                    sh[a] = wrap_k(df[a], p->domain[a] * 0.5f);
+                    df[a] = df[a] - p->domain[a] * sh[a];
+                }
+            }
+            r2 = df[0] * df[0] + df[1] * df[1];
+            if (D == 3) r2 = r2 + df[2] * df[2];
+            r2 = r2 + eps2;
+            if (b2[k] < r2) {
+                double d[3] = {0, 0, 0}, rr = eps2d;
+                for (int a = 0; a < D; a++) {
+                    d[a] = r[1 + a] - (double)xi[a] - (double)p->domain[a] * sh[a];
+                    rr += d[a] * d[a];
+                }
+                const double inv = 1.0 / sqrt(rr), inv2 = inv * inv, inv3 = inv2 * inv;
+                const double inv5 = inv3 * inv2, inv7 = inv5 * inv2;
+                double I[3][3] = {{0}};
+                for (int a = 0; a < D; a++)
+                    for (int b = a; b < D; b++) I[a][b] = I[b][a] = (double)(float)r[mom_index(D, a, b)];
+                double Id[3] = {0, 0, 0}, dId = 0.0, tr = 0.0;
+                for (int a = 0; a < D; a++) {
+                    for (int b = 0; b < D; b++) Id[a] += I[a][b] * d[b];
+                    dId += d[a] * Id[a];
+                    tr += I[a][a];
+                }
+                const double M = (double)(float)r[0];
+                const double cm = M * inv3 - 1.5 * tr * inv5 + 7.5 * dId * inv7;
+                for (int a = 0; a < D; a++) f[a] += cm * d[a] - 3.0 * Id[a] * inv5;
+                cnt++;
+                k += t->next[k] + 1;
+            } else if (is_leaf(t, k)) {
+                for (uint32_t j = t->start[k]; j < t->end[k]; j++) {
+                    if ((int64_t)j == i || m[j] == 0.0f) continue;
+                    double d[3] = {0, 0, 0}, rr = eps2d;
+                    for (int a = 0; a < D; a++) {
+                        float dj = pos[a][j] - xi[a];
+                        if (p->periodic) dj = dj - p->domain[a] * wrap_k(dj, p->domain[a] * 0.5f);
+                        d[a] = (double)dj;
+                        rr += d[a] * d[a];
+                    }
+                    const double inv = 1.0 / sqrt(rr), fm = (double)m[j] * inv * inv * inv;
+                    for (int a = 0; a < D; a++) f[a] += fm * d[a];
+                    cnt++;
+                }
+                k += t->next[k] + 1;
+            } else {
+                k++;
+            }
+        }
+        ax[i] = G * f[0];
+        ay[i] = G * f[1];
+        if (D == 3 && az) az[i] = G * f[2];
+        if (inter) inter[i] = cnt;
+    }
+    free(mom); free(b2); free(hi);
+}

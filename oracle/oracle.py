@@ -93,6 +93,8 @@ def _load(strict=True):
                                _f32p, _f32p, _f32p, C.c_int]
     lib.or_direct_f64.argtypes = [C.c_int, C.c_int64, _f32p, _f32p, _vp, _f32p, C.c_double,
                                   C.c_double, C.c_int64, _i64p, _f64p, _f64p, _vp, C.c_int]
+    lib.or_walk_mixed.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
+                                  C.POINTER(Params), _f64p, _f64p, _vp, _vp, C.c_int]
     lib.or_integrate_start.argtypes = [C.c_int, C.c_int64] + [_vp] * 12 + [_vp, C.POINTER(Params)]
     lib.or_integrate_end.argtypes = [C.c_int, C.c_int64] + [_vp] * 6 + [_vp, C.POINTER(Params)]
     lib.or_frame.argtypes = [C.POINTER(Params), C.c_int64] + [_vp] * 16 + [C.c_int, C.c_int,
@@ -241,6 +243,22 @@ def walk(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False, wa
         out.append(inter)
     if want_cond:
         out.append(cond)
+    return out
+
+
+def walk_mixed(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False):
+    """The mixed-precision walk (FP64 moments, offset-corrected opening test,
+    softened quadrupole) on the reference tree; accelerations in FP64."""
+    x, y, m = _f32(x), _f32(y), _f32(m)
+    n = len(x)
+    out = [np.zeros(n, np.float64) for _ in range(2 if z is None else 3)]
+    inter = np.zeros(n, np.uint32) if want_counts else None
+    zz = None if z is None else _f32(z)
+    lib().or_walk_mixed(n, x, y, _ptr(zz), m, C.byref(tree_holder.t), C.byref(params),
+                        out[0], out[1], _ptr(out[2]) if z is not None else None,
+                        _ptr(inter), nthreads)
+    if want_counts:
+        out.append(inter)
     return out
 
 

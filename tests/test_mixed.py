@@ -1,0 +1,120 @@
+"""GPU: the mixed-precision mode (GE_PREC_MIXED).
+
+The mode keeps the reference's tree and walk order and changes what a node
+contributes (FP64 moments, double-float centre of mass, offset-corrected
+opening test, softened quadrupole, Kahan sums).  Checks:
+  * the device walk against the oracle's statement of the same algorithm
+    (oracle/ge_oracle_mixed.c, FP64) on the same tree: the opening decisions
+    are made from the same FP32 values on both sides, so only the FP32
+    evaluation of the accepted terms differs;
+  * the accuracy bound against the FP64 direct sum (median <= 1e-3 at
+    theta 0.6 in 2D and theta 0.5 in 3D);
+  * the Kahan-compensated leapfrog: a drift below half an ulp per step still
+    moves the particle;
+  * a simulation's result alone and inside a batch is the same.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIXED = 2
+
+
+def _sorted_forces(ge, p, st):
+    with ge.Simulation(p) as s:
+        s.upload(st)
+        s.compute_morton_keys()
+        s.sort_particles_by_morton_key()
+        s.build_tree()
+        s.calculate_force_from_grid()
+        return s.download()
+
+
+def _rel(a, b):
+    num = sum((a[k] - b[k]) ** 2 for k in range(len(a)))
+    den = sum(b[k] ** 2 for k in range(len(b)))
+    return np.sqrt(num / np.maximum(den, 1e-300))
+
+
+@pytest.mark.parametrize("dims,n,theta,eps2", [(2, 16384, 0.6, 1e-4), (2, 30000, 0.7, 1e-4),
+                                               (3, 16384, 0.5, 0.01)])
+def test_mixed_walk_matches_oracle(ge, ics, O, dims, n, theta, eps2):
+    st = ics.disk2d(n, seed=3) if dims == 2 else ics.plummer3d(n, seed=3)
+    p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4, dt=1e-3,
+                          precision=MIXED)
+    out = _sorted_forces(ge, p, st)
+    z = out.get("z")
+    bb = O.bbox(out["x"], out["y"], z)
+    tree = O.build_tree(out["x"], out["y"], out["m"], bb, z=z, leaf_cap=4, holder=True)
+    op = O.make_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4)
+    ref = O.walk_mixed(out["x"], out["y"], out["m"], tree, op, z=z)
+    got = [out["ax"], out["ay"]] + ([out["az"]] if dims == 3 else [])
+    e = _rel(got, ref)
+    print(f"mixed vs oracle: median {np.median(e):.2e} p99 {np.percentile(e, 99):.2e} "
+          f"max {e.max():.2e}")
+    assert np.median(e) <= 1e-6
+    assert np.percentile(e, 99) <= 5e-6
+    assert e.max() <= 1e-4
+
+
+@pytest.mark.parametrize("dims,n,theta,eps2", [(2, 1 << 18, 0.6, 0.005 ** 2),
+                                               (3, 1 << 17, 0.5, 0.01)])
+def test_mixed_accuracy_vs_fp64(ge, ics, dims, n, theta, eps2):
+    st = ics.two_disks2d(n, seed=5) if dims == 2 else ics.plummer3d(n, seed=5)
+    res = {}
+    for prec in (0, MIXED):
+        p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4, dt=1e-3,
+                              precision=prec)
+        with ge.Simulation(p) as s:
+            s.upload(st)
+            s.step(1)
+            out = s.download()
+            idx = np.sort(np.random.default_rng(1).choice(n, 4096, replace=False)).astype(np.uint32)
+            ref = s.direct_sum_f64(idx)
+        got = [out["ax"][idx], out["ay"][idx]] + ([out["az"][idx]] if dims == 3 else [])
+        res[prec] = np.median(_rel(got, ref))
+    print(f"median error vs FP64: fast {res[0]:.2e} mixed {res[MIXED]:.2e}")
+    assert res[MIXED] <= 1e-3
+    assert res[MIXED] < 0.2 * res[0]
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_mixed_kahan_leapfrog(ge, dims):
+    """One particle (no force) drifting 1e-8 per step from x = 1: each step is
+    below half an ulp of 1.0, so the plain update never moves it; the
+    compensated update moves it by the full 1000 * 1e-8 after 1000 steps."""
+    st = {"x": np.array([1.0], np.float32), "y": np.array([1.0], np.float32),
+          "vx": np.array([1e-5], np.float32), "vy": np.array([0.0], np.float32),
+          "m": np.array([1.0], np.float32)}
+    if dims == 3:
+        st["z"] = np.array([1.0], np.float32)
+        st["vz"] = np.array([-1e-5], np.float32)
+    res = {}
+    for prec in (0, MIXED):
+        p = ge.default_params(dims, G=1.0, theta=0.7, eps2=1e-4, dt=1e-3, precision=prec)
+        with ge.Simulation(p) as s:
+            s.upload(st)
+            s.step(1000)
+            res[prec] = s.download()
+    assert res[0]["x"][0] == np.float32(1.0)
+    assert abs(float(res[MIXED]["x"][0]) - (1.0 + 1e-5)) <= 2e-7
+    if dims == 3:
+        assert abs(float(res[MIXED]["z"][0]) - (1.0 - 1e-5)) <= 2e-7
+
+
+def test_mixed_batch_equals_alone(ge, ics):
+    p = ge.default_params(2, G=1.0, theta=0.6, softening=0.01, dt=1e-3, precision=MIXED)
+    sizes = [3000, 1, 17000, 4097]
+    sts = [ics.disk2d(n, seed=20 + k, center=(2.0 * k, 0.0)) for k, n in enumerate(sizes)]
+    with ge.Simulation(p) as b:
+        h = [b.add_sim(s) for s in sts]
+        b.step(3)
+        for k, s in enumerate(sts):
+            got = b.download_sim(h[k])
+            with ge.Simulation(p) as a:
+                a.upload(s)
+                a.step(3)
+                ref = a.download()
+            for key in ("x", "y", "vx", "vy", "ax", "ay", "id"):
+                assert np.array_equal(got[key], ref[key]), key
