@@ -65,6 +65,28 @@ class Stats(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    """ge_server_config (include/ge_bh.h)."""
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_int64), ("frac_2d", C.c_double), ("max_sims", C.c_int32),
+        ("reserved", C.c_int32 * 7), ("params", Params * 2),
+    ]
+
+
+class ServerStats(C.Structure):
+    """ge_server_stats (include/ge_bh.h)."""
+    _fields_ = [
+        ("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+        ("queued", C.c_int64), ("running", C.c_int64), ("iterations", C.c_int64),
+        ("particle_steps", C.c_int64), ("busy_s", C.c_double), ("step_ms_p50", C.c_double),
+        ("step_ms_p99", C.c_double), ("latency_s_p50", C.c_double),
+        ("latency_s_p99", C.c_double), ("pool_bytes", C.c_int64 * 2),
+        ("pool_capacity", C.c_int64 * 2),
+    ]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 _vp = C.c_void_p
 _LIB = None
 
@@ -106,6 +128,26 @@ SIGNATURES = {
     "ge_batch_list": ([_vp, C.c_int32, _vp, C.POINTER(C.c_int32)], C.c_int),
     "ge_batch_query": ([_vp, C.c_int32, _vp, _vp, _vp], C.c_int),
     "ge_batch_download_sim": ([_vp, C.c_int32] + [_vp] * 11, C.c_int),
+    "ge_batch_remove_sims": ([_vp, C.c_int32, _vp], C.c_int),
+    "ge_step_async": ([_vp, C.c_int32], C.c_int),
+    "ge_step_wait": ([_vp], C.c_int),
+    "ge_reserve": ([_vp, C.c_int64, C.c_int64], C.c_int),
+    "ge_memory_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
+    "ge_estimate_bytes": ([C.POINTER(Params), C.c_int64, C.c_int64, C.POINTER(C.c_int64)],
+                          C.c_int),
+    "ge_server_create": ([C.POINTER(ServerConfig), C.POINTER(_vp)], C.c_int),
+    "ge_server_destroy": ([_vp], C.c_int),
+    "ge_server_last_error": ([_vp], C.c_char_p),
+    "ge_server_submit": ([_vp, C.c_int32, C.c_int64] + [_vp] * 7 + [C.c_int32,
+                         C.POINTER(C.c_int64)], C.c_int),
+    "ge_server_start": ([_vp], C.c_int),
+    "ge_server_stop": ([_vp], C.c_int),
+    "ge_server_poll": ([_vp, C.POINTER(C.c_int32)], C.c_int),
+    "ge_server_wait": ([_vp, C.c_int64, C.c_double], C.c_int),
+    "ge_server_status": ([_vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                          C.POINTER(C.c_double)], C.c_int),
+    "ge_server_take": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
+    "ge_server_get_stats": ([_vp, C.POINTER(ServerStats)], C.c_int),
 }
 NOALLOC_MAX_N = 262144   # GE_NOALLOC_MAX_N
 
@@ -256,6 +298,25 @@ class Simulation:
         self._check(lib().ge_batch_remove_sim(self._h, int(sim)))
         self.n = int(self.stats().n)
 
+    def remove_sims(self, sims):
+        h = np.ascontiguousarray(sims, np.int32)
+        self._check(lib().ge_batch_remove_sims(self._h, len(h), _ptr(h)))
+        self.n = int(self.stats().n)
+
+    def step_async(self, nsteps=1):
+        self._check(lib().ge_step_async(self._h, int(nsteps)))
+
+    def step_wait(self):
+        self._check(lib().ge_step_wait(self._h))
+
+    def reserve(self, n, sims=1):
+        self._check(lib().ge_reserve(self._h, int(n), int(sims)))
+
+    def memory_bytes(self):
+        b = C.c_int64(0)
+        self._check(lib().ge_memory_bytes(self._h, C.byref(b)))
+        return b.value
+
     def sims(self):
         """Handles of the simulations, in slot order."""
         cnt = C.c_int32(0)
@@ -374,3 +435,104 @@ class Simulation:
                                          _ptr(out["child"])))
         k = cnt.value
         return {a: v[:k] for a, v in out.items()}
+
+
+def estimate_bytes(params, n, sims=1):
+    """Device bytes of a context with these parameters after reserve(n, sims)."""
+    b = C.c_int64(0)
+    rc = lib().ge_estimate_bytes(C.byref(params), int(n), int(sims), C.byref(b))
+    if rc != 0:
+        raise GeError(rc, "ge_estimate_bytes failed")
+    return b.value
+
+
+class Server:
+    """Continuous-batching server (ge_server): requests are simulations with a
+    step count, run in a 2D and a 3D pool sized from an HBM budget."""
+
+    def __init__(self, hbm_budget_bytes, params2d=None, params3d=None, frac_2d=0.5,
+                 max_sims=1024):
+        cfg = ServerConfig()
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        cfg.frac_2d = float(frac_2d)
+        cfg.max_sims = int(max_sims)
+        cfg.params[0] = params2d if params2d is not None else default_params(2)
+        cfg.params[1] = params3d if params3d is not None else default_params(3)
+        h = _vp()
+        rc = lib().ge_server_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise GeError(rc, "ge_server_create failed")
+        self._h = h
+        self._keep = {}
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().ge_server_last_error(self._h)
+            raise GeError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ge_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, state, steps):
+        """Queue a simulation (dict as Simulation.upload; 3D when it has z)."""
+        g = state.get
+        dims = 3 if g("z") is not None else 2
+        a = {k: _f32(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        rid = C.c_int64(0)
+        self._check(lib().ge_server_submit(self._h, dims, len(a["x"]), _ptr(a["x"]), _ptr(a["y"]),
+                                           _ptr(a["z"]), _ptr(a["vx"]), _ptr(a["vy"]),
+                                           _ptr(a["vz"]), _ptr(a["m"]), int(steps), C.byref(rid)))
+        self._keep[rid.value] = (dims, len(a["x"]))
+        return rid.value
+
+    def start(self):
+        self._check(lib().ge_server_start(self._h))
+
+    def stop(self):
+        self._check(lib().ge_server_stop(self._h))
+
+    def poll(self):
+        st = C.c_int32(0)
+        self._check(lib().ge_server_poll(self._h, C.byref(st)))
+        return bool(st.value)
+
+    def wait(self, rid, timeout_s=600.0):
+        self._check(lib().ge_server_wait(self._h, int(rid), float(timeout_s)))
+
+    def status(self, rid):
+        st, done, lat = C.c_int32(0), C.c_int32(0), C.c_double(0)
+        self._check(lib().ge_server_status(self._h, int(rid), C.byref(st), C.byref(done),
+                                           C.byref(lat)))
+        return st.value, done.value, lat.value
+
+    def take(self, rid):
+        dims, n = self._keep.pop(rid)
+        out = {k: np.empty(n, np.float32) for k in ("x", "y", "vx", "vy", "ax", "ay", "m")}
+        if dims == 3:
+            for k in ("z", "vz", "az"):
+                out[k] = np.empty(n, np.float32)
+        out["id"] = np.empty(n, np.uint32)
+        g = out.get
+        self._check(lib().ge_server_take(
+            self._h, int(rid), *[_ptr(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay",
+                                                       "az", "m", "id")]))
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        self._check(lib().ge_server_get_stats(self._h, C.byref(s)))
+        return s

@@ -30,6 +30,14 @@ using namespace ge;
 
 namespace gehost {
 
+// Device allocations of one buffer set.  A dry list only adds up the bytes
+// (ge_estimate_bytes): its pointers are placeholders that are never used.
+struct AllocList {
+    std::vector<void *> ptrs;
+    size_t bytes = 0;
+    bool dry = false;
+};
+
 // Device buffers sized for a particle capacity; replaced as a whole when the
 // capacity grows (the particle state is copied across).
 struct Buffers {
@@ -41,7 +49,7 @@ struct Buffers {
     bool prev = false;     // prevVel arrays allocated
     bool pinned = false;   // pin flag arrays allocated
     bool mixed = false;    // GE_PREC_MIXED arrays allocated
-    std::vector<void *> allocs;
+    AllocList allocs;
 };
 
 // Segment tables, sized for a segment, tile and particle capacity.
@@ -51,7 +59,7 @@ struct SegBuffers {
     float4 *box = nullptr;
     uint32_t *boxmm = nullptr, *root_begin = nullptr, *root_end = nullptr;
     uint32_t *hist = nullptr, *status = nullptr;
-    std::vector<void *> allocs;
+    AllocList allocs;
 };
 
 struct SimRec {
@@ -60,17 +68,26 @@ struct SimRec {
     int64_t step0;   // context steps when the simulation was added
 };
 
-inline void free_all(std::vector<void *> &v) {
-    for (void *q : v) cudaFree(q);
-    v.clear();
+inline void free_all(AllocList &L) {
+    if (!L.dry)
+        for (void *q : L.ptrs) cudaFree(q);
+    L.ptrs.clear();
+    L.bytes = 0;
 }
 
 template <typename T>
-cudaError_t dalloc(std::vector<void *> &list, T **p, size_t count) {
+cudaError_t dalloc(AllocList &L, T **p, size_t count) {
+    const size_t bytes = sizeof(T) * (count ? count : 1);
+    if (L.dry) {
+        L.bytes += (bytes + 255) & ~size_t(255);
+        *p = reinterpret_cast<T *>(uintptr_t(256));
+        return cudaSuccess;
+    }
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return e;
-    list.push_back(q);
+    L.ptrs.push_back(q);
+    L.bytes += bytes;
     *p = (T *)q;
     return cudaSuccess;
 }
@@ -94,8 +111,10 @@ struct ge_ctx {
     SegBuffers sb;
     Segs g{};
     std::vector<SimRec> sims;     // in slot order
+    int64_t sims_reserved = 0;    // segment capacity asked for by ge_reserve
     int32_t next_handle = 1;
     int64_t total_steps = 0;
+    int32_t pending_steps = 0;    // steps enqueued by ge_step_async, not yet waited for
     std::vector<uint32_t> h_off, h_tile_base;
     uint32_t *d_err = nullptr;
     uint32_t *h_meta = nullptr;   // pinned copy of the tree meta words
@@ -235,7 +254,7 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     GE_CHECK(c, dalloc(L, &t.lvl_alloc, kMaxLevels + 2));
     GE_CHECK(c, dalloc(L, &t.meta, 16));
     GE_CHECK(c, dalloc(L, &t.tl, kTimeline));
-    GE_CHECK(c, cudaMemsetAsync(t.meta, 0, 16 * sizeof(uint32_t), c->stream));
+    if (!L.dry) GE_CHECK(c, cudaMemsetAsync(t.meta, 0, 16 * sizeof(uint32_t), c->stream));
     GE_CHECK(c, dalloc(L, &nb.d_inter, 1));
     return GE_OK;
 }
@@ -252,7 +271,7 @@ int alloc_mixed(ge_ctx *c, Buffers &nb) {
         for (int a = 0; a < 6; a++) {
             if (D == 2 && (a == 2 || a == 5)) continue;
             GE_CHECK(c, dalloc(L, kp[a], N));
-            GE_CHECK(c, cudaMemsetAsync(*kp[a], 0, sizeof(float) * N, c->stream));
+            if (!L.dry) GE_CHECK(c, cudaMemsetAsync(*kp[a], 0, sizeof(float) * N, c->stream));
         }
     }
     Tree &t = nb.tree;
@@ -300,7 +319,7 @@ int64_t node_cap_for(const ge_ctx *c, int64_t n, int64_t S, int64_t slack) {
 
 // Makes the buffers hold n particles in S simulations.  With `keep` the
 // current c->n particles survive a reallocation (they move to st[0]).
-int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep) {
+int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep, bool exact = false) {
     const int D = c->p.dims;
     const int64_t slack = build_node_slack(D, c->num_sms);
     if (slack <= 0) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");
@@ -313,7 +332,7 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep) {
     // a live context grows by half again at least, so adding simulations one
     // by one reallocates O(log) times
     int64_t cap = n, scap = S;
-    if (keep && ob.cap_n > 0) {
+    if (keep && ob.cap_n > 0 && !exact) {
         cap = std::max(n, ob.cap_n + ob.cap_n / 2);
         scap = S + S / 2;
         const int64_t lim = D == 2 ? (1ll << 28) - 1 : (1ll << 31) - 1;
@@ -347,6 +366,32 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep) {
     return GE_OK;
 }
 
+// Segment tables for seg_cap simulations over n_cap particles.
+int alloc_segs(ge_ctx *c, SegBuffers &nb, int64_t seg_cap, int64_t n_cap, int64_t tiles) {
+    nb.seg_cap = std::max<int64_t>(seg_cap, 1);
+    nb.n_cap = n_cap;
+    nb.tile_cap = std::max<int64_t>(tiles, nb.n_cap / kSortTile + nb.seg_cap + 1);
+    const size_t SC = (size_t)nb.seg_cap, TC = (size_t)nb.tile_cap;
+    auto &L = nb.allocs;
+    GE_CHECK(c, dalloc(L, &nb.off, SC + 1));
+    GE_CHECK(c, dalloc(L, &nb.tile_base, SC + 1));
+    GE_CHECK(c, dalloc(L, &nb.seg_of, (size_t)nb.n_cap));
+    GE_CHECK(c, dalloc(L, &nb.tile_seg, TC));
+    GE_CHECK(c, dalloc(L, &nb.box, SC));
+    GE_CHECK(c, dalloc(L, &nb.boxmm, 6 * SC));
+    GE_CHECK(c, dalloc(L, &nb.root_begin, SC));
+    GE_CHECK(c, dalloc(L, &nb.root_end, SC));
+    GE_CHECK(c, dalloc(L, &nb.hist, (size_t)kMaxPasses * SC * 256));
+    GE_CHECK(c, dalloc(L, &nb.status, (size_t)kMaxPasses * TC * 256));
+    if (!L.dry) {
+        Segs all{};
+        all.S = (int)nb.seg_cap;
+        all.boxmm = nb.boxmm;
+        GE_CHECK(c, launch_reset_boxes(all, c->stream));
+    }
+    return GE_OK;
+}
+
 // Rebuilds the segment tables from c->sims (after any change of the
 // simulations or of the capacity) and binds them to the sort scratch.
 int sync_segments(ge_ctx *c) {
@@ -362,32 +407,13 @@ int sync_segments(ge_ctx *c) {
     SegBuffers &sb = c->sb;
     if (S > sb.seg_cap || tiles > sb.tile_cap || c->b.cap_n > sb.n_cap) {
         SegBuffers nb;
-        nb.seg_cap = std::max<int64_t>(std::max<int64_t>(S, 1), sb.seg_cap + sb.seg_cap / 2);
-        nb.n_cap = c->b.cap_n;
-        nb.tile_cap = std::max<int64_t>(tiles, nb.n_cap / kSortTile + nb.seg_cap + 1);
-        const size_t SC = (size_t)nb.seg_cap, TC = (size_t)nb.tile_cap;
-        auto &L = nb.allocs;
-        cudaError_t e = cudaSuccess;
-        if (e == cudaSuccess) e = dalloc(L, &nb.off, SC + 1);
-        if (e == cudaSuccess) e = dalloc(L, &nb.tile_base, SC + 1);
-        if (e == cudaSuccess) e = dalloc(L, &nb.seg_of, (size_t)nb.n_cap);
-        if (e == cudaSuccess) e = dalloc(L, &nb.tile_seg, TC);
-        if (e == cudaSuccess) e = dalloc(L, &nb.box, SC);
-        if (e == cudaSuccess) e = dalloc(L, &nb.boxmm, 6 * SC);
-        if (e == cudaSuccess) e = dalloc(L, &nb.root_begin, SC);
-        if (e == cudaSuccess) e = dalloc(L, &nb.root_end, SC);
-        if (e == cudaSuccess) e = dalloc(L, &nb.hist, (size_t)kMaxPasses * SC * 256);
-        if (e == cudaSuccess) e = dalloc(L, &nb.status, (size_t)kMaxPasses * TC * 256);
-        if (e == cudaSuccess) {
-            Segs all{};
-            all.S = (int)nb.seg_cap;
-            all.boxmm = nb.boxmm;
-            e = launch_reset_boxes(all, c->stream);
-        }
-        if (e != cudaSuccess) {
+        const int64_t scap = std::max<int64_t>(std::max<int64_t>(S, c->sims_reserved),
+                                               sb.seg_cap + sb.seg_cap / 2);
+        int rc = alloc_segs(c, nb, scap, c->b.cap_n, tiles);
+        if (rc) {
             cudaStreamSynchronize(c->stream);
-            free_all(L);
-            return cuda_fail(c, e, "segment tables");
+            free_all(nb.allocs);
+            return rc;
         }
         GE_CHECK(c, cudaStreamSynchronize(c->stream));
         free_all(sb.allocs);
@@ -755,6 +781,7 @@ int ge_upload(ge_ctx *c, int64_t n, const float *x, const float *y, const float 
               const float *vx, const float *vy, const float *vz, const float *m,
               const uint32_t *id, const float *ax, const float *ay, const float *az) {
     if (!c) return GE_ERR_ARG;
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
     int rc = check_host_arrays(c, n, x, y, z, vx, vy, vz, m);
     if (rc) return rc;
     if ((rc = ensure_capacity(c, n, 1, false))) return rc;
@@ -806,16 +833,27 @@ int ge_download_prev_vel(ge_ctx *c, float *pvx, float *pvy, float *pvz) {
     return GE_OK;
 }
 
-int ge_step(ge_ctx *c, int32_t nsteps) {
+int ge_step_async(ge_ctx *c, int32_t nsteps) {
     int rc = require_state(c);
     if (rc) return rc;
     if (nsteps < 0) return fail(c, GE_ERR_ARG, "nsteps must be >= 0");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
     if (nsteps == 0) return GE_OK;
     GE_CHECK(c, cudaEventRecord(c->ev[6], c->stream));
     for (int k = 0; k < nsteps; k++)
         if ((rc = enqueue_frame(c, nullptr))) return rc;
     GE_CHECK(c, cudaEventRecord(c->ev[7], c->stream));
-    rc = check_device(c);
+    c->pending_steps = nsteps;
+    c->tree_valid = false;
+    return GE_OK;
+}
+
+int ge_step_wait(ge_ctx *c) {
+    if (!c) return GE_ERR_ARG;
+    const int32_t nsteps = c->pending_steps;
+    if (!nsteps) return GE_OK;
+    c->pending_steps = 0;
+    int rc = check_device(c);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
     c->stats.ms_last_step = ms / (float)nsteps;
@@ -828,6 +866,12 @@ int ge_step(ge_ctx *c, int32_t nsteps) {
         c->stats.interactions = v;
     }
     return rc;
+}
+
+int ge_step(ge_ctx *c, int32_t nsteps) {
+    int rc = ge_step_async(c, nsteps);
+    if (rc) return rc;
+    return ge_step_wait(c);
 }
 
 int ge_batch_step(ge_ctx *c, int32_t nsteps) { return ge_step(c, nsteps); }
@@ -1017,12 +1061,60 @@ int ge_sums_f64(ge_ctx *c, double *out) {
     return GE_OK;
 }
 
+// --- capacity and memory ------------------------------------------------
+
+int ge_reserve(ge_ctx *c, int64_t n, int64_t sims) {
+    if (!c) return GE_ERR_ARG;
+    if (n < 1 || sims < 1) return fail(c, GE_ERR_ARG, "n and sims must be >= 1");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    c->sims_reserved = std::max<int64_t>(c->sims_reserved, sims);
+    int rc = ensure_capacity(c, std::max<int64_t>(n, c->n), std::max<int64_t>(sims, (int64_t)c->sims.size()),
+                             true, true);
+    if (rc) return rc;
+    if ((rc = ensure_mode(c))) return rc;
+    return sync_segments(c);
+}
+
+int ge_memory_bytes(ge_ctx *c, int64_t *bytes) {
+    if (!c || !bytes) return GE_ERR_ARG;
+    *bytes = (int64_t)(c->b.allocs.bytes + c->sb.allocs.bytes);
+    return GE_OK;
+}
+
+int ge_estimate_bytes(const ge_params *p, int64_t n, int64_t sims, int64_t *bytes) {
+    if (!bytes) return GE_ERR_ARG;
+    ge_ctx tmp;
+    int rc = validate(&tmp, p);
+    if (rc) return rc;
+    if (n < 1 || sims < 1) return GE_ERR_ARG;
+    tmp.p = *p;
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return GE_ERR_NO_DEVICE;
+    tmp.num_sms = prop.multiProcessorCount;
+    const int64_t slack = build_node_slack(p->dims, tmp.num_sms);
+    if (slack <= 0) return GE_ERR_CUDA;
+    Buffers nb;
+    nb.allocs.dry = true;
+    rc = alloc_buffers(&tmp, nb, n, node_cap_for(&tmp, n, sims, slack), p->track_prev_vel != 0,
+                       false);
+    if (!rc && p->precision == GE_PREC_MIXED) rc = alloc_mixed(&tmp, nb);
+    SegBuffers sb;
+    sb.allocs.dry = true;
+    if (!rc) rc = alloc_segs(&tmp, sb, sims, n, n / kSortTile + sims + 1);
+    if (rc) return rc;
+    *bytes = (int64_t)(nb.allocs.bytes + sb.allocs.bytes);
+    return GE_OK;
+}
+
 // --- batched simulations ------------------------------------------------
 
 int ge_batch_add_sim(ge_ctx *c, int64_t n, const float *x, const float *y, const float *z,
                      const float *vx, const float *vy, const float *vz, const float *m,
                      const uint32_t *id, int32_t *sim) {
     if (!c) return GE_ERR_ARG;
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
     int rc = check_host_arrays(c, n, x, y, z, vx, vy, vz, m);
     if (rc) return rc;
     if (c->next_handle == INT32_MAX) return fail(c, GE_ERR_CAPACITY, "simulation handles exhausted");
@@ -1043,26 +1135,48 @@ int ge_batch_add_sim(ge_ctx *c, int64_t n, const float *x, const float *y, const
     return GE_OK;
 }
 
-int ge_batch_remove_sim(ge_ctx *c, int32_t sim) {
-    if (!c) return GE_ERR_ARG;
-    const int r = find_sim(c, sim);
-    if (r < 0) return fail(c, GE_ERR_ARG, "no such simulation");
-    const int64_t lo = c->h_off[(size_t)r], hi = c->h_off[(size_t)r + 1];
-    const int64_t n = c->n;
-    if (hi - lo < n) {
-        // the simulations after it move down by its size (through the other
-        // state buffer, so no copy overlaps itself)
-        const State &src = c->b.st[c->cur];
-        const State &dst = c->b.st[c->cur ^ 1];
-        int rc = copy_range(c, dst, 0, src, 0, lo, c->b.prev, c->b.pinned);
-        if (!rc) rc = copy_range(c, dst, lo, src, hi, n - hi, c->b.prev, c->b.pinned);
-        if (rc) return rc;
-        c->cur ^= 1;
+int ge_batch_remove_sims(ge_ctx *c, int32_t count, const int32_t *sims) {
+    if (!c || count < 0 || (count && !sims)) return GE_ERR_ARG;
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    std::vector<char> drop(c->sims.size(), 0);
+    for (int32_t k = 0; k < count; k++) {
+        const int r = find_sim(c, sims[k]);
+        if (r < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+        drop[(size_t)r] = 1;
     }
-    c->sims.erase(c->sims.begin() + r);
-    c->n = n - (hi - lo);
+    size_t first_drop = 0;
+    while (first_drop < drop.size() && !drop[first_drop]) first_drop++;
+    bool suffix = true;
+    for (size_t r = first_drop; r < drop.size(); r++) suffix = suffix && drop[r];
+    if (suffix) {   // only the last simulations go: nothing moves
+        c->n = c->h_off[first_drop];
+        c->sims.resize(first_drop);
+        return sync_segments(c);
+    }
+    // the kept simulations move down, in order, through the other state
+    // buffer (no copy overlaps itself); runs of kept simulations move as one
+    const State &src = c->b.st[c->cur];
+    const State &dst = c->b.st[c->cur ^ 1];
+    std::vector<SimRec> kept;
+    int64_t out = 0;
+    size_t r = 0;
+    bool moved = false;
+    while (r < c->sims.size()) {
+        if (drop[r]) { r++; moved = true; continue; }
+        const size_t r0 = r;
+        while (r < c->sims.size() && !drop[r]) kept.push_back(c->sims[r++]);
+        const int64_t lo = c->h_off[r0], hi = c->h_off[r];
+        int rc = copy_range(c, dst, out, src, lo, hi - lo, c->b.prev, c->b.pinned);
+        if (rc) return rc;
+        out += hi - lo;
+    }
+    if (moved) c->cur ^= 1;
+    c->sims.swap(kept);
+    c->n = out;
     return sync_segments(c);
 }
+
+int ge_batch_remove_sim(ge_ctx *c, int32_t sim) { return ge_batch_remove_sims(c, 1, &sim); }
 
 int ge_batch_list(ge_ctx *c, int32_t cap, int32_t *sims, int32_t *count) {
     if (!c || !count) return GE_ERR_ARG;

@@ -123,6 +123,13 @@ int ge_download_prev_vel(ge_ctx *ctx, float *pvx, float *pvy, float *pvz);
 /* nsteps full frames on the resident state (globalLogic.cpp:1155-1370 /
    :1584-1719 with dt != 0), all on the device. */
 int ge_step(ge_ctx *ctx, int32_t nsteps);
+/* The same in two halves: ge_step_async enqueues the frames on the context's
+   stream and returns at once; ge_step_wait waits for them and reports
+   errors and timing.  Contexts on different streams then step concurrently.
+   Between the two calls only ge_step_wait, ge_sync and ge_get_stats may be
+   used on the context. */
+int ge_step_async(ge_ctx *ctx, int32_t nsteps);
+int ge_step_wait(ge_ctx *ctx);
 /* one frame with per-stage CUDA-event timing into ge_stats.stage_ms */
 int ge_profile_step(ge_ctx *ctx);
 /* One frame on HOST buffers: upload, step, download, all inside the call.
@@ -218,6 +225,8 @@ int ge_batch_add_sim(ge_ctx *ctx, int64_t n, const float *x, const float *y, con
                      const uint32_t *id, int32_t *sim);
 /* removes a sim; the others keep their state */
 int ge_batch_remove_sim(ge_ctx *ctx, int32_t sim);
+/* removes count sims at once (one compaction) */
+int ge_batch_remove_sims(ge_ctx *ctx, int32_t count, const int32_t *sims);
 /* number of sims and, when sims != NULL, up to cap handles in slot order */
 int ge_batch_list(ge_ctx *ctx, int32_t cap, int32_t *sims, int32_t *count);
 /* a sim's particle count, first slot in the context's arrays, and steps taken
@@ -227,6 +236,89 @@ int ge_batch_query(ge_ctx *ctx, int32_t sim, int64_t *n, int64_t *offset, int64_
 int ge_batch_download_sim(ge_ctx *ctx, int32_t sim, float *x, float *y, float *z, float *vx,
                           float *vy, float *vz, float *ax, float *ay, float *az, float *m,
                           uint32_t *id);
+
+/* --- device memory ------------------------------------------------------
+ * No counterpart in the reference.  A context's device memory is its
+ * particle capacity (state, sort scratch, node arrays sized node_cap_factor
+ * times the capacity) plus per-simulation tables.  ge_reserve sizes it up
+ * front for n particles in up to `sims` simulations, so that later uploads
+ * and additions within those limits never reallocate; ge_memory_bytes
+ * reports what the context holds; ge_estimate_bytes reports what a context
+ * with these parameters would hold after ge_reserve(n, sims). */
+int ge_reserve(ge_ctx *ctx, int64_t n, int64_t sims);
+int ge_memory_bytes(ge_ctx *ctx, int64_t *bytes);
+int ge_estimate_bytes(const ge_params *p, int64_t n, int64_t sims, int64_t *bytes);
+
+/* --- serving ------------------------------------------------------------
+ * No counterpart in the reference.  A server runs requests -- a simulation
+ * plus a step count -- with continuous batching under a device-memory
+ * budget.  It owns two batch contexts (pools: params[0] for 2D requests,
+ * params[1] for 3D), each reserved once at creation from its share of
+ * hbm_budget_bytes (frac_2d for 2D, the rest for 3D), so the pools together
+ * never hold more than the budget and admission never allocates.  The loop
+ * (a worker thread after ge_server_start, or one iteration per
+ * ge_server_poll on the calling thread) admits queued requests first come
+ * first served while their pool has room (particles and max_sims), takes
+ * one step of every admitted simulation in both pools (the pools' kernels
+ * overlap on the device), and retires simulations that reached their step
+ * count: their final state is copied to host memory and their room freed.
+ * A result equals the same request run alone on a context with the same
+ * parameters.  submit / status / wait / take / get_stats may be called from
+ * any thread. */
+typedef struct ge_server ge_server;
+
+typedef enum {
+    GE_REQ_QUEUED = 0,
+    GE_REQ_RUNNING = 1,
+    GE_REQ_DONE = 2,
+    GE_REQ_FAILED = 3
+} ge_request_state;
+
+typedef struct {
+    int64_t hbm_budget_bytes;  /* device memory of both pools together */
+    double frac_2d;            /* share of the budget for the 2D pool */
+    int32_t max_sims;          /* simulations per pool at once */
+    int32_t reserved[7];
+    ge_params params[2];       /* [0]: 2D pool (dims 2), [1]: 3D pool (dims 3) */
+} ge_server_config;
+
+typedef struct {
+    int64_t submitted, completed, failed, queued, running;
+    int64_t iterations;          /* batched steps taken */
+    int64_t particle_steps;      /* particles stepped, summed over iterations */
+    double busy_s;               /* wall time spent in batched steps */
+    double step_ms_p50, step_ms_p99;      /* wall time of one batched step */
+    double latency_s_p50, latency_s_p99;  /* submit -> done, completed requests */
+    int64_t pool_bytes[2];       /* device memory held by each pool */
+    int64_t pool_capacity[2];    /* particles each pool runs at once */
+} ge_server_stats;
+
+int ge_server_create(const ge_server_config *cfg, ge_server **out);
+int ge_server_destroy(ge_server *srv);
+const char *ge_server_last_error(const ge_server *srv);
+/* queues a request (the host arrays are copied); *request receives its id.
+   GE_ERR_CAPACITY when n exceeds its pool's capacity. */
+int ge_server_submit(ge_server *srv, int32_t dims, int64_t n, const float *x, const float *y,
+                     const float *z, const float *vx, const float *vy, const float *vz,
+                     const float *m, int32_t steps, int64_t *request);
+int ge_server_start(ge_server *srv);
+/* stops the worker after its current iteration; returns the loop's error */
+int ge_server_stop(ge_server *srv);
+/* one loop iteration on the calling thread (server not started);
+   *stepped = 1 when a batched step ran */
+int ge_server_poll(ge_server *srv, int32_t *stepped);
+/* waits (worker running) until the request is done; GE_ERR_TIMEOUT after
+   timeout_s seconds */
+int ge_server_wait(ge_server *srv, int64_t request, double timeout_s);
+/* state (ge_request_state), steps taken, and submit-to-done seconds (-1 until done) */
+int ge_server_status(ge_server *srv, int64_t request, int32_t *state, int32_t *steps_done,
+                     double *latency_s);
+/* copies a finished request's final state (its particles in Morton order,
+   id = index in the submitted arrays) and releases it */
+int ge_server_take(ge_server *srv, int64_t request, float *x, float *y, float *z, float *vx,
+                   float *vy, float *vz, float *ax, float *ay, float *az, float *m,
+                   uint32_t *id);
+int ge_server_get_stats(ge_server *srv, ge_server_stats *out);
 
 /* --- tree export: the reference's globalNodes in DFS pre-order --------- */
 /* Returns the node count in *count (with several sims: every sim's tree, one

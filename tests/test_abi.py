@@ -52,6 +52,34 @@ def test_struct_layouts_match_header(ge):
     assert C.sizeof(ge.Stats) == 88
 
 
+def test_struct_layouts_match_c_compiler(ge, tmp_path):
+    """sizeof / offsetof of every ABI struct as the C compiler lays it out
+    against the ctypes mirrors."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    structs = {"ge_params": ge.Params, "ge_stats": ge.Stats,
+               "ge_server_config": ge.ServerConfig, "ge_server_stats": ge.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ge_bh.h"', 'int main(void) {']
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-I", inc, "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for f in cls._fields_:
+            assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
+
+
 @pytest.mark.skipif(gpu_available(), reason="checks the no-GPU refusal")
 def test_no_cpu_fallback_without_gpu(ge):
     with pytest.raises(ge.GeError) as ei:
