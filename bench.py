@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-frames", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, batched and serving measurements")
+    ap.add_argument("--batch-sims", type=int, default=512)
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
     return ap.parse_args()
 
 
@@ -204,6 +208,195 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+LAUNCHES_PER_STEP = {"fast": 11, "mixed": 13}   # 2D: box 2, keys 1, sort 5, gather 1, build 1,
+                                                # walk 1 (+ moments 2 in the mixed mode)
+
+
+def _err(got, ref):
+    num = sum((got[k] - ref[k]) ** 2 for k in range(len(ref)))
+    den = sum(ref[k] ** 2 for k in range(len(ref)))
+    return np.sqrt(num / np.maximum(den, 1e-300))
+
+
+def _timed_steps(torch, stream, sim, K, flush=None):
+    """K single steps timed with CUDA events on the simulation's stream."""
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    torch.cuda.synchronize()
+    for k in range(K):
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush.zero_()
+        e0[k].record(stream)
+        sim.step(1)
+        e1[k].record(stream)
+    torch.cuda.synchronize()
+    return np.array([e0[k].elapsed_time(e1[k]) for k in range(K)])
+
+
+def bench_mixed(ge, torch, stream, st, n, flush, K=10):
+    """The two-disk workload in the mixed-precision mode at theta 0.6 (the
+    opening angle at which its median error is below 1e-3)."""
+    p = ge.default_params(2, G=1.0, theta=0.6, softening=SOFT, dt=DT, leaf_cap=LEAF,
+                          precision=ge.PREC_MIXED)
+    with ge.Simulation(p) as sim:
+        sim.set_stream(stream.cuda_stream)
+        sim.upload(st)
+        sim.step(3)
+        times = _timed_steps(torch, stream, sim, K, flush)
+        out = sim.download()
+        idx = np.sort(np.random.Generator(np.random.PCG64(1)).choice(
+            n, size=min(16384, n), replace=False)).astype(np.uint32)
+        ref = sim.direct_sum_f64(idx)
+        err = _err([out["ax"][idx], out["ay"][idx]], ref)
+        stage = np.array(sim.profile_step())
+    return {"workload": f"two-disk 2D, N={n}", "theta": 0.6, "precision": "mixed",
+            "value": n / (times.mean() * 1e-3), "unit": UNIT, "ms_per_step": float(times.mean()),
+            "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+            "steps": K, "stage_ms": {"kick_drift_bbox": stage[0], "keys": stage[1],
+                                     "sort": stage[2], "permute": stage[3],
+                                     "build_and_moments": stage[4], "walk": stage[5]},
+            "force_err_vs_fp64": {"median": float(np.median(err)),
+                                  "p99": float(np.percentile(err, 99)), "sample": int(len(idx))}}
+
+
+def bench_batched(ge, ics, torch, count, K=5, Kp=2):
+    """512 independent 2D disks, N log-uniform in [1024, 262144] (seed 2), theta
+    0.7, softening 0.01: one context stepping all of them (batched) against one
+    context per simulation stepped one after another (plain), in the
+    reference-arithmetic mode and in the mixed mode at theta 0.6."""
+    sizes = [int(v) for v in ics.batch_sizes(count=count, seed=2)]
+    sts = [ics.disk2d(nn, seed=1000 + k) for k, nn in enumerate(sizes)]
+    total = int(sum(sizes))
+    out = {"workload": f"{count} 2D disks, N log-uniform [1024, 262144], seed 2",
+           "particles": total, "softening": 0.01, "unit": UNIT,
+           "l2": "inputs larger than L2 (all simulations resident, several GB)"}
+    stream = torch.cuda.Stream()
+    rng = np.random.Generator(np.random.PCG64(1))
+    for mode, theta, prec in (("fast", 0.7, ge.PREC_FAST), ("mixed", 0.6, ge.PREC_MIXED)):
+        p = ge.default_params(2, G=1.0, theta=theta, softening=0.01, dt=DT, leaf_cap=LEAF,
+                              precision=prec)
+        res = {"theta": theta}
+        with ge.Simulation(p) as b:
+            b.set_stream(stream.cuda_stream)
+            b.reserve(total, count)
+            for s_ in sts:
+                b.add_sim(s_)
+            b.step(3)
+            times = _timed_steps(torch, stream, b, K)
+            res["batched"] = {"value": total / (times.mean() * 1e-3),
+                              "ms_per_step": float(times.mean()),
+                              "p50_ms": float(np.percentile(times, 50)),
+                              "p99_ms": float(np.percentile(times, 99)), "steps": K,
+                              "launches_per_step": LAUNCHES_PER_STEP[mode]}
+            stt = b.download()
+            idx = np.sort(rng.choice(total, size=8192, replace=False)).astype(np.uint32)
+            ref = b.direct_sum_f64(idx)
+            err = _err([stt["ax"][idx], stt["ay"][idx]], ref)
+            res["force_err_vs_fp64"] = {"median": float(np.median(err)),
+                                        "p99": float(np.percentile(err, 99)),
+                                        "sample": int(len(idx))}
+        ctxs = []
+        for s_ in sts:
+            c = ge.Simulation(p)
+            c.upload(s_)
+            ctxs.append(c)
+        for c in ctxs:
+            c.step(1)
+        torch.cuda.synchronize()
+        sweep = []
+        for _ in range(Kp):
+            t0 = time.perf_counter()
+            for c in ctxs:
+                c.step(1)
+            sweep.append(time.perf_counter() - t0)
+        for c in ctxs:
+            c.close()
+        tp = float(np.mean(sweep))
+        res["plain"] = {"value": total / tp, "ms_per_step": tp * 1e3, "steps": Kp,
+                        "how": "one context per simulation, stepped one after another "
+                               "(wall clock of a sweep; each ge_step waits for its frame)",
+                        "launches_per_step": LAUNCHES_PER_STEP[mode] * count}
+        res["batched_over_plain"] = res["batched"]["value"] / res["plain"]["value"]
+        out[mode] = res
+    return out
+
+
+def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
+    """Poisson arrivals (50 requests/s) for `seconds` seconds: 70% 2D disks, 30%
+    3D Plummer spheres, N log-uniform in [4096, 2097152], steps uniform in
+    [10, 500]; mixed precision (theta 0.6 in 2D, 0.5 in 3D, softening 0.01);
+    a 120 GB budget split between the 2D and 3D pools."""
+    import threading
+    rng = np.random.Generator(np.random.PCG64(seed))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 3) + 10))
+    arrivals = arrivals[arrivals < seconds]
+    reqs = []
+    for k, t in enumerate(arrivals):
+        dims = 2 if rng.random() < 0.7 else 3
+        n = int(np.exp(rng.uniform(np.log(4096), np.log(2097152))))
+        steps = int(rng.integers(10, 501))
+        reqs.append((float(t), dims, n, steps, 5000 + k))
+    sts = [ics.disk2d(n, seed=sd) if d == 2 else ics.plummer3d(n, seed=sd)
+           for _, d, n, _, sd in reqs]
+    p2 = ge.default_params(2, G=1.0, theta=0.6, softening=0.01, dt=DT, precision=ge.PREC_MIXED)
+    p3 = ge.default_params(3, G=1.0, theta=0.5, softening=0.01, dt=DT, precision=ge.PREC_MIXED)
+    mem2 = sum(n * 2 for _, d, n, _, _ in reqs if d == 2) or 1
+    mem3 = sum(n * 3 for _, d, n, _, _ in reqs if d == 3) or 1
+    frac = mem2 / (mem2 + mem3)
+    srv = ge.Server(budget, p2, p3, frac_2d=frac, max_sims=1024)
+    ids = [None] * len(reqs)
+    srv.start()
+    t0 = time.perf_counter()
+
+    def feeder():
+        for k, (t, _, _, steps, _) in enumerate(reqs):
+            dt_ = t - (time.perf_counter() - t0)
+            if dt_ > 0:
+                time.sleep(dt_)
+            ids[k] = srv.submit(sts[k], steps)
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    for r in ids:
+        srv.wait(r, 1800.0)
+    wall = time.perf_counter() - t0
+    srv.stop()
+    s = srv.stats()
+    errs = []
+    check = [k for k in range(len(reqs))][:: max(1, len(reqs) // 8)][:8]
+    outs = {k: srv.take(ids[k]) for k in check}
+    for k in check:
+        d = reqs[k][1]
+        o = outs[k]
+        with ge.Simulation(p2 if d == 2 else p3) as c:
+            c.upload(o)
+            idx = np.sort(rng.choice(len(o["x"]), size=min(1024, len(o["x"])),
+                                     replace=False)).astype(np.uint32)
+            ref = c.direct_sum_f64(idx)
+        got = [o["ax"][idx], o["ay"][idx]] + ([o["az"][idx]] if d == 3 else [])
+        errs.append(float(np.median(_err(got, ref))))
+    for k in range(len(reqs)):
+        if k not in outs:
+            srv.take(ids[k])
+    res = {"workload": f"Poisson {rate:g} req/s for {seconds:g} s: 70% 2D disk / 30% 3D Plummer, "
+                       f"N log-uniform [4096, 2097152], steps U[10, 500]",
+           "requests": len(reqs), "completed": int(s.completed), "failed": int(s.failed),
+           "hbm_budget_gb": budget / 2 ** 30,
+           "pool_gb": [s.pool_bytes[0] / 2 ** 30, s.pool_bytes[1] / 2 ** 30],
+           "pool_capacity": [int(s.pool_capacity[0]), int(s.pool_capacity[1])],
+           "particle_steps": int(s.particle_steps), "wall_s": wall,
+           "value": s.particle_steps / wall, "unit": UNIT,
+           "busy_value": s.particle_steps / max(s.busy_s, 1e-9),
+           "step_ms_p50": s.step_ms_p50, "step_ms_p99": s.step_ms_p99,
+           "request_latency_s_p50": s.latency_s_p50, "request_latency_s_p99": s.latency_s_p99,
+           "batched_steps": int(s.iterations), "precision": "mixed",
+           "per_request_median_err_vs_fp64": errs}
+    srv.close()
+    return res
+
+
 def run_ours(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -319,7 +512,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h, "steps": ke,
                 "api": "ge_frame_host (pinned host SoA buffers)"},
-        "gpu_launches": 10 * K,
+        "gpu_launches": LAUNCHES_PER_STEP["fast"] * K,
         "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops,
                      "peak": fp32_peak, "unit": "TFLOP/s", "frac": walk_tflops / fp32_peak,
                      "traffic": traffic,
@@ -343,6 +536,12 @@ def run_ours(args, world, rank, local):
                          "sort_gather": cstage[3], "build": cstage[4], "walk": cstage[5],
                          "integrate_end": cstage[6]}}
     sim.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["mixed"] = bench_mixed(ge, torch, stream, st, n, flush)
+        del flush
+        torch.cuda.empty_cache()
+        line["batched"] = bench_batched(ge, ics, torch, args.batch_sims)
+        line["serving"] = bench_serving(ge, ics, args.serve_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
