@@ -52,7 +52,7 @@ class Params(C.Structure):
         ("eps2", C.c_float), ("dt", C.c_float), ("leaf_cap", C.c_uint32),
         ("size_gate", C.c_float), ("min_size", C.c_float), ("node_cap_factor", C.c_float),
         ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("group_size", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -81,7 +81,8 @@ class ServerStats(C.Structure):
         ("particle_steps", C.c_int64), ("busy_s", C.c_double), ("step_ms_p50", C.c_double),
         ("step_ms_p99", C.c_double), ("latency_s_p50", C.c_double),
         ("latency_s_p99", C.c_double), ("pool_bytes", C.c_int64 * 2),
-        ("pool_capacity", C.c_int64 * 2),
+        ("pool_capacity", C.c_int64 * 2), ("pool_iterations", C.c_int64 * 2),
+        ("pool_step_ms_p50", C.c_double * 2), ("pool_step_ms_p99", C.c_double * 2),
     ]
 
 

@@ -48,7 +48,9 @@ struct Buffers {
     unsigned long long *d_inter = nullptr;
     bool prev = false;     // prevVel arrays allocated
     bool pinned = false;   // pin flag arrays allocated
-    bool mixed = false;    // GE_PREC_MIXED arrays allocated
+    bool mixed = false;    // GE_PREC_MIXED Kahan terms and node moments allocated
+    bool mixed_entry = false;   // ... the per-particle walk's entry arrays
+    bool mixed_group = false;   // ... the group walk's slot arrays and work stacks
     AllocList allocs;
 };
 
@@ -174,6 +176,7 @@ StepParams step_params(const ge_ctx *c) {
     s.size_gate = c->p.size_gate;
     s.min_size = c->p.min_size;
     s.periodic = c->p.periodic ? 1 : 0;
+    s.group_size = c->p.group_size;
     for (int a = 0; a < 3; a++) {
         s.domain[a] = c->p.domain[a];
         s.half_domain[a] = c->p.domain[a] * 0.5f;
@@ -191,6 +194,8 @@ int validate(ge_ctx *c, const ge_params *p) {
     if (!(p->eps2 >= 0.0f)) return fail(c, GE_ERR_ARG, "eps2 must be >= 0");
     if (p->leaf_cap < 1) return fail(c, GE_ERR_ARG, "leaf_cap must be >= 1");
     if (!(p->node_cap_factor >= 1.0f)) return fail(c, GE_ERR_ARG, "node_cap_factor must be >= 1");
+    if (p->group_size != 0 && p->group_size != 32 && p->group_size != 64 && p->group_size != 128)
+        return fail(c, GE_ERR_ARG, "group_size must be 0, 32, 64 or 128");
     if (p->periodic && (!(p->domain[0] > 0) || !(p->domain[1] > 0) ||
                         (p->dims == 3 && !(p->domain[2] > 0))))
         return fail(c, GE_ERR_ARG, "periodic wrap needs a positive domain");
@@ -259,28 +264,63 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     return GE_OK;
 }
 
-// GE_PREC_MIXED arrays: Kahan terms of both state buffers (zeroed) and the
-// node moments.
+// Whether the mixed mode walks in groups (a group size is set and the
+// domain is not periodic) or particle by particle.
+bool wants_group(const ge_params &p) { return p.group_size != 0 && !p.periodic; }
+
+// GE_PREC_MIXED arrays: Kahan terms of both state buffers (zeroed), the node
+// moments, and the node data of the walk the group size selects.
 int alloc_mixed(ge_ctx *c, Buffers &nb) {
     const int D = c->p.dims;
     const size_t N = (size_t)nb.cap_n, E = N + (size_t)nb.tree.cap + 1;
+    const size_t NC = (size_t)nb.tree.cap;
     auto &L = nb.allocs;
-    for (int k = 0; k < 2; k++) {
-        State &s = nb.st[k];
-        float **kp[6] = {&s.kx, &s.ky, &s.kz, &s.kvx, &s.kvy, &s.kvz};
-        for (int a = 0; a < 6; a++) {
-            if (D == 2 && (a == 2 || a == 5)) continue;
-            GE_CHECK(c, dalloc(L, kp[a], N));
-            if (!L.dry) GE_CHECK(c, cudaMemsetAsync(*kp[a], 0, sizeof(float) * N, c->stream));
-        }
-    }
     Tree &t = nb.tree;
-    GE_CHECK(c, dalloc(L, &t.mom, (size_t)t.cap * (D == 2 ? MomWords<2>::value : MomWords<3>::value)));
-    GE_CHECK(c, dalloc(L, &t.mq0, E));
-    if (D == 3) GE_CHECK(c, dalloc(L, &t.mq1, E));
-    GE_CHECK(c, dalloc(L, &t.mq2, E));
-    nb.mixed = true;
+    if (!nb.mixed) {
+        for (int k = 0; k < 2; k++) {
+            State &s = nb.st[k];
+            float **kp[6] = {&s.kx, &s.ky, &s.kz, &s.kvx, &s.kvy, &s.kvz};
+            for (int a = 0; a < 6; a++) {
+                if (D == 2 && (a == 2 || a == 5)) continue;
+                GE_CHECK(c, dalloc(L, kp[a], N));
+                if (!L.dry) GE_CHECK(c, cudaMemsetAsync(*kp[a], 0, sizeof(float) * N, c->stream));
+            }
+        }
+        GE_CHECK(c, dalloc(L, &t.mom, NC * (D == 2 ? MomWords<2>::value : MomWords<3>::value)));
+        nb.mixed = true;
+    }
+    if (!wants_group(c->p) && !nb.mixed_entry) {
+        GE_CHECK(c, dalloc(L, &t.mq0, E));
+        if (D == 3) GE_CHECK(c, dalloc(L, &t.mq1, E));
+        GE_CHECK(c, dalloc(L, &t.mq2, E));
+        nb.mixed_entry = true;
+    }
+    if (wants_group(c->p) && !nb.mixed_group) {
+        GE_CHECK(c, dalloc(L, &t.gw, NC));
+        GE_CHECK(c, dalloc(L, &t.gq0, NC));
+        if (D == 3) GE_CHECK(c, dalloc(L, &t.gq1, NC));
+        GE_CHECK(c, dalloc(L, &t.gq2, NC));
+        const int warps = group_walk_warps(D, c->num_sms);
+        if (warps < 1) return fail(c, GE_ERR_CUDA, "group walk kernel cannot be made resident");
+        GE_CHECK(c, dalloc(L, &t.wl, (size_t)warps * group_walk_stack_entries()));
+        GE_CHECK(c, dalloc(L, &t.grp, N + 1));
+        t.wl_warps = (uint32_t)warps;
+        nb.mixed_group = true;
+    }
     return GE_OK;
+}
+
+// The tree as a mixed-mode pass sees it: only the node arrays of the walk
+// that runs.
+Tree mixed_view(const ge_ctx *c) {
+    Tree t = c->b.tree;
+    if (!wants_group(c->p)) t.gw = t.gq0 = t.gq1 = nullptr, t.gq2 = nullptr;
+    else t.mq0 = t.mq1 = nullptr, t.mq2 = nullptr;
+    return t;
+}
+
+bool group_walk_on(const ge_ctx *c) {
+    return c->p.precision == GE_PREC_MIXED && wants_group(c->p);
 }
 
 // Copies particles [soff, soff + cnt) of src to [doff, doff + cnt) of dst
@@ -343,6 +383,18 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep, bool exact = fal
     Buffers nb;
     int rc = alloc_buffers(c, nb, cap, node_cap, want_prev, ob.pinned);
     if (!rc && (ob.mixed || c->p.precision == GE_PREC_MIXED)) rc = alloc_mixed(c, nb);
+    if (!rc && ((ob.mixed_entry && !nb.mixed_entry) || (ob.mixed_group && !nb.mixed_group))) {
+        // keep every array set the old buffers had
+        const ge_params keep = c->p;
+        c->p.periodic = 0;
+        c->p.group_size = ob.mixed_entry && !nb.mixed_entry ? 0 : 32;
+        rc = alloc_mixed(c, nb);
+        if (!rc && ob.mixed_group && !nb.mixed_group) {
+            c->p.group_size = 32;
+            rc = alloc_mixed(c, nb);
+        }
+        c->p = keep;
+    }
     if (rc) {
         cudaStreamSynchronize(c->stream);
         free_all(nb.allocs);
@@ -514,15 +566,20 @@ int enqueue_build(ge_ctx *c) {
     StepParams p = step_params(c);
     GE_CHECK(c, launch_build(c->p.dims, cur_state(c), p, c->g, c->b.tree, c->d_err, c->num_sms,
                              c->stream));
-    if (c->p.precision == GE_PREC_MIXED)
-        GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, c->b.tree, c->d_err, c->num_sms,
+    if (c->p.precision == GE_PREC_MIXED) {
+        Tree t = mixed_view(c);
+        GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, t, c->d_err, c->num_sms,
                                    c->stream));
+    }
     return GE_OK;
 }
 
-// The mixed-precision arrays, when the mode was switched on after the upload.
+// The mixed-precision arrays, when the mode (or its walk) was switched on
+// after the upload.
 int ensure_mode(ge_ctx *c) {
-    if (c->p.precision != GE_PREC_MIXED || c->b.mixed) return GE_OK;
+    if (c->p.precision != GE_PREC_MIXED) return GE_OK;
+    const bool have = c->b.mixed && (wants_group(c->p) ? c->b.mixed_group : c->b.mixed_entry);
+    if (have) return GE_OK;
     int rc = alloc_mixed(c, c->b);
     if (rc) return rc;
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
@@ -536,7 +593,13 @@ int enqueue_walk(ge_ctx *c, bool integrate_end) {
         GE_CHECK(c, cudaMemsetAsync(c->b.d_inter, 0, sizeof(unsigned long long), c->stream));
         cnt = c->b.d_inter;
     }
-    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, cur_state(c), p, c->g, c->b.tree,
+    if (group_walk_on(c)) {
+        GE_CHECK(c, launch_group_walk(c->p.dims, cur_state(c), p, c->g, mixed_view(c),
+                                      integrate_end, cnt, c->b.tree.meta + 10, c->d_err,
+                                      c->stream));
+        return GE_OK;
+    }
+    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, cur_state(c), p, c->g, mixed_view(c),
                             integrate_end, cnt, c->d_err, c->stream));
     return GE_OK;
 }
@@ -669,6 +732,7 @@ void ge_params_default(ge_params *p, int dims) {
     p->domain[0] = p->dims == 2 ? 3840.0f : 1300.0f;   // parameters.h:97-99
     p->domain[1] = p->dims == 2 ? 2160.0f : 1300.0f;
     p->domain[2] = 1300.0f;
+    p->group_size = 32;
 }
 
 int ge_create(const ge_params *p, ge_ctx **out) {

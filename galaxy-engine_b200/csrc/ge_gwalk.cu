@@ -1,0 +1,477 @@
+// ge_gwalk.cu -- the group walk of the mixed-precision mode.
+//
+// No counterpart in the reference: its walk (physics.cpp:91-205,
+// physics3D.cpp:131-253) is one traversal per particle.  Here one warp walks
+// the tree once for a group of at most GS = 32 x PPL particles that share a
+// small cell of the tree (k_make_groups):
+//   * the group's bounding box decides the opening test for all of them: a
+//     node is accepted when b^2 < dmin^2 + eps2, dmin the distance from its
+//     centre of mass to the box and b the node's opening radius (ge_moments.cu),
+//     which is at least as strict as every member's own test;
+//   * up to 32 candidate nodes are tested at once, one per lane, taken from a
+//     per-warp work stack in global memory;
+//   * accepted nodes (centre of mass, mass, second moments) and the
+//     particles of opened leaves are staged in shared memory and, when a list
+//     fills up or the walk ends, every lane evaluates them for its own
+//     particles (monopole + softened quadrupole for nodes, the softened pair
+//     force for particles; the particle itself is skipped);
+//   * each lane sums a list pass in FP32 and adds that sum to its running
+//     total with Kahan compensation.
+// Which nodes a particle interacts with depends only on its group, not on the
+// traversal order, so the interaction set is deterministic; only the FP32
+// summation order within a list pass follows the traversal.
+#include <cfloat>
+
+#include "ge_bh.h"
+#include "ge_device.cuh"
+#include "ge_internal.h"
+
+namespace ge {
+
+constexpr int kGWWarps = 4;
+constexpr int kGWThreads = kGWWarps * 32;
+constexpr int kGWNodes = 64;           // staged accepted nodes per warp
+constexpr int kGWParts = 64;           // staged leaf particles per warp
+constexpr uint32_t kGWStack = 8192;    // work stack entries per warp (global memory)
+constexpr int kMetaGroupCtr = 10;      // tree meta word: next group to walk
+constexpr int kMetaGroupCount = 11;    // tree meta word: groups made
+constexpr int kMetaSlotsW = 9;         // tree meta word: node slots of the last build
+
+template <int D>
+struct GWSmem {
+    float4 nA[kGWNodes];   // 2D {hi.x, hi.y, m, b^2}; 3D {hi.x, hi.y, hi.z, m}
+    float4 nB[kGWNodes];   // {lo..., Ixx...} as gq0
+    float4 nC[D == 3 ? kGWNodes : 1];   // 3D {Iyy, Izz, Ixy, Ixz}
+    float nD[kGWNodes];    // 2D Iyy, 3D Iyz
+    float4 pA[kGWParts];   // {x, y, z, m}
+    uint32_t pI[kGWParts]; // particle slot
+};
+
+__device__ __forceinline__ float rsqrt_fast(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+template <int D, int PPL>
+struct GroupState {
+    float x[PPL][3];
+    float f[PPL][3], fc[PPL][3];   // running sums and their Kahan compensation
+    uint32_t idx[PPL];
+    bool act[PPL];
+    unsigned long long count;
+};
+
+// accepted nodes: monopole + quadrupole of the softened kernel
+template <int D, int PPL>
+__device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupState<D, PPL> &g,
+                                            float eps2, bool count) {
+    float acc[PPL][3];
+#pragma unroll
+    for (int k = 0; k < PPL; k++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) acc[k][a] = 0.0f;
+    for (int j = 0; j < nl; j++) {
+        const float4 A = sm.nA[j], B = sm.nB[j];
+        const float4 C = D == 3 ? sm.nC[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float E = sm.nD[j];
+        const float m = D == 2 ? A.z : A.w;
+        const float ixx = D == 2 ? B.z : B.w;
+        const float ixy = D == 2 ? B.w : C.z;
+        const float iyy = D == 2 ? E : C.x;
+#pragma unroll
+        for (int k = 0; k < PPL; k++) {
+            float d[3];
+            d[0] = (A.x - g.x[k][0]) + B.x;
+            d[1] = (A.y - g.x[k][1]) + B.y;
+            d[2] = D == 3 ? (A.z - g.x[k][2]) + B.z : 0.0f;
+            float rr = d[0] * d[0] + d[1] * d[1] + eps2;
+            if (D == 3) rr += d[2] * d[2];
+            const float inv = rsqrt_fast(rr);
+            const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2, inv7 = inv5 * inv2;
+            float Id[3], tr;
+            if (D == 2) {
+                Id[0] = ixx * d[0] + ixy * d[1];
+                Id[1] = ixy * d[0] + iyy * d[1];
+                Id[2] = 0.0f;
+                tr = ixx + iyy;
+            } else {
+                const float izz = C.y, ixz = C.w, iyz = E;
+                Id[0] = ixx * d[0] + ixy * d[1] + ixz * d[2];
+                Id[1] = ixy * d[0] + iyy * d[1] + iyz * d[2];
+                Id[2] = ixz * d[0] + iyz * d[1] + izz * d[2];
+                tr = ixx + iyy + izz;
+            }
+            float dId = d[0] * Id[0] + d[1] * Id[1];
+            if (D == 3) dId += d[2] * Id[2];
+            const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
+            const float ci = -3.0f * inv5;
+#pragma unroll
+            for (int a = 0; a < D; a++) acc[k][a] += cm * d[a] + ci * Id[a];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PPL; k++) {
+#pragma unroll
+        for (int a = 0; a < D; a++) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
+        if (count && g.act[k]) g.count += (unsigned long long)nl;
+    }
+}
+
+// particles of opened leaves: the softened pair force, the particle itself skipped
+template <int D, int PPL>
+__device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupState<D, PPL> &g,
+                                            float eps2, bool count) {
+    float acc[PPL][3];
+    uint32_t self_hits = 0;
+#pragma unroll
+    for (int k = 0; k < PPL; k++)
+#pragma unroll
+        for (int a = 0; a < 3; a++) acc[k][a] = 0.0f;
+    for (int j = 0; j < pl; j++) {
+        const float4 P = sm.pA[j];
+        const uint32_t pj = sm.pI[j];
+#pragma unroll
+        for (int k = 0; k < PPL; k++) {
+            float d[3];
+            d[0] = P.x - g.x[k][0];
+            d[1] = P.y - g.x[k][1];
+            d[2] = D == 3 ? P.z - g.x[k][2] : 0.0f;
+            float rr = d[0] * d[0] + d[1] * d[1] + eps2;
+            if (D == 3) rr += d[2] * d[2];
+            const float inv = rsqrt_fast(rr);
+            const bool self = pj == g.idx[k];
+            self_hits += (self && g.act[k]) ? 1u : 0u;
+            const float fm = self ? 0.0f : P.w * (inv * inv * inv);
+#pragma unroll
+            for (int a = 0; a < D; a++) acc[k][a] += d[a] * fm;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PPL; k++) {
+#pragma unroll
+        for (int a = 0; a < D; a++) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
+        if (count && g.act[k]) g.count += (unsigned long long)pl;
+    }
+    if (count) g.count -= self_hits;
+}
+
+// Groups: every particle belongs to exactly one node that holds at most GS
+// particles while its parent holds more (or that is its simulation's root);
+// runs of such nodes that are adjacent children of one parent are packed
+// into one group while the run holds at most GS particles.  A group is then
+// a contiguous particle range inside one cell (its parent's), so its
+// bounding box stays compact.  A leaf of more than GS particles (a cell at
+// the minimum size) is cut into GS-particle pieces.  The groups depend only
+// on the tree, so a simulation forms the same groups alone and in a batch.
+__device__ __forceinline__ void emit_group(const Tree &t, uint32_t a, uint32_t b) {
+    const uint32_t k = atomicAdd(&t.meta[kMetaGroupCount], 1u);
+    t.grp[k] = make_uint2(a, b);
+}
+
+__global__ void k_make_groups(Tree t, uint32_t GS) {
+    const uint32_t slots = __ldcg(&t.meta[kMetaSlotsW]);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += stride) {
+        const uint4 inf = __ldcg(&t.info[k]);
+        if (inf.w <= inf.z) continue;   // hole
+        const uint32_t cnt = inf.w - inf.z;
+        if (cnt <= GS) {
+            if (__ldcg(&t.aux[k]).z == kEmpty) emit_group(t, inf.z, inf.w);   // a small root
+            continue;
+        }
+        if (!inf.y) {   // a leaf larger than a group
+            for (uint32_t a = inf.z; a < inf.w; a += GS) emit_group(t, a, min(a + GS, inf.w));
+            continue;
+        }
+        const int nc = __popc(inf.y);
+        uint32_t ra = 0, rb = 0;   // current run of small adjacent children
+        for (int c = 0; c < nc; c++) {
+            const uint4 ci = __ldcg(&t.info[inf.x + (uint32_t)c]);
+            const uint32_t cc = ci.w - ci.z;
+            if (cc > GS) {
+                if (rb > ra) emit_group(t, ra, rb);
+                ra = rb = 0;
+                continue;
+            }
+            if (rb > ra && rb == ci.z && (ci.w - ra) <= GS) {
+                rb = ci.w;
+            } else {
+                if (rb > ra) emit_group(t, ra, rb);
+                ra = ci.z;
+                rb = ci.w;
+            }
+        }
+        if (rb > ra) emit_group(t, ra, rb);
+    }
+}
+
+template <int D, int PPL, bool COUNT>
+__global__ void __launch_bounds__(kGWThreads)
+k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
+             unsigned long long *inter, uint32_t *err) {
+    __shared__ GWSmem<D> smem[kGWWarps];
+    GWSmem<D> &sm = smem[threadIdx.x >> 5];
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t *wl = t.wl + (size_t)gwarp * kGWStack;
+    const uint32_t ngroups = __ldcg(&t.meta[kMetaGroupCount]);
+    const float eps2 = p.eps2;
+    const float *pos[3] = {s.x, s.y, s.z};
+    GroupState<D, PPL> g;
+    g.count = 0;
+    while (true) {
+        uint32_t grp = 0;
+        if (lane == 0) grp = atomicAdd(&t.meta[kMetaGroupCtr], 1u);
+        grp = __shfl_sync(0xffffffffu, grp, 0);
+        if (grp >= ngroups) break;
+        const uint2 range = __ldcg(&t.grp[grp]);
+        const uint32_t base = range.x, seg_end = range.y;
+        const uint32_t sg = sg_tab.seg_of ? sg_tab.seg_of[base] : 0u;
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+        for (int k = 0; k < PPL; k++) {
+            const uint32_t i = base + (uint32_t)k * 32u + lane;
+            g.idx[k] = i;
+            g.act[k] = i < seg_end;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                g.x[k][a] = (g.act[k] && a < D) ? pos[a][i] : 0.0f;
+                g.f[k][a] = 0.0f;
+                g.fc[k][a] = 0.0f;
+            }
+            if (g.act[k]) {
+#pragma unroll
+                for (int a = 0; a < D; a++) {
+                    lo[a] = fminf(lo[a], g.x[k][a]);
+                    hi[a] = fmaxf(hi[a], g.x[k][a]);
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < D; a++)
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+                hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+            }
+        int nl = 0, pl = 0;
+        uint32_t top = 1;
+        if (lane == 0) wl[0] = sg;   // the simulation's root node slot
+        __syncwarp();
+        bool overflow = false;
+        while (top > 0) {
+            const uint32_t take = min(top, 32u);
+            top -= take;
+            const uint32_t c = lane < take ? __ldcg(&wl[top + lane]) : kEmpty;
+            __syncwarp();
+            int kind = 0;   // 1 accepted node, 2 opened leaf, 3 opened internal node
+            float4 A = make_float4(0.f, 0.f, 0.f, 0.f);
+            uint4 inf = make_uint4(0u, 0u, 0u, 0u);
+            if (c != kEmpty) {
+                A = __ldg(&t.gw[c]);
+                inf = __ldg(&t.info[c]);
+                const float m = D == 2 ? A.z : A.w;
+                const float b2 = D == 2 ? A.w : __ldg(&t.gq2[c]).y;
+                if (m > 0.0f) {
+                    const float com[3] = {A.x, A.y, A.z};
+                    float dm = eps2;
+#pragma unroll
+                    for (int a = 0; a < D; a++) {
+                        const float e = fmaxf(fmaxf(lo[a] - com[a], com[a] - hi[a]), 0.0f);
+                        dm = __fmaf_rn(e, e, dm);
+                    }
+                    kind = b2 < dm ? 1 : (inf.y ? 3 : 2);
+                }
+            }
+            // 1. accepted nodes into the node list
+            const unsigned accb = __ballot_sync(0xffffffffu, kind == 1);
+            if (nl + __popc(accb) > kGWNodes) {
+                flush_nodes<D, PPL>(sm, nl, g, eps2, COUNT);
+                nl = 0;
+                __syncwarp();
+            }
+            if (kind == 1) {
+                const int q = nl + __popc(accb & lt);
+                sm.nA[q] = A;
+                sm.nB[q] = __ldg(&t.gq0[c]);
+                if (D == 3) sm.nC[q] = __ldg(&t.gq1[c]);
+                sm.nD[q] = __ldg(&t.gq2[c]).x;
+            }
+            nl += __popc(accb);
+            // 2. children of opened internal nodes onto the work stack
+            const uint32_t nch = kind == 3 ? (uint32_t)__popc(inf.y) : 0u;
+            uint32_t incl = nch;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (unsigned)o) incl += v;
+            }
+            const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+            if (top + tot > kGWStack) {   // warp-uniform
+                overflow = true;
+                break;
+            }
+            for (uint32_t q = 0; q < nch; q++) wl[top + incl - nch + q] = inf.x + q;
+            top += tot;
+            // 3. particles of opened leaves into the particle list
+            uint32_t pc = kind == 2 ? inf.w - inf.z : 0u;
+            uint32_t pbeg = inf.z;
+            unsigned pend = __ballot_sync(0xffffffffu, pc > 0u);
+            while (pend) {
+                uint32_t pin = pc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, pin, o);
+                    if (lane >= (unsigned)o) pin += v;
+                }
+                const uint32_t ptot = __shfl_sync(0xffffffffu, pin, 31);
+                if (pl + ptot <= (uint32_t)kGWParts) {
+                    for (uint32_t j = 0; j < pc; j++) {
+                        const uint32_t q = pl + pin - pc + j, src = pbeg + j;
+                        sm.pA[q] = make_float4(s.x[src], s.y[src], D == 3 ? s.z[src] : 0.0f,
+                                               s.m[src]);
+                        sm.pI[q] = src;
+                    }
+                    pl += (int)ptot;
+                    break;
+                }
+                // does not fit: flush, then move the first pending leaf in
+                // list-sized chunks
+                __syncwarp();
+                flush_parts<D, PPL>(sm, pl, g, eps2, COUNT);
+                __syncwarp();
+                const int L = __ffs(pend) - 1;
+                const uint32_t lb = __shfl_sync(0xffffffffu, pbeg, L);
+                const uint32_t lc = __shfl_sync(0xffffffffu, pc, L);
+                const uint32_t chunk = min(lc, (uint32_t)kGWParts);
+                for (uint32_t j = lane; j < chunk; j += 32) {
+                    sm.pA[j] = make_float4(s.x[lb + j], s.y[lb + j], D == 3 ? s.z[lb + j] : 0.0f,
+                                           s.m[lb + j]);
+                    sm.pI[j] = lb + j;
+                }
+                pl = (int)chunk;
+                if ((int)lane == L) {
+                    pbeg += chunk;
+                    pc -= chunk;
+                }
+                __syncwarp();
+                pend = __ballot_sync(0xffffffffu, pc > 0u);
+            }
+            __syncwarp();
+        }
+        if (overflow) {
+            if (lane == 0) set_err(err, kErrStack);
+            nl = 0;
+            pl = 0;
+        }
+        __syncwarp();
+        if (nl) flush_nodes<D, PPL>(sm, nl, g, eps2, COUNT);
+        if (pl) flush_parts<D, PPL>(sm, pl, g, eps2, COUNT);
+        __syncwarp();
+        // results and the fused second half kick
+#pragma unroll
+        for (int k = 0; k < PPL; k++) {
+            if (!g.act[k]) continue;
+            const uint32_t i = g.idx[k];
+            float a3[3];
+#pragma unroll
+            for (int a = 0; a < D; a++) a3[a] = p.G * (g.f[k][a] - g.fc[k][a]);
+            s.ax[i] = a3[0];
+            s.ay[i] = a3[1];
+            if (D == 3) s.az[i] = a3[2];
+            if (integrate_end && !(s.pinned && s.pinned[i])) {
+                float *vel[3] = {s.vx, s.vy, s.vz};
+                if (s.kvx) {
+                    float *kv[3] = {s.kvx, s.kvy, s.kvz};
+#pragma unroll
+                    for (int a = 0; a < D; a++) kahan_add(vel[a][i], kv[a][i], fmul(a3[a], p.half_dt));
+                } else {
+#pragma unroll
+                    for (int a = 0; a < D; a++) vel[a][i] = fadd(vel[a][i], fmul(a3[a], p.half_dt));
+                }
+            }
+        }
+    }
+    if (COUNT) {
+        unsigned long long v = g.count;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(inter, v);
+    }
+}
+
+static int grid_blocks(int n) {
+    int b = (n + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    return b < 1 ? 1 : b;
+}
+
+template <int D, int PPL, bool COUNT>
+static int resident_blocks() {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_group_walk<D, PPL, COUNT>,
+                                                      kGWThreads, 0) != cudaSuccess)
+        return 0;
+    return per_sm;
+}
+
+template <int D>
+static int most_resident() {
+    int m = resident_blocks<D, 1, false>();
+    m = max(m, resident_blocks<D, 2, false>());
+    m = max(m, resident_blocks<D, 4, false>());
+    m = max(m, resident_blocks<D, 1, true>());
+    m = max(m, resident_blocks<D, 2, true>());
+    m = max(m, resident_blocks<D, 4, true>());
+    return m;
+}
+
+// Warps the group walk keeps resident (its work stacks are sized for them).
+int group_walk_warps(int dims, int num_sms) {
+    const int per_sm = dims == 2 ? most_resident<2>() : most_resident<3>();
+    return per_sm * num_sms * kGWWarps;
+}
+
+uint32_t group_walk_stack_entries() { return kGWStack; }
+
+template <int D, int PPL, bool COUNT>
+static cudaError_t gw_launch(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    k_make_groups<<<grid_blocks(p.n), 256, 0, st>>>(t, 32u * PPL);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // one work stack per warp bounds the grid; groups number at most n
+    int blocks = (int)(t.wl_warps / kGWWarps);
+    const int64_t want = ((int64_t)p.n + kGWWarps - 1) / kGWWarps;
+    if (blocks > want) blocks = (int)want;
+    if (blocks < 1) blocks = 1;
+    k_group_walk<D, PPL, COUNT><<<blocks, kGWThreads, 0, st>>>(s, p, g, t, ie, inter, err);
+    return cudaGetLastError();
+}
+
+template <int D>
+static cudaError_t gw_dims(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                           int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if (inter) {
+        if (p.group_size >= 128) return gw_launch<D, 4, true>(s, p, g, t, ie, inter, err, st);
+        if (p.group_size >= 64) return gw_launch<D, 2, true>(s, p, g, t, ie, inter, err, st);
+        return gw_launch<D, 1, true>(s, p, g, t, ie, inter, err, st);
+    }
+    if (p.group_size >= 128) return gw_launch<D, 4, false>(s, p, g, t, ie, inter, err, st);
+    if (p.group_size >= 64) return gw_launch<D, 2, false>(s, p, g, t, ie, inter, err, st);
+    return gw_launch<D, 1, false>(s, p, g, t, ie, inter, err, st);
+}
+
+cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, const Segs &g,
+                              const Tree &t, bool integrate_end, unsigned long long *inter_count,
+                              uint32_t *counter, uint32_t *err, cudaStream_t st) {
+    if (!t.wl || !t.grp || t.wl_warps < (uint32_t)kGWWarps) return cudaErrorInvalidValue;
+    // counter[0]: next group to walk, counter[1]: groups made
+    cudaError_t e = cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const int ie = integrate_end ? 1 : 0;
+    return dims == 2 ? gw_dims<2>(s, p, g, t, ie, inter_count, err, st)
+                     : gw_dims<3>(s, p, g, t, ie, inter_count, err, st);
+}
+
+}  // namespace ge

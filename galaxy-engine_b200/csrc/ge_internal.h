@@ -78,6 +78,16 @@ struct Tree {
     double *mom;
     float4 *mq0, *mq1;
     float *mq2;
+    // the same per node slot, for the group walk (nullptr when unused):
+    //   gw    float4  2D {com_hi.x, com_hi.y, mass, b^2}  3D {com_hi.x, com_hi.y, com_hi.z, mass}
+    //   gq0   float4  as mq0;  gq1 float4 3D as mq1
+    //   gq2   float2  2D {Iyy, 0}   3D {Iyz, b^2}
+    // (mass 0 marks a massless node)
+    float4 *gw, *gq0, *gq1;
+    float2 *gq2;
+    uint32_t *wl;         // group walk: a work stack per resident warp
+    uint32_t wl_warps;    // warps the work stacks are sized for
+    uint2 *grp;           // group walk: particle range of each group [n + 1]
     int64_t cap;
 };
 
@@ -127,6 +137,7 @@ struct StepParams {
     float size_gate, min_size;
     int periodic;
     float domain[3], half_domain[3];
+    int group_size;   // GE_PREC_MIXED: 0 = per-particle walk, else the group walk
 };
 
 constexpr int kBBoxThreads = 256;
@@ -168,6 +179,13 @@ int build_grid_blocks(int dims, int num_sms);
 int64_t build_node_slack(int dims, int num_sms);
 cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Segs &g, Tree &t,
                          uint32_t *err, int num_sms, cudaStream_t st);
+// GE_PREC_MIXED group walk (ge_gwalk.cu): warps walk for groups of
+// p.group_size consecutive particles of one simulation; counter = one word
+int group_walk_warps(int dims, int num_sms);
+uint32_t group_walk_stack_entries();
+cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, const Segs &g,
+                              const Tree &t, bool integrate_end, unsigned long long *inter_count,
+                              uint32_t *counter, uint32_t *err, cudaStream_t st);
 // tree walk; integrate_end fuses integrateEnd (v += a*dt/2)
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
                         const Segs &g, const Tree &t, bool integrate_end,

@@ -45,8 +45,12 @@ __global__ void k_pend_init(Tree t) {
 template <int D>
 __device__ void write_entry(const Tree &t, uint32_t k, const double *r, double inv_theta) {
     const double M = r[0];
-    if (!(M > 0.0)) return;   // massless: laid out as an accepted entry without mass
-    const uint32_t e = __ldcg(&t.aux[k]).w;
+    if (!(M > 0.0)) {
+        // massless: the walk layout already holds an accepted entry without
+        // mass; the group walk skips a node of mass 0
+        if (t.gw) t.gw[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     const float4 cell = __ldcg(&t.cell[k]);
     const double half = 0.5 * (double)cell.w;
     const double cc[3] = {(double)cell.x + half, (double)cell.y + half, (double)cell.z + half};
@@ -62,6 +66,20 @@ __device__ void write_entry(const Tree &t, uint32_t k, const double *r, double i
     }
     const double b = __fma_rn((double)cell.w, inv_theta, sqrt(del2));
     const float b2 = (float)__dmul_rn(b, b);
+    if (t.gw) {   // per node slot, for the group walk
+        if (D == 2) {
+            t.gw[k] = make_float4(hi[0], hi[1], (float)M, b2);
+            t.gq0[k] = make_float4(lo[0], lo[1], (float)r[3], (float)r[4]);
+            t.gq2[k] = make_float2((float)r[5], 0.0f);
+        } else {
+            t.gw[k] = make_float4(hi[0], hi[1], hi[2], (float)M);
+            t.gq0[k] = make_float4(lo[0], lo[1], lo[2], (float)r[4]);
+            t.gq1[k] = make_float4((float)r[5], (float)r[6], (float)r[7], (float)r[8]);
+            t.gq2[k] = make_float2((float)r[9], b2);
+        }
+    }
+    if (!t.mq0) return;
+    const uint32_t e = __ldcg(&t.aux[k]).w;
     if (D == 2) {
         t.src[e] = make_float4(hi[0], hi[1], (float)M, b2);
         t.mq0[e] = make_float4(lo[0], lo[1], (float)r[3], (float)r[4]);

@@ -6,15 +6,17 @@
 // once at creation from its share of the HBM budget (ge_estimate_bytes /
 // ge_reserve), so admission never allocates and the pools never exceed the
 // budget.  Requests (a simulation and a step count) are queued by
-// ge_server_submit from any host thread.  The loop -- on a worker thread
-// (ge_server_start) or driven by ge_server_poll -- repeats:
+// ge_server_submit from any host thread.  Each pool's loop -- on its own
+// worker thread (ge_server_start), or both pools per ge_server_poll --
+// repeats:
 //   1. admit: queued requests join their pool, first come first served, as
 //      long as the pool's particle and simulation capacity allow (a request
 //      that does not fit waits for running ones to finish; later requests of
 //      the same pool wait behind it);
-//   2. step: every pool with running simulations takes one step of all of
-//      them (ge_step_async on each pool's stream, then ge_step_wait on each),
-//      so the 2D and 3D pools' kernels overlap on the device;
+//   2. step: one step of all of the pool's running simulations
+//      (ge_step_async on the pool's stream, then ge_step_wait); the pools step
+//      independently, each at its own rate, and their kernels overlap on the
+//      device;
 //   3. retire: simulations that reached their step count are copied to host
 //      memory and removed from their pool in one compaction.
 // A simulation's result does not depend on what else runs in its pool
@@ -65,6 +67,13 @@ struct Pool {
     int32_t max_sims = 0;
     std::deque<int64_t> queue;  // waiting requests, first come first served
     std::vector<int64_t> running;
+    // the pool's loop
+    std::thread worker;
+    bool stepping = false;
+    Clock::time_point t_step;
+    int64_t iterations = 0;
+    double busy_s = 0.0;
+    std::vector<double> step_ms;
 };
 
 double percentile(std::vector<double> v, double q) {
@@ -86,14 +95,12 @@ struct ge_server {
     std::condition_variable cv;       // submissions and completions
     std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
     int64_t next_id = 1;
-    std::thread worker;
     bool running_thread = false;
     bool stop = false;
     Clock::time_point t0 = Clock::now();
     // statistics
-    int64_t submitted = 0, completed = 0, failed = 0, iterations = 0, particle_steps = 0;
-    double busy_s = 0.0;
-    std::vector<double> step_ms, latency_s;
+    int64_t submitted = 0, completed = 0, failed = 0, particle_steps = 0;
+    std::vector<double> latency_s;
     std::string err;
     int loop_error = GE_OK;
 };
@@ -127,150 +134,155 @@ int size_pool(const ge_params *p, int64_t share, int32_t max_sims, int64_t *cap)
     return GE_OK;
 }
 
-// 1. admit queued requests that fit (caller holds no lock)
-int admit(ge_server *s) {
-    for (int k = 0; k < 2; k++) {
-        Pool &P = s->pool[k];
-        if (!P.ctx) continue;
-        while (true) {
-            Request *r = nullptr;
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                if (P.queue.empty()) break;
-                Request *h = s->reqs[P.queue.front()].get();
-                if (P.used_n + h->n > P.cap_n || (int32_t)P.running.size() >= P.max_sims) break;
-                P.queue.pop_front();
-                r = h;
-            }
-            const int64_t n = r->n;
-            const float *b = r->in.data();
-            const bool d3 = P.dims == 3;
-            const float *x = b, *y = b + n, *z = d3 ? b + 2 * n : nullptr;
-            const float *vx = b + (d3 ? 3 : 2) * n, *vy = vx + n, *vz = d3 ? vy + n : nullptr;
-            const float *m = b + (d3 ? 6 : 4) * n;
-            int32_t h = 0;
-            const int rc = ge_batch_add_sim(P.ctx, n, x, y, z, vx, vy, vz, m, nullptr, &h);
+// 1. admit queued requests of pool k that fit (caller holds no lock)
+int admit(ge_server *s, int k) {
+    Pool &P = s->pool[k];
+    if (!P.ctx) return GE_OK;
+    while (true) {
+        Request *r = nullptr;
+        {
             std::lock_guard<std::mutex> lk(s->mu);
-            if (rc) {
-                r->state = GE_REQ_FAILED;
-                s->failed++;
-                s->err = ge_last_error(P.ctx);
-                s->cv.notify_all();
-                continue;
-            }
-            r->sim = h;
-            r->state = GE_REQ_RUNNING;
-            r->t_admit = seconds_since(s->t0);
-            r->in.clear();
-            r->in.shrink_to_fit();
-            P.used_n += n;
-            P.running.push_back(r->id);
+            if (P.queue.empty()) break;
+            Request *h = s->reqs[P.queue.front()].get();
+            if (P.used_n + h->n > P.cap_n || (int32_t)P.running.size() >= P.max_sims) break;
+            P.queue.pop_front();
+            r = h;
         }
+        const int64_t n = r->n;
+        const float *b = r->in.data();
+        const bool d3 = P.dims == 3;
+        const float *x = b, *y = b + n, *z = d3 ? b + 2 * n : nullptr;
+        const float *vx = b + (d3 ? 3 : 2) * n, *vy = vx + n, *vz = d3 ? vy + n : nullptr;
+        const float *m = b + (d3 ? 6 : 4) * n;
+        int32_t h = 0;
+        const int rc = ge_batch_add_sim(P.ctx, n, x, y, z, vx, vy, vz, m, nullptr, &h);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (rc) {
+            r->state = GE_REQ_FAILED;
+            s->failed++;
+            s->err = ge_last_error(P.ctx);
+            s->cv.notify_all();
+            continue;
+        }
+        r->sim = h;
+        r->state = GE_REQ_RUNNING;
+        r->t_admit = seconds_since(s->t0);
+        r->in.clear();
+        r->in.shrink_to_fit();
+        P.used_n += n;
+        P.running.push_back(r->id);
     }
     return GE_OK;
 }
 
-// 2 + 3. one step of every running simulation, then retire the finished ones
-int step_and_retire(ge_server *s, int32_t *stepped) {
-    *stepped = 0;
-    const auto t0 = Clock::now();
-    bool any = false;
-    for (Pool &P : s->pool)
-        if (P.ctx && !P.running.empty()) {
-            const int rc = ge_step_async(P.ctx, 1);
-            if (rc) return sfail(s, rc, ge_last_error(P.ctx));
-            any = true;
-        }
-    if (!any) return GE_OK;
-    int64_t ps = 0;
-    for (Pool &P : s->pool)
-        if (P.ctx && !P.running.empty()) {
-            const int rc = ge_step_wait(P.ctx);
-            if (rc) return sfail(s, rc, ge_last_error(P.ctx));
-            ps += P.used_n;
-        }
-    const double dt = seconds_since(t0);
+// 2. one step of every running simulation of pool k, in two halves so that
+// several pools can be in flight on their own streams
+int start_step(ge_server *s, int k) {
+    Pool &P = s->pool[k];
+    if (!P.ctx || P.running.empty()) return GE_OK;
+    P.t_step = Clock::now();
+    P.stepping = true;
+    const int rc = ge_step_async(P.ctx, 1);
+    if (rc) {
+        P.stepping = false;
+        return sfail(s, rc, ge_last_error(P.ctx));
+    }
+    return GE_OK;
+}
+
+// finish the step of pool k, then 3. retire its finished simulations
+int finish_step(ge_server *s, int k, int32_t *stepped) {
+    Pool &P = s->pool[k];
+    if (!P.stepping) return GE_OK;
+    P.stepping = false;
+    int rc = ge_step_wait(P.ctx);
+    if (rc) return sfail(s, rc, ge_last_error(P.ctx));
+    const double dt = seconds_since(P.t_step);
+    const int64_t ps = P.used_n;
     *stepped = 1;
-    for (Pool &P : s->pool) {
-        if (!P.ctx || P.running.empty()) continue;
-        std::vector<int32_t> gone;
-        std::vector<int64_t> keep, done;
-        std::vector<Request *> fin;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            for (int64_t id : P.running) {
-                Request *r = s->reqs[id].get();
-                r->steps_done++;
-                if (r->steps_done < r->steps) keep.push_back(id);
-                else { fin.push_back(r); done.push_back(id); }
-            }
-        }
-        for (Request *r : fin) {   // running requests are only touched by this loop
-            const int64_t n = r->n;
-            const int q = P.dims;
-            r->out.resize((size_t)n * (3 * q + 1));
-            r->out_id.resize((size_t)n);
-            float *o = r->out.data();
-            float *x = o, *y = o + n, *z = q == 3 ? o + 2 * n : nullptr;
-            float *vx = o + q * n, *vy = vx + n, *vz = q == 3 ? vy + n : nullptr;
-            float *ax = o + 2 * q * n, *ay = ax + n, *az = q == 3 ? ay + n : nullptr;
-            float *m = o + 3 * q * n;
-            const int rc = ge_batch_download_sim(P.ctx, r->sim, x, y, z, vx, vy, vz, ax, ay, az, m,
-                                                 r->out_id.data());
-            if (rc) return sfail(s, rc, ge_last_error(P.ctx));
-            gone.push_back(r->sim);
-        }
-        if (!gone.empty()) {
-            const int rc = ge_batch_remove_sims(P.ctx, (int32_t)gone.size(), gone.data());
-            if (rc) return sfail(s, rc, ge_last_error(P.ctx));
-        }
+    std::vector<int32_t> gone;
+    std::vector<int64_t> keep, done;
+    std::vector<Request *> fin;
+    {
         std::lock_guard<std::mutex> lk(s->mu);
-        for (int64_t id : done) {
+        for (int64_t id : P.running) {
             Request *r = s->reqs[id].get();
-            r->state = GE_REQ_DONE;
-            r->t_done = seconds_since(s->t0);
-            P.used_n -= r->n;
-            s->completed++;
-            s->latency_s.push_back(r->t_done - r->t_submit);
+            r->steps_done++;
+            if (r->steps_done < r->steps) keep.push_back(id);
+            else { fin.push_back(r); done.push_back(id); }
         }
-        P.running.swap(keep);
+    }
+    for (Request *r : fin) {   // running requests are only touched by their pool's loop
+        const int64_t n = r->n;
+        const int q = P.dims;
+        r->out.resize((size_t)n * (3 * q + 1));
+        r->out_id.resize((size_t)n);
+        float *o = r->out.data();
+        float *x = o, *y = o + n, *z = q == 3 ? o + 2 * n : nullptr;
+        float *vx = o + q * n, *vy = vx + n, *vz = q == 3 ? vy + n : nullptr;
+        float *ax = o + 2 * q * n, *ay = ax + n, *az = q == 3 ? ay + n : nullptr;
+        float *m = o + 3 * q * n;
+        rc = ge_batch_download_sim(P.ctx, r->sim, x, y, z, vx, vy, vz, ax, ay, az, m,
+                                   r->out_id.data());
+        if (rc) return sfail(s, rc, ge_last_error(P.ctx));
+        gone.push_back(r->sim);
+    }
+    if (!gone.empty()) {
+        rc = ge_batch_remove_sims(P.ctx, (int32_t)gone.size(), gone.data());
+        if (rc) return sfail(s, rc, ge_last_error(P.ctx));
     }
     std::lock_guard<std::mutex> lk(s->mu);
-    s->iterations++;
+    for (int64_t id : done) {
+        Request *r = s->reqs[id].get();
+        r->state = GE_REQ_DONE;
+        r->t_done = seconds_since(s->t0);
+        P.used_n -= r->n;
+        s->completed++;
+        s->latency_s.push_back(r->t_done - r->t_submit);
+    }
+    P.running.swap(keep);
+    P.iterations++;
     s->particle_steps += ps;
-    s->busy_s += dt;
-    if (s->step_ms.size() < (1u << 22)) s->step_ms.push_back(dt * 1e3);
+    P.busy_s += dt;
+    if (P.step_ms.size() < (1u << 22)) P.step_ms.push_back(dt * 1e3);
     s->cv.notify_all();
     return GE_OK;
 }
 
-int iterate(ge_server *s, int32_t *stepped) {
-    int rc = admit(s);
-    if (rc) return rc;
-    return step_and_retire(s, stepped);
+// One loop iteration of each pool on the calling thread: both pools' steps
+// are in flight together.
+int iterate_all(ge_server *s, int32_t *stepped) {
+    int rc;
+    for (int k = 0; k < 2; k++)
+        if ((rc = admit(s, k))) return rc;
+    for (int k = 0; k < 2; k++)
+        if ((rc = start_step(s, k))) return rc;
+    for (int k = 0; k < 2; k++)
+        if ((rc = finish_step(s, k, stepped))) return rc;
+    return GE_OK;
 }
 
-void worker_main(ge_server *s) {
+// The loop of one pool on its own thread.
+void worker_main(ge_server *s, int k) {
     cudaSetDevice(s->dev);
+    Pool &P = s->pool[k];
     while (true) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (s->stop) break;
         }
         int32_t stepped = 0;
-        const int rc = iterate(s, &stepped);
+        int rc = admit(s, k);
+        if (!rc) rc = start_step(s, k);
+        if (!rc) rc = finish_step(s, k, &stepped);
         std::unique_lock<std::mutex> lk(s->mu);
         if (rc) {
             s->loop_error = rc;
             s->cv.notify_all();
             break;
         }
-        if (!stepped) {
-            // nothing running: sleep until a submission (or stop)
-            const bool queued = !s->pool[0].queue.empty() || !s->pool[1].queue.empty();
-            if (!queued && !s->stop)
-                s->cv.wait_for(lk, std::chrono::milliseconds(20));
-        }
+        // nothing running in this pool: sleep until a submission (or stop)
+        if (!stepped && P.queue.empty() && !s->stop) s->cv.wait_for(lk, std::chrono::milliseconds(20));
     }
 }
 
@@ -366,7 +378,8 @@ int ge_server_start(ge_server *s) {
     if (s->running_thread) return GE_OK;
     s->stop = false;
     s->running_thread = true;
-    s->worker = std::thread(worker_main, s);
+    for (int k = 0; k < 2; k++)
+        if (s->pool[k].ctx) s->pool[k].worker = std::thread(worker_main, s, k);
     return GE_OK;
 }
 
@@ -378,7 +391,8 @@ int ge_server_stop(ge_server *s) {
         s->stop = true;
         s->cv.notify_all();
     }
-    s->worker.join();
+    for (Pool &P : s->pool)
+        if (P.worker.joinable()) P.worker.join();
     std::lock_guard<std::mutex> lk(s->mu);
     s->running_thread = false;
     return s->loop_error;
@@ -391,7 +405,7 @@ int ge_server_poll(ge_server *s, int32_t *stepped) {
         if (s->running_thread) return GE_ERR_STATE;
     }
     int32_t st = 0;
-    const int rc = iterate(s, &st);
+    const int rc = iterate_all(s, &st);
     if (stepped) *stepped = st;
     return rc;
 }
@@ -464,11 +478,19 @@ int ge_server_get_stats(ge_server *s, ge_server_stats *out) {
     out->failed = s->failed;
     out->queued = (int64_t)(s->pool[0].queue.size() + s->pool[1].queue.size());
     out->running = (int64_t)(s->pool[0].running.size() + s->pool[1].running.size());
-    out->iterations = s->iterations;
     out->particle_steps = s->particle_steps;
-    out->busy_s = s->busy_s;
-    out->step_ms_p50 = percentile(s->step_ms, 0.50);
-    out->step_ms_p99 = percentile(s->step_ms, 0.99);
+    std::vector<double> all;
+    for (int k = 0; k < 2; k++) {
+        const Pool &P = s->pool[k];
+        out->iterations += P.iterations;
+        out->busy_s += P.busy_s;
+        out->pool_iterations[k] = P.iterations;
+        out->pool_step_ms_p50[k] = percentile(P.step_ms, 0.50);
+        out->pool_step_ms_p99[k] = percentile(P.step_ms, 0.99);
+        all.insert(all.end(), P.step_ms.begin(), P.step_ms.end());
+    }
+    out->step_ms_p50 = percentile(all, 0.50);
+    out->step_ms_p99 = percentile(all, 0.99);
     out->latency_s_p50 = percentile(s->latency_s, 0.50);
     out->latency_s_p99 = percentile(s->latency_s, 0.99);
     for (int k = 0; k < 2; k++) {

@@ -72,7 +72,9 @@ typedef struct {
     int32_t periodic;        /* periodic wrap (isPeriodicBoundaryEnabled && !infiniteDomain) */
     float domain[3];         /* domainSize / domainSize3D */
     int32_t track_prev_vel;  /* keep prevVel as the reference does (integrateStart) */
-    int32_t reserved[7];
+    int32_t group_size;      /* GE_PREC_MIXED walk: particles that share one traversal
+                                (32, 64 or 128; 0 = every particle walks alone) */
+    int32_t reserved[6];
 } ge_params;
 
 typedef struct {
@@ -255,13 +257,14 @@ int ge_estimate_bytes(const ge_params *p, int64_t n, int64_t sims, int64_t *byte
  * budget.  It owns two batch contexts (pools: params[0] for 2D requests,
  * params[1] for 3D), each reserved once at creation from its share of
  * hbm_budget_bytes (frac_2d for 2D, the rest for 3D), so the pools together
- * never hold more than the budget and admission never allocates.  The loop
- * (a worker thread after ge_server_start, or one iteration per
- * ge_server_poll on the calling thread) admits queued requests first come
- * first served while their pool has room (particles and max_sims), takes
- * one step of every admitted simulation in both pools (the pools' kernels
- * overlap on the device), and retires simulations that reached their step
- * count: their final state is copied to host memory and their room freed.
+ * never hold more than the budget and admission never allocates.  Each
+ * pool's loop (its own worker thread after ge_server_start; both pools per
+ * ge_server_poll call on the calling thread) admits queued requests first
+ * come first served while the pool has room (particles and max_sims), takes
+ * one step of all of its admitted simulations (the two pools step at their
+ * own rates and their kernels overlap on the device), and retires
+ * simulations that reached their step count: their final state is copied to
+ * host memory and their room freed.
  * A result equals the same request run alone on a context with the same
  * parameters.  submit / status / wait / take / get_stats may be called from
  * any thread. */
@@ -284,13 +287,15 @@ typedef struct {
 
 typedef struct {
     int64_t submitted, completed, failed, queued, running;
-    int64_t iterations;          /* batched steps taken */
+    int64_t iterations;          /* batched steps taken (both pools) */
     int64_t particle_steps;      /* particles stepped, summed over iterations */
-    double busy_s;               /* wall time spent in batched steps */
+    double busy_s;               /* wall time spent in batched steps (both pools) */
     double step_ms_p50, step_ms_p99;      /* wall time of one batched step */
     double latency_s_p50, latency_s_p99;  /* submit -> done, completed requests */
     int64_t pool_bytes[2];       /* device memory held by each pool */
     int64_t pool_capacity[2];    /* particles each pool runs at once */
+    int64_t pool_iterations[2];
+    double pool_step_ms_p50[2], pool_step_ms_p99[2];
 } ge_server_stats;
 
 int ge_server_create(const ge_server_config *cfg, ge_server **out);

@@ -134,6 +134,11 @@ int or_moments_mixed(const or_tree *t, const float *x, const float *y, const flo
 void or_walk_mixed(int64_t n, const float *x, const float *y, const float *z, const float *m,
                    const or_tree *t, const or_params *p, double *ax, double *ay, double *az,
                    uint32_t *inter, int nthreads);
+/* the same with the group walk: groups of group_size consecutive particles
+ * share one opening test against their bounding box (ge_oracle_mixed.c) */
+void or_walk_group(int64_t n, const float *x, const float *y, const float *z, const float *m,
+                   const or_tree *t, const or_params *p, int group_size, double *ax, double *ay,
+                   double *az, uint32_t *inter, int nthreads);
 
 /* --- leapfrog --------------------------------------------------------- */
 void or_integrate_start(int dims, int64_t n, float *x, float *y, float *z,

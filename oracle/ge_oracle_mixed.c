@@ -196,3 +196,169 @@ void or_walk_mixed(int64_t n, const float *x, const float *y, const float *z, co
     }
     free(mom); free(b2); free(hi);
 }
+
+/* Groups of the group walk: each particle belongs to exactly one node of at
+ * most GS particles whose parent holds more (or that is the root); runs of
+ * such nodes that are adjacent children of one parent are packed into one
+ * group while the run holds at most GS particles; a leaf of more than GS
+ * particles is cut into GS-particle pieces.  ranges receives {start, end}. */
+static void push_range(int64_t *ranges, int64_t *ng, int64_t a, int64_t b) {
+    ranges[2 * *ng] = a;
+    ranges[2 * *ng + 1] = b;
+    (*ng)++;
+}
+
+static void make_groups(const or_tree *t, int64_t k, int64_t GS, int is_root, int64_t *ranges,
+                        int64_t *ng) {
+    const int nq = 1 << t->dims;
+    const int64_t a = t->start[k], b = t->end[k];
+    if (b - a <= GS) {
+        if (is_root && b > a) push_range(ranges, ng, a, b);
+        return;
+    }
+    if (is_leaf(t, k)) {
+        for (int64_t s = a; s < b; s += GS) push_range(ranges, ng, s, s + GS < b ? s + GS : b);
+        return;
+    }
+    int64_t ra = 0, rb = 0;
+    for (int q = 0; q < nq; q++) {
+        const uint32_t c = t->child[k * nq + q];
+        if (c == EMPTY) continue;
+        const int64_t ca = t->start[c], cb = t->end[c];
+        if (cb - ca > GS) {
+            if (rb > ra) push_range(ranges, ng, ra, rb);
+            ra = rb = 0;
+            make_groups(t, c, GS, 0, ranges, ng);
+            continue;
+        }
+        if (rb > ra && rb == ca && cb - ra <= GS) {
+            rb = cb;
+        } else {
+            if (rb > ra) push_range(ranges, ng, ra, rb);
+            ra = ca;
+            rb = cb;
+        }
+    }
+    if (rb > ra) push_range(ranges, ng, ra, rb);
+}
+
+/* Group walk (the mixed mode with group_size > 0): the groups above; a node
+ * is accepted for the whole group when
+ * b^2 < eps2 + sum_a max(lo_a - com_a, com_a - hi_a, 0)^2 (FP32, fused
+ * multiply-adds in axis order, [lo, hi] the group's bounding box); an opened
+ * leaf contributes its particles.  The interaction set is evaluated in FP64
+ * for each member (the particle itself skipped). */
+static void group_visit(const or_tree *t, const double *mom, const float *b2, const float *hi,
+                        int64_t k, const float lo_b[3], const float hi_b[3], float eps2,
+                        int64_t *nodes, int64_t *nn, int64_t *leaves, int64_t *nl) {
+    const int D = t->dims, R = D == 2 ? 6 : 10, nq = 1 << D;
+    if (!(mom[k * R] > 0.0)) return;
+    float dm = eps2;
+    for (int a = 0; a < D; a++) {
+        const float c = hi[k * 3 + a];
+        const float e = fmaxf(fmaxf(lo_b[a] - c, c - hi_b[a]), 0.0f);
+        dm = fmaf(e, e, dm);
+    }
+    if (b2[k] < dm) { nodes[(*nn)++] = k; return; }
+    if (is_leaf(t, k)) { leaves[(*nl)++] = k; return; }
+    for (int q = 0; q < nq; q++) {
+        const uint32_t c = t->child[k * nq + q];
+        if (c != EMPTY) group_visit(t, mom, b2, hi, c, lo_b, hi_b, eps2, nodes, nn, leaves, nl);
+    }
+}
+
+void or_walk_group(int64_t n, const float *x, const float *y, const float *z, const float *m,
+                   const or_tree *t, const or_params *p, int group_size, double *ax, double *ay,
+                   double *az, uint32_t *inter, int nthreads) {
+    const int D = t->dims, R = D == 2 ? 6 : 10;
+    const int64_t cnt = t->count > 0 ? t->count : 1;
+    double *mom = (double *)malloc(sizeof(double) * (size_t)cnt * R);
+    float *b2 = (float *)malloc(sizeof(float) * (size_t)cnt);
+    float *hi = (float *)malloc(sizeof(float) * (size_t)cnt * 3);
+    if (!mom || !b2 || !hi) { free(mom); free(b2); free(hi); return; }
+    or_moments_mixed(t, x, y, z, m, mom);
+    const double inv_theta = 1.0 / (double)p->theta;
+    for (int64_t k = 0; k < t->count; k++) {
+        const double *r = mom + k * R;
+        const double half = 0.5 * (double)t->size[k];
+        double del2 = 0.0;
+        for (int a = 0; a < D; a++) {
+            hi[k * 3 + a] = (float)r[1 + a];
+            const double dc = r[1 + a] - ((double)t->pos[k * D + a] + half);
+            del2 = fma(dc, dc, del2);
+        }
+        const double b = fma((double)t->size[k], inv_theta, sqrt(del2));
+        b2[k] = (float)(b * b);
+    }
+    const float *pos[3] = {x, y, z};
+    const int64_t GS = group_size;
+    int64_t *ranges = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)(n > 0 ? n : 1));
+    int64_t ngroups = 0;
+    if (!ranges) { free(mom); free(b2); free(hi); return; }
+    if (t->count > 0) make_groups(t, 0, GS, 1, ranges, &ngroups);
+    const double G = p->G, eps2d = p->eps2;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+    for (int64_t g = 0; g < ngroups; g++) {
+        const int64_t i0 = ranges[2 * g], i1 = ranges[2 * g + 1];
+        float lo_b[3] = {INFINITY, INFINITY, INFINITY}, hi_b[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = i0; i < i1; i++)
+            for (int a = 0; a < D; a++) {
+                lo_b[a] = fminf(lo_b[a], pos[a][i]);
+                hi_b[a] = fmaxf(hi_b[a], pos[a][i]);
+            }
+        int64_t *nodes = (int64_t *)malloc(sizeof(int64_t) * (size_t)cnt);
+        int64_t *leaves = (int64_t *)malloc(sizeof(int64_t) * (size_t)cnt);
+        int64_t nn = 0, nl = 0;
+        if (nodes && leaves && t->count > 0)
+            group_visit(t, mom, b2, hi, 0, lo_b, hi_b, p->eps2, nodes, &nn, leaves, &nl);
+        for (int64_t i = i0; i < i1; i++) {
+            double f[3] = {0, 0, 0};
+            uint32_t c = 0;
+            for (int64_t u = 0; u < nn; u++) {
+                const double *r = mom + nodes[u] * R;
+                double d[3] = {0, 0, 0}, rr = eps2d;
+                for (int a = 0; a < D; a++) {
+                    d[a] = r[1 + a] - (double)pos[a][i];
+                    rr += d[a] * d[a];
+                }
+                const double inv = 1.0 / sqrt(rr), inv2 = inv * inv, inv3 = inv2 * inv;
+                const double inv5 = inv3 * inv2, inv7 = inv5 * inv2;
+                double I[3][3] = {{0}};
+                for (int a = 0; a < D; a++)
+                    for (int b = a; b < D; b++) I[a][b] = I[b][a] = (double)(float)r[mom_index(D, a, b)];
+                double Id[3] = {0, 0, 0}, dId = 0.0, tr = 0.0;
+                for (int a = 0; a < D; a++) {
+                    for (int b = 0; b < D; b++) Id[a] += I[a][b] * d[b];
+                    dId += d[a] * Id[a];
+                    tr += I[a][a];
+                }
+                const double M = (double)(float)r[0];
+                const double cm = M * inv3 - 1.5 * tr * inv5 + 7.5 * dId * inv7;
+                for (int a = 0; a < D; a++) f[a] += cm * d[a] - 3.0 * Id[a] * inv5;
+                c++;
+            }
+            for (int64_t u = 0; u < nl; u++) {
+                const int64_t k = leaves[u];
+                for (uint32_t j = t->start[k]; j < t->end[k]; j++) {
+                    if ((int64_t)j == i) continue;
+                    double d[3] = {0, 0, 0}, rr = eps2d;
+                    for (int a = 0; a < D; a++) {
+                        d[a] = (double)pos[a][j] - (double)pos[a][i];
+                        rr += d[a] * d[a];
+                    }
+                    const double inv = 1.0 / sqrt(rr), fm = (double)m[j] * inv * inv * inv;
+                    for (int a = 0; a < D; a++) f[a] += fm * d[a];
+                    c++;
+                }
+            }
+            ax[i] = G * f[0];
+            ay[i] = G * f[1];
+            if (D == 3 && az) az[i] = G * f[2];
+            if (inter) inter[i] = c;
+        }
+        free(nodes);
+        free(leaves);
+    }
+    free(ranges);
+    free(mom); free(b2); free(hi);
+}

@@ -95,6 +95,8 @@ def _load(strict=True):
                                   C.c_double, C.c_int64, _i64p, _f64p, _f64p, _vp, C.c_int]
     lib.or_walk_mixed.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
                                   C.POINTER(Params), _f64p, _f64p, _vp, _vp, C.c_int]
+    lib.or_walk_group.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
+                                  C.POINTER(Params), C.c_int, _f64p, _f64p, _vp, _vp, C.c_int]
     lib.or_integrate_start.argtypes = [C.c_int, C.c_int64] + [_vp] * 12 + [_vp, C.POINTER(Params)]
     lib.or_integrate_end.argtypes = [C.c_int, C.c_int64] + [_vp] * 6 + [_vp, C.POINTER(Params)]
     lib.or_frame.argtypes = [C.POINTER(Params), C.c_int64] + [_vp] * 16 + [C.c_int, C.c_int,
@@ -257,6 +259,23 @@ def walk_mixed(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=Fal
     lib().or_walk_mixed(n, x, y, _ptr(zz), m, C.byref(tree_holder.t), C.byref(params),
                         out[0], out[1], _ptr(out[2]) if z is not None else None,
                         _ptr(inter), nthreads)
+    if want_counts:
+        out.append(inter)
+    return out
+
+
+def walk_group(x, y, m, tree_holder, params, group_size=32, z=None, nthreads=8,
+               want_counts=False):
+    """The mixed-precision group walk (groups of group_size consecutive
+    particles share one opening test); accelerations in FP64."""
+    x, y, m = _f32(x), _f32(y), _f32(m)
+    n = len(x)
+    out = [np.zeros(n, np.float64) for _ in range(2 if z is None else 3)]
+    inter = np.zeros(n, np.uint32) if want_counts else None
+    zz = None if z is None else _f32(z)
+    lib().or_walk_group(n, x, y, _ptr(zz), m, C.byref(tree_holder.t), C.byref(params),
+                        int(group_size), out[0], out[1],
+                        _ptr(out[2]) if z is not None else None, _ptr(inter), nthreads)
     if want_counts:
         out.append(inter)
     return out

@@ -3,12 +3,15 @@
 The mode keeps the reference's tree and walk order and changes what a node
 contributes (FP64 moments, double-float centre of mass, offset-corrected
 opening test, softened quadrupole, Kahan sums).  Checks:
-  * the device walk against the oracle's statement of the same algorithm
+  * the device walk -- particle by particle (group_size 0) and in groups of
+    32, 64 or 128 -- against the oracle's statement of the same algorithm
     (oracle/ge_oracle_mixed.c, FP64) on the same tree: the opening decisions
-    are made from the same FP32 values on both sides, so only the FP32
-    evaluation of the accepted terms differs;
-  * the accuracy bound against the FP64 direct sum (median <= 1e-3 at
-    theta 0.6 in 2D and theta 0.5 in 3D);
+    are made from the same FP32 values on both sides (the group walk's
+    interaction counts agree exactly), so only the FP32 evaluation of the
+    accepted terms differs;
+  * the accuracy bound against the FP64 direct sum (median <= 1e-3: 2D at
+    theta 0.6 particle by particle and at theta 0.7 in groups of 32, 3D at
+    theta 0.5);
   * the Kahan-compensated leapfrog: a drift below half an ulp per step still
     moves the particle;
   * a simulation's result alone and inside a batch is the same.
@@ -42,7 +45,7 @@ def _rel(a, b):
 def test_mixed_walk_matches_oracle(ge, ics, O, dims, n, theta, eps2):
     st = ics.disk2d(n, seed=3) if dims == 2 else ics.plummer3d(n, seed=3)
     p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4, dt=1e-3,
-                          precision=MIXED)
+                          precision=MIXED, group_size=0)
     out = _sorted_forces(ge, p, st)
     z = out.get("z")
     bb = O.bbox(out["x"], out["y"], z)
@@ -58,14 +61,54 @@ def test_mixed_walk_matches_oracle(ge, ics, O, dims, n, theta, eps2):
     assert e.max() <= 1e-4
 
 
-@pytest.mark.parametrize("dims,n,theta,eps2", [(2, 1 << 18, 0.6, 0.005 ** 2),
-                                               (3, 1 << 17, 0.5, 0.01)])
-def test_mixed_accuracy_vs_fp64(ge, ics, dims, n, theta, eps2):
+@pytest.mark.parametrize("dims,n,theta,eps2,gs", [(2, 16384, 0.6, 1e-4, 32),
+                                                  (2, 30000, 0.7, 1e-4, 64),
+                                                  (2, 20000, 0.7, 1e-4, 128),
+                                                  (3, 16384, 0.5, 0.01, 32),
+                                                  (3, 12000, 0.7, 0.01, 64)])
+def test_group_walk_matches_oracle(ge, ics, O, dims, n, theta, eps2, gs):
+    """The group walk against the oracle's statement of it: the same groups,
+    the same opening decisions (FP32 on both sides, so the interaction counts
+    agree exactly), the accepted terms evaluated in FP32 on the device and in
+    FP64 by the oracle."""
+    st = ics.disk2d(n, seed=4) if dims == 2 else ics.plummer3d(n, seed=4)
+    p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4, dt=1e-3,
+                          precision=MIXED, group_size=gs)
+    with ge.Simulation(p) as s:
+        s.upload(st)
+        s.compute_morton_keys()
+        s.sort_particles_by_morton_key()
+        s.build_tree()
+        s.count_interactions(True)
+        s.calculate_force_from_grid()
+        inter = s.stats().interactions
+        out = s.download()
+    z = out.get("z")
+    bb = O.bbox(out["x"], out["y"], z)
+    tree = O.build_tree(out["x"], out["y"], out["m"], bb, z=z, leaf_cap=4, holder=True)
+    op = O.make_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4)
+    ref = O.walk_group(out["x"], out["y"], out["m"], tree, op, group_size=gs, z=z,
+                       want_counts=True)
+    got = [out["ax"], out["ay"]] + ([out["az"]] if dims == 3 else [])
+    e = _rel(got, ref[:-1])
+    print(f"group walk vs oracle: median {np.median(e):.2e} p99 {np.percentile(e, 99):.2e} "
+          f"max {e.max():.2e}; interactions {inter} vs {int(ref[-1].sum())}")
+    assert inter == int(ref[-1].sum())
+    assert np.median(e) <= 1e-6
+    assert np.percentile(e, 99) <= 5e-6
+    assert e.max() <= 1e-4
+
+
+@pytest.mark.parametrize("dims,n,theta,eps2,gs", [(2, 1 << 18, 0.6, 0.005 ** 2, 0),
+                                                  (2, 1 << 18, 0.7, 0.005 ** 2, 64),
+                                                  (3, 1 << 17, 0.5, 0.01, 0),
+                                                  (3, 1 << 17, 0.5, 0.01, 32)])
+def test_mixed_accuracy_vs_fp64(ge, ics, dims, n, theta, eps2, gs):
     st = ics.two_disks2d(n, seed=5) if dims == 2 else ics.plummer3d(n, seed=5)
     res = {}
     for prec in (0, MIXED):
         p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, leaf_cap=4, dt=1e-3,
-                              precision=prec)
+                              precision=prec, group_size=gs)
         with ge.Simulation(p) as s:
             s.upload(st)
             s.step(1)
