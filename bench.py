@@ -208,8 +208,9 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-LAUNCHES_PER_STEP = {"fast": 11, "mixed": 13}   # 2D: box 2, keys 1, sort 5, gather 1, build 1,
-                                                # walk 1 (+ moments 2 in the mixed mode)
+# 2D: box 2, keys 1, sort 5, gather 1, build 1, walk 1; the mixed mode adds the
+# moment pass (2) and the grouping of its group walk (1)
+LAUNCHES_PER_STEP = {"fast": 11, "mixed": 14}
 
 
 def _err(got, ref):
@@ -235,14 +236,17 @@ def _timed_steps(torch, stream, sim, K, flush=None):
 
 
 def bench_mixed(ge, torch, stream, st, n, flush, K=10):
-    """The two-disk workload in the mixed-precision mode at theta 0.6 (the
-    opening angle at which its median error is below 1e-3)."""
-    p = ge.default_params(2, G=1.0, theta=0.6, softening=SOFT, dt=DT, leaf_cap=LEAF,
-                          precision=ge.PREC_MIXED)
+    """The two-disk workload in the mixed-precision mode (group walk) at the
+    configuration's theta 0.7, group size and leaf capacity from the
+    autotuner."""
+    p = ge.default_params(2, G=1.0, theta=THETA, softening=SOFT, dt=DT, leaf_cap=LEAF,
+                          precision=ge.PREC_MIXED, group_size=64)
     with ge.Simulation(p) as sim:
         sim.set_stream(stream.cuda_stream)
         sim.upload(st)
-        sim.step(3)
+        sim.step(2)
+        gs, leaf, table = sim.autotune(reps=2)
+        sim.step(2)
         times = _timed_steps(torch, stream, sim, K, flush)
         out = sim.download()
         idx = np.sort(np.random.Generator(np.random.PCG64(1)).choice(
@@ -250,7 +254,9 @@ def bench_mixed(ge, torch, stream, st, n, flush, K=10):
         ref = sim.direct_sum_f64(idx)
         err = _err([out["ax"][idx], out["ay"][idx]], ref)
         stage = np.array(sim.profile_step())
-    return {"workload": f"two-disk 2D, N={n}", "theta": 0.6, "precision": "mixed",
+    return {"workload": f"two-disk 2D, N={n}", "theta": THETA, "precision": "mixed",
+            "group_size": gs, "leaf_cap": leaf,
+            "autotune_ms": {f"g{g}_l{l}": v for (g, l), v in table.items()},
             "value": n / (times.mean() * 1e-3), "unit": UNIT, "ms_per_step": float(times.mean()),
             "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
             "steps": K, "stage_ms": {"kick_drift_bbox": stage[0], "keys": stage[1],
@@ -264,7 +270,8 @@ def bench_batched(ge, ics, torch, count, K=5, Kp=2):
     """512 independent 2D disks, N log-uniform in [1024, 262144] (seed 2), theta
     0.7, softening 0.01: one context stepping all of them (batched) against one
     context per simulation stepped one after another (plain), in the
-    reference-arithmetic mode and in the mixed mode at theta 0.6."""
+    reference-arithmetic mode and in the mixed mode (group walk, autotuned on
+    the batch)."""
     sizes = [int(v) for v in ics.batch_sizes(count=count, seed=2)]
     sts = [ics.disk2d(nn, seed=1000 + k) for k, nn in enumerate(sizes)]
     total = int(sum(sizes))
@@ -273,16 +280,21 @@ def bench_batched(ge, ics, torch, count, K=5, Kp=2):
            "l2": "inputs larger than L2 (all simulations resident, several GB)"}
     stream = torch.cuda.Stream()
     rng = np.random.Generator(np.random.PCG64(1))
-    for mode, theta, prec in (("fast", 0.7, ge.PREC_FAST), ("mixed", 0.6, ge.PREC_MIXED)):
+    for mode, theta, prec in (("fast", 0.7, ge.PREC_FAST), ("mixed", 0.7, ge.PREC_MIXED)):
         p = ge.default_params(2, G=1.0, theta=theta, softening=0.01, dt=DT, leaf_cap=LEAF,
-                              precision=prec)
+                              precision=prec, group_size=64)
         res = {"theta": theta}
         with ge.Simulation(p) as b:
             b.set_stream(stream.cuda_stream)
             b.reserve(total, count)
             for s_ in sts:
                 b.add_sim(s_)
-            b.step(3)
+            b.step(2)
+            if prec == ge.PREC_MIXED:
+                gs, leaf, _ = b.autotune(reps=1)
+                p.group_size, p.leaf_cap = gs, leaf
+                res["group_size"], res["leaf_cap"] = gs, leaf
+            b.step(2)
             times = _timed_steps(torch, stream, b, K)
             res["batched"] = {"value": total / (times.mean() * 1e-3),
                               "ms_per_step": float(times.mean()),
@@ -325,7 +337,8 @@ def bench_batched(ge, ics, torch, count, K=5, Kp=2):
 def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
     """Poisson arrivals (50 requests/s) for `seconds` seconds: 70% 2D disks, 30%
     3D Plummer spheres, N log-uniform in [4096, 2097152], steps uniform in
-    [10, 500]; mixed precision (theta 0.6 in 2D, 0.5 in 3D, softening 0.01);
+    [10, 500]; mixed precision with the group walk (theta 0.7 in 2D, 0.5 in 3D,
+    softening 0.01);
     a 120 GB budget split between the 2D and 3D pools."""
     import threading
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -339,8 +352,10 @@ def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
         reqs.append((float(t), dims, n, steps, 5000 + k))
     sts = [ics.disk2d(n, seed=sd) if d == 2 else ics.plummer3d(n, seed=sd)
            for _, d, n, _, sd in reqs]
-    p2 = ge.default_params(2, G=1.0, theta=0.6, softening=0.01, dt=DT, precision=ge.PREC_MIXED)
-    p3 = ge.default_params(3, G=1.0, theta=0.5, softening=0.01, dt=DT, precision=ge.PREC_MIXED)
+    p2 = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
+                           group_size=64)
+    p3 = ge.default_params(3, G=1.0, theta=0.5, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
+                           group_size=32)
     mem2 = sum(n * 2 for _, d, n, _, _ in reqs if d == 2) or 1
     mem3 = sum(n * 3 for _, d, n, _, _ in reqs if d == 3) or 1
     frac = mem2 / (mem2 + mem3)
@@ -390,6 +405,9 @@ def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
            "value": s.particle_steps / wall, "unit": UNIT,
            "busy_value": s.particle_steps / max(s.busy_s, 1e-9),
            "step_ms_p50": s.step_ms_p50, "step_ms_p99": s.step_ms_p99,
+           "pool_step_ms_p50": [s.pool_step_ms_p50[0], s.pool_step_ms_p50[1]],
+           "pool_step_ms_p99": [s.pool_step_ms_p99[0], s.pool_step_ms_p99[1]],
+           "pool_steps": [int(s.pool_iterations[0]), int(s.pool_iterations[1])],
            "request_latency_s_p50": s.latency_s_p50, "request_latency_s_p99": s.latency_s_p99,
            "batched_steps": int(s.iterations), "precision": "mixed",
            "per_request_median_err_vs_fp64": errs}

@@ -86,6 +86,12 @@ class ServerStats(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    """ge_tune_result (include/ge_bh.h)."""
+    _fields_ = [("group_size", C.c_int32), ("leaf_cap", C.c_int32), ("tried", C.c_int32),
+                ("reserved", C.c_int32), ("ms", C.c_float * 12)]
+
+
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 _vp = C.c_void_p
@@ -131,6 +137,7 @@ SIGNATURES = {
     "ge_batch_download_sim": ([_vp, C.c_int32] + [_vp] * 11, C.c_int),
     "ge_batch_remove_sims": ([_vp, C.c_int32, _vp], C.c_int),
     "ge_step_async": ([_vp, C.c_int32], C.c_int),
+    "ge_autotune": ([_vp, C.c_int32, C.POINTER(TuneResult)], C.c_int),
     "ge_step_wait": ([_vp], C.c_int),
     "ge_reserve": ([_vp, C.c_int64, C.c_int64], C.c_int),
     "ge_memory_bytes": ([_vp, C.POINTER(C.c_int64)], C.c_int),
@@ -303,6 +310,17 @@ class Simulation:
         h = np.ascontiguousarray(sims, np.int32)
         self._check(lib().ge_batch_remove_sims(self._h, len(h), _ptr(h)))
         self.n = int(self.stats().n)
+
+    def autotune(self, reps=2):
+        """Mixed mode: pick group_size and leaf_cap by timing the force pass
+        on the resident state; returns (group_size, leaf_cap, {(g, l): ms})."""
+        r = TuneResult()
+        self._check(lib().ge_autotune(self._h, int(reps), C.byref(r)))
+        self.params.group_size = r.group_size
+        self.params.leaf_cap = r.leaf_cap
+        table = {(g, l): float(r.ms[4 * a + b]) for a, g in enumerate((32, 64, 128))
+                 for b, l in enumerate((1, 4, 8, 16))}
+        return r.group_size, r.leaf_cap, table
 
     def step_async(self, nsteps=1):
         self._check(lib().ge_step_async(self._h, int(nsteps)))

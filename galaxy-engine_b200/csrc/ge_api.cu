@@ -300,8 +300,12 @@ int alloc_mixed(ge_ctx *c, Buffers &nb) {
         GE_CHECK(c, dalloc(L, &t.gq0, NC));
         if (D == 3) GE_CHECK(c, dalloc(L, &t.gq1, NC));
         GE_CHECK(c, dalloc(L, &t.gq2, NC));
-        const int warps = group_walk_warps(D, c->num_sms);
+        // a work stack per resident warp, but no more warps than one per 16
+        // particles of capacity (a group holds up to 128 particles)
+        int warps = group_walk_warps(D, c->num_sms);
         if (warps < 1) return fail(c, GE_ERR_CUDA, "group walk kernel cannot be made resident");
+        const int64_t need = ((nb.cap_n + 15) / 16 + 3) / 4 * 4;
+        if (need < warps) warps = (int)need;
         GE_CHECK(c, dalloc(L, &t.wl, (size_t)warps * group_walk_stack_entries()));
         GE_CHECK(c, dalloc(L, &t.grp, N + 1));
         t.wl_warps = (uint32_t)warps;
@@ -939,6 +943,60 @@ int ge_step(ge_ctx *c, int32_t nsteps) {
 }
 
 int ge_batch_step(ge_ctx *c, int32_t nsteps) { return ge_step(c, nsteps); }
+
+int ge_autotune(ge_ctx *c, int32_t reps, ge_tune_result *out) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!out || reps < 1) return fail(c, GE_ERR_ARG, "bad autotune arguments");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    if (c->p.precision != GE_PREC_MIXED || c->p.periodic)
+        return fail(c, GE_ERR_STATE, "autotuning needs the mixed mode's group walk");
+    std::memset(out, 0, sizeof(*out));
+    const ge_params keep = c->p;
+    static const int32_t kGroups[3] = {32, 64, 128}, kLeaves[4] = {1, 4, 8, 16};
+    // the tree is built over the Morton order of the current positions
+    if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_keys(c)) || (rc = enqueue_sort(c)) ||
+        (rc = enqueue_permute(c, true)))
+        return rc;
+    float best = 3.0e38f;
+    int bi = -1;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 4; b++) {
+            c->p.group_size = kGroups[a];
+            c->p.leaf_cap = (uint32_t)kLeaves[b];
+            float tmin = 3.0e38f;
+            for (int r = 0; r < reps + 1; r++) {   // the first pass is a warm-up
+                GE_CHECK(c, cudaEventRecord(c->ev[0], c->stream));
+                if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c)) ||
+                    (rc = enqueue_walk(c, false))) {
+                    c->p = keep;
+                    return rc;
+                }
+                GE_CHECK(c, cudaEventRecord(c->ev[1], c->stream));
+                if ((rc = check_device(c))) {
+                    c->p = keep;
+                    return rc;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+                if (r > 0) tmin = std::min(tmin, ms);
+            }
+            out->ms[a * 4 + b] = tmin;
+            out->tried++;
+            if (tmin < best) { best = tmin; bi = a * 4 + b; }
+        }
+    c->p = keep;
+    c->p.group_size = kGroups[bi / 4];
+    c->p.leaf_cap = (uint32_t)kLeaves[bi % 4];
+    out->group_size = c->p.group_size;
+    out->leaf_cap = (int32_t)c->p.leaf_cap;
+    // accelerations of the current positions under the chosen configuration
+    if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c)) || (rc = enqueue_walk(c, false)))
+        return rc;
+    rc = check_device(c);
+    c->tree_valid = rc == GE_OK;
+    return rc;
+}
 
 int ge_profile_step(ge_ctx *c) {
     int rc = require_state(c);

@@ -32,7 +32,7 @@ constexpr int kGWWarps = 4;
 constexpr int kGWThreads = kGWWarps * 32;
 constexpr int kGWNodes = 64;           // staged accepted nodes per warp
 constexpr int kGWParts = 64;           // staged leaf particles per warp
-constexpr uint32_t kGWStack = 8192;    // work stack entries per warp (global memory)
+constexpr uint32_t kGWStack = 2048;    // work stack entries per warp (global memory)
 constexpr int kMetaGroupCtr = 10;      // tree meta word: next group to walk
 constexpr int kMetaGroupCount = 11;    // tree meta word: groups made
 constexpr int kMetaSlotsW = 9;         // tree meta word: node slots of the last build

@@ -132,6 +132,22 @@ int ge_step(ge_ctx *ctx, int32_t nsteps);
    used on the context. */
 int ge_step_async(ge_ctx *ctx, int32_t nsteps);
 int ge_step_wait(ge_ctx *ctx);
+/* Autotuner of the mixed mode's group walk (no counterpart in the
+   reference).  On the resident state, times the force pass -- tree build,
+   node moments and the group walk, best of `reps` after a warm-up -- for
+   every group_size in {32, 64, 128} and leaf_cap in {1, 4, 8, 16}, keeps the
+   fastest in the context's parameters (ge_set_params can override it) and
+   recomputes the accelerations with it.  Positions and velocities are not
+   changed.  ms[4 * g + l] is the time of group size g and leaf capacity l in
+   those orders.  GE_ERR_STATE outside GE_PREC_MIXED: the other modes keep the
+   reference's leaf capacity. */
+typedef struct {
+    int32_t group_size, leaf_cap;   /* chosen */
+    int32_t tried;                  /* configurations measured */
+    int32_t reserved;
+    float ms[12];
+} ge_tune_result;
+int ge_autotune(ge_ctx *ctx, int32_t reps, ge_tune_result *out);
 /* one frame with per-stage CUDA-event timing into ge_stats.stage_ms */
 int ge_profile_step(ge_ctx *ctx);
 /* One frame on HOST buffers: upload, step, download, all inside the call.

@@ -161,3 +161,45 @@ def test_mixed_batch_equals_alone(ge, ics):
                 ref = a.download()
             for key in ("x", "y", "vx", "vy", "ax", "ay", "id"):
                 assert np.array_equal(got[key], ref[key]), key
+
+
+def test_autotune_picks_a_configuration_and_keeps_state(ge, ics):
+    """The autotuner times all 12 (group size, leaf capacity) pairs, keeps the
+    fastest, leaves positions and velocities alone, and leaves the
+    accelerations of the chosen configuration in the state."""
+    st = ics.disk2d(65536, seed=8)
+    p = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=1e-3, precision=MIXED)
+    with ge.Simulation(p) as s:
+        s.upload(st)
+        s.step(2)
+        before = s.download()
+        gs, leaf, table = s.autotune(reps=1)
+        after = s.download()
+        assert gs in (32, 64, 128) and leaf in (1, 4, 8, 16)
+        assert len(table) == 12 and all(v > 0 for v in table.values())
+        assert table[(gs, leaf)] == min(table.values())
+        ob, oa = np.argsort(before["id"]), np.argsort(after["id"])
+        for k in ("x", "y", "vx", "vy", "m"):
+            assert np.array_equal(before[k][ob], after[k][oa]), k
+        s.step(1)   # the chosen configuration steps on
+    q = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=1e-3, precision=MIXED,
+                          group_size=gs, leaf_cap=leaf)
+    with ge.Simulation(q) as r:
+        r.upload({k: after[k] for k in ("x", "y", "vx", "vy", "m", "id")})
+        r.compute_morton_keys()
+        r.sort_particles_by_morton_key()
+        r.build_tree()
+        r.calculate_force_from_grid()
+        ref = r.download()
+    orr = np.argsort(ref["id"])
+    e = _rel([after["ax"][oa], after["ay"][oa]], [ref["ax"][orr], ref["ay"][orr]])
+    assert np.max(e) <= 1e-5
+
+
+def test_autotune_refused_outside_mixed(ge, ics):
+    p = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=1e-3, precision=0)
+    with ge.Simulation(p) as s:
+        s.upload(ics.disk2d(4096, seed=1))
+        with pytest.raises(ge.GeError) as ei:
+            s.autotune()
+        assert ei.value.code == 5
