@@ -43,7 +43,8 @@ constexpr uint32_t kSmallNode = 32;
 
 // meta[] words used by the build
 constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 3,
-              kMetaSmall = 5, kMetaP2Alloc = 6, kMetaReal = 8, kMetaSlots = 9;
+              kMetaSmall = 5, kMetaP2Alloc = 6, kMetaReal = 8, kMetaSlots = 9,
+              kMetaP2Task = 12;
 constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
@@ -513,6 +514,8 @@ struct SubTreeSmem {
     uint32_t lvl[kSubMax + 1];
 };
 
+// The upward mass pass from R (finish_upward) is left to the caller, which
+// runs those of up to 32 subtrees at once, one per lane.
 template <int D>
 __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tree &t,
                                          uint32_t R, uint32_t node_base, SubTreeSmem &sm,
@@ -683,10 +686,7 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
     }
     for (int o = 16; o > 0; o >>= 1) maxlev = max(maxlev, __shfl_xor_sync(0xffffffffu, maxlev, o));
     __syncwarp();
-    if (lane == 0) {
-        atomicMax(&t.meta[kMetaLevels], maxlev + 1u);
-        finish_upward<D>(t, R);
-    }
+    if (lane == 0) atomicMax(&t.meta[kMetaLevels], maxlev + 1u);
     return true;
 }
 
@@ -745,12 +745,33 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
         __shared__ SubTreeSmem s_sub[kBuildThreads / 32];
         SubTreeSmem &sm = s_sub[threadIdx.x >> 5];
         WarpAlloc wa{0u, 0u, 0u};
-        for (uint32_t task = gwarp; task < nsmall; task += nwarps) {
+        // tasks are taken from a counter (their costs differ); lane j holds the
+        // j-th finished subtree root whose upward pass is still to run, and the
+        // warp runs 32 of them at once, so their atomics' round trips overlap
+        uint32_t held = kEmpty, nheld = 0;
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(&t.meta[kMetaP2Task], 1u);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        while (task < nsmall) {
+            uint32_t next = 0;
+            if (lane == 0) next = atomicAdd(&t.meta[kMetaP2Task], 1u);
             const uint32_t R = __ldcg(&t.small[task]);
-            if (!build_small_subtree_smem<D>(s, p, t, R, le, sm, wa, err))
-                build_small_subtree<D>(s, p, t, R, le, wa, err);
+            if (build_small_subtree_smem<D>(s, p, t, R, le, sm, wa, err)) {
+                if (lane == nheld) held = R;
+                if (++nheld == 32u) {
+                    __syncwarp();
+                    finish_upward<D>(t, held);
+                    held = kEmpty;
+                    nheld = 0;
+                }
+            } else {
+                build_small_subtree<D>(s, p, t, R, le, wa, err);   // passes its own leaves upward
+            }
             __syncwarp();
+            task = __shfl_sync(0xffffffffu, next, 0);
         }
+        __syncwarp();
+        if (held != kEmpty) finish_upward<D>(t, held);
         mark_holes(t, wa.next, wa.end);
         if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
     }
@@ -909,6 +930,8 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Se
     if (e != cudaSuccess) return e;
     // small-queue length, phase-2 slots, timeline count, real phase-2 nodes, slots
     e = cudaMemsetAsync(t.meta + kMetaSmall, 0, 5 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(t.meta + kMetaP2Task, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const int blocks = build_grid_blocks(dims, num_sms);
     if (blocks < 1) return cudaErrorLaunchOutOfResources;
