@@ -69,7 +69,6 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
     const LT *__restrict__ link = (const LT *)t.link;
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
-    const uint32_t limit = (uint32_t)n + __ldg(&t.meta[0]) + 1;   // every entry is met at most once
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
@@ -86,9 +85,8 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         const uint32_t sg = g.seg_of ? __ldg(&g.seg_of[i]) : 0u;
         uint32_t k = __ldg(&g.root_begin[sg]);
         const uint32_t end = __ldg(&g.root_end[sg]);
-        uint32_t steps = 0, cnt = 0;
+        uint32_t cnt = 0;
         while (k < end) {
-            if (++steps > limit) { set_err(err, kErrStack); break; }
             const float4 A = __ldg(&src[k]);
             const LT L = __ldg(&link[k]);
             const float m = D == 2 ? A.z : A.w;
@@ -180,7 +178,9 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
 #pragma unroll
                 for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
             }
-            k = acc ? link_skip(L) : k + 1;
+            // a valid skip lies past k; max() keeps k increasing whatever the
+            // layout holds, so the walk ends within end - begin entries
+            k = max(k + 1, acc ? link_skip(L) : k + 1);
         }
         float a3[3];
 #pragma unroll
