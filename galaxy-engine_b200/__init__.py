@@ -52,7 +52,8 @@ class Params(C.Structure):
         ("eps2", C.c_float), ("dt", C.c_float), ("leaf_cap", C.c_uint32),
         ("size_gate", C.c_float), ("min_size", C.c_float), ("node_cap_factor", C.c_float),
         ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
-        ("group_size", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("group_size", C.c_int32), ("temp_enabled", C.c_int32), ("heat_cond", C.c_float),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -112,6 +113,8 @@ SIGNATURES = {
     "ge_download": ([_vp] + [_vp] * 11, C.c_int),
     "ge_upload_pinned": ([_vp, _vp], C.c_int),
     "ge_download_prev_vel": ([_vp, _vp, _vp, _vp], C.c_int),
+    "ge_upload_temp": ([_vp, _vp], C.c_int),
+    "ge_download_temp": ([_vp, _vp], C.c_int),
     "ge_step": ([_vp, C.c_int32], C.c_int),
     "ge_profile_step": ([_vp], C.c_int),
     "ge_frame_host": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
@@ -356,6 +359,15 @@ class Simulation:
         out, ptrs = self._host_state(n)
         self._check(lib().ge_batch_download_sim(self._h, int(sim), *ptrs))
         return out
+
+    def upload_temp(self, temp):
+        t = np.ascontiguousarray(temp, np.float32)
+        self._check(lib().ge_upload_temp(self._h, _ptr(t)))
+
+    def download_temp(self):
+        t = np.empty(self.n, np.float32)
+        self._check(lib().ge_download_temp(self._h, _ptr(t)))
+        return t
 
     def download_prev_vel(self):
         n = self.n

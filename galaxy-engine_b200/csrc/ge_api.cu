@@ -48,6 +48,7 @@ struct Buffers {
     unsigned long long *d_inter = nullptr;
     bool prev = false;     // prevVel arrays allocated
     bool pinned = false;   // pin flag arrays allocated
+    bool temp = false;     // temperatures and node temperature arrays allocated
     bool mixed = false;    // GE_PREC_MIXED Kahan terms and node moments allocated
     bool mixed_entry = false;   // ... the per-particle walk's entry arrays
     bool mixed_group = false;   // ... the group walk's slot arrays and work stacks
@@ -177,6 +178,7 @@ StepParams step_params(const ge_ctx *c) {
     s.min_size = c->p.min_size;
     s.periodic = c->p.periodic ? 1 : 0;
     s.group_size = c->p.group_size;
+    s.heat_cond = c->p.heat_cond;
     for (int a = 0; a < 3; a++) {
         s.domain[a] = c->p.domain[a];
         s.half_domain[a] = c->p.domain[a] * 0.5f;
@@ -194,6 +196,8 @@ int validate(ge_ctx *c, const ge_params *p) {
     if (!(p->eps2 >= 0.0f)) return fail(c, GE_ERR_ARG, "eps2 must be >= 0");
     if (p->leaf_cap < 1) return fail(c, GE_ERR_ARG, "leaf_cap must be >= 1");
     if (!(p->node_cap_factor >= 1.0f)) return fail(c, GE_ERR_ARG, "node_cap_factor must be >= 1");
+    if (p->temp_enabled && p->precision == GE_PREC_MIXED)
+        return fail(c, GE_ERR_UNSUPPORTED, "heat exchange runs in GE_PREC_EXACT and GE_PREC_FAST");
     if (p->group_size != 0 && p->group_size != 32 && p->group_size != 64 && p->group_size != 128)
         return fail(c, GE_ERR_ARG, "group_size must be 0, 32, 64 or 128");
     if (p->periodic && (!(p->domain[0] > 0) || !(p->domain[1] > 0) ||
@@ -203,7 +207,8 @@ int validate(ge_ctx *c, const ge_params *p) {
 }
 
 // Allocates every per-particle and tree buffer of `nb` for cap particles.
-int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool prev, bool pinned) {
+int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool prev, bool pinned,
+                  bool temp = false) {
     const int D = c->p.dims;
     const size_t N = (size_t)cap;
     auto &L = nb.allocs;
@@ -226,6 +231,10 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
             if (D == 3) GE_CHECK(c, dalloc(L, &s.pvz, N));
         }
         if (pinned) GE_CHECK(c, dalloc(L, &s.pinned, N));
+        if (temp) {
+            GE_CHECK(c, dalloc(L, &s.temp, N));
+            if (!L.dry) GE_CHECK(c, cudaMemsetAsync(s.temp, 0, sizeof(float) * N, c->stream));
+        }
     }
     SortScratch &ss = nb.ss;
     GE_CHECK(c, dalloc(L, &ss.keys[0], N)); GE_CHECK(c, dalloc(L, &ss.keys[1], N));
@@ -259,6 +268,11 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     GE_CHECK(c, dalloc(L, &t.lvl_alloc, kMaxLevels + 2));
     GE_CHECK(c, dalloc(L, &t.meta, 16));
     GE_CHECK(c, dalloc(L, &t.tl, kTimeline));
+    if (temp) {
+        GE_CHECK(c, dalloc(L, &t.ntemp, (size_t)node_cap));
+        GE_CHECK(c, dalloc(L, &t.tv, N + (size_t)node_cap + 1));
+    }
+    nb.temp = temp;
     if (!L.dry) GE_CHECK(c, cudaMemsetAsync(t.meta, 0, 16 * sizeof(uint32_t), c->stream));
     GE_CHECK(c, dalloc(L, &nb.d_inter, 1));
     return GE_OK;
@@ -354,6 +368,9 @@ int copy_range(ge_ctx *c, const State &dst, int64_t doff, const State &src, int6
     if (pinned)
         GE_CHECK(c, cudaMemcpyAsync(dst.pinned + doff, src.pinned + soff, (size_t)cnt,
                                     cudaMemcpyDeviceToDevice, c->stream));
+    if (dst.temp && src.temp)
+        GE_CHECK(c, cudaMemcpyAsync(dst.temp + doff, src.temp + soff, B, cudaMemcpyDeviceToDevice,
+                                    c->stream));
     return GE_OK;
 }
 
@@ -385,7 +402,7 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep, bool exact = fal
     const int64_t node_cap = node_cap_for(c, cap, scap, slack);
     if (node_cap >= (1ll << 32) - 1) return fail(c, GE_ERR_ARG, "node capacity exceeds 2^32");
     Buffers nb;
-    int rc = alloc_buffers(c, nb, cap, node_cap, want_prev, ob.pinned);
+    int rc = alloc_buffers(c, nb, cap, node_cap, want_prev, ob.pinned, ob.temp);
     if (!rc && (ob.mixed || c->p.precision == GE_PREC_MIXED)) rc = alloc_mixed(c, nb);
     if (!rc && ((ob.mixed_entry && !nb.mixed_entry) || (ob.mixed_group && !nb.mixed_group))) {
         // keep every array set the old buffers had
@@ -531,12 +548,13 @@ int check_device(ge_ctx *c) {
 }
 
 // The state as the kernels see it: pin flags only when uploaded, Kahan terms
-// only in the mixed mode.
+// only in the mixed mode (the walk sees temperatures only with heat exchange
+// on, enqueue_walk).
 State view(ge_ctx *c, int which) {
     State s = c->b.st[which];
     if (!c->has_pinned) s.pinned = nullptr;
     if (c->p.precision != GE_PREC_MIXED) s.kx = s.ky = s.kz = s.kvx = s.kvy = s.kvz = nullptr;
-    return s;
+    return s;   // temperatures travel with the particles whenever they exist
 }
 
 State cur_state(ge_ctx *c) { return view(c, c->cur); }
@@ -575,6 +593,9 @@ int enqueue_build(ge_ctx *c) {
         GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, t, c->d_err, c->num_sms,
                                    c->stream));
     }
+    if (c->p.temp_enabled && c->b.temp)
+        GE_CHECK(c, launch_node_temps(c->p.dims, cur_state(c), p, c->b.tree, c->num_sms,
+                                      c->stream));
     return GE_OK;
 }
 
@@ -603,8 +624,10 @@ int enqueue_walk(ge_ctx *c, bool integrate_end) {
                                       c->stream));
         return GE_OK;
     }
-    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, cur_state(c), p, c->g, mixed_view(c),
-                            integrate_end, cnt, c->d_err, c->stream));
+    State s = cur_state(c);
+    if (!c->p.temp_enabled) s.temp = nullptr;
+    GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, s, p, c->g, mixed_view(c), integrate_end,
+                            cnt, c->d_err, c->stream));
     return GE_OK;
 }
 
@@ -683,6 +706,7 @@ int put_host(ge_ctx *c, int64_t off, int64_t n, const float *x, const float *y, 
             GE_CHECK(c, cudaMemcpyAsync(s.pvz + off, s.vz + off, B, cudaMemcpyDeviceToDevice, st));
     }
     if (c->b.pinned) GE_CHECK(c, cudaMemsetAsync(s.pinned + off, 0, (size_t)n, st));
+    if (s.temp) GE_CHECK(c, cudaMemsetAsync(s.temp + off, 0, B, st));
     if (s.kx) {
         float *kp[6] = {s.kx, s.ky, s.kz, s.kvx, s.kvy, s.kvz};
         for (float *q : kp)
@@ -737,6 +761,7 @@ void ge_params_default(ge_params *p, int dims) {
     p->domain[1] = p->dims == 2 ? 2160.0f : 1300.0f;
     p->domain[2] = 1300.0f;
     p->group_size = 32;
+    p->heat_cond = 0.045f;      // globalHeatConductivity (parameters.h:120)
 }
 
 int ge_create(const ge_params *p, ge_ctx **out) {
@@ -877,6 +902,40 @@ int ge_upload_pinned(ge_ctx *c, const uint8_t *pinned) {
                                 cudaMemcpyHostToDevice, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     c->has_pinned = true;
+    return GE_OK;
+}
+
+int ge_upload_temp(ge_ctx *c, const float *temp) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!temp) return fail(c, GE_ERR_ARG, "temp is NULL");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    if (!c->b.temp) {
+        auto &L = c->b.allocs;
+        const size_t N = (size_t)c->b.cap_n;
+        for (int k = 0; k < 2; k++) {
+            GE_CHECK(c, dalloc(L, &c->b.st[k].temp, N));
+            GE_CHECK(c, cudaMemsetAsync(c->b.st[k].temp, 0, sizeof(float) * N, c->stream));
+        }
+        GE_CHECK(c, dalloc(L, &c->b.tree.ntemp, (size_t)c->b.tree.cap));
+        GE_CHECK(c, dalloc(L, &c->b.tree.tv, N + (size_t)c->b.tree.cap + 1));
+        c->b.temp = true;
+    }
+    GE_CHECK(c, cudaMemcpyAsync(c->b.st[c->cur].temp, temp, sizeof(float) * (size_t)c->n,
+                                cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    c->tree_valid = false;
+    return GE_OK;
+}
+
+int ge_download_temp(ge_ctx *c, float *temp) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!temp) return fail(c, GE_ERR_ARG, "temp is NULL");
+    if (!c->b.temp) return fail(c, GE_ERR_STATE, "no temperatures uploaded");
+    GE_CHECK(c, cudaMemcpyAsync(temp, c->b.st[c->cur].temp, sizeof(float) * (size_t)c->n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
     return GE_OK;
 }
 

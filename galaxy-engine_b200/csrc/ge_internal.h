@@ -20,6 +20,7 @@ struct State {
     // (nullptr in the other modes)
     float *kx, *ky, *kz;
     float *kvx, *kvy, *kvz;
+    float *temp;          // temperatures (nullptr unless heat exchange is on)
 };
 
 // Tree nodes, structure-of-arrays.
@@ -41,7 +42,7 @@ struct State {
 //   src     float4  2D node {com.x, com.y, mass, size^2}; particle {x, y, m, -1}
 //                   3D node {com.x, com.y, com.z, mass};  particle {x, y, z, m}
 //   link    2D uint32 skip; 3D uint2 {skip, size^2 bits} (particles: size^2 = -1,
-//                   which every opening test accepts).  skip is where the walk
+//                   massless nodes: -2, both accepted by every opening test).  skip is where the walk
 //                   goes after accepting the entry: the successor of the node's
 //                   subtree, or the next entry for a particle.
 //   slot_of uint32  entry index of each particle (for the self test)
@@ -88,6 +89,11 @@ struct Tree {
     uint32_t *wl;         // group walk: a work stack per resident warp
     uint32_t wl_warps;    // warps the work stacks are sized for
     uint2 *grp;           // group walk: particle range of each group [n + 1]
+    // heat exchange (nullptr unless on): node temperature sums per slot, and
+    // per walk entry the temperature the walk reads (a node's average, a
+    // particle's own, both as before the walk)
+    float *ntemp;
+    float *tv;
     int64_t cap;
 };
 
@@ -138,6 +144,7 @@ struct StepParams {
     int periodic;
     float domain[3], half_domain[3];
     int group_size;   // GE_PREC_MIXED: 0 = per-particle walk, else the group walk
+    float heat_cond;  // heat exchange coefficient (used when State::temp is set)
 };
 
 constexpr int kBBoxThreads = 256;
@@ -191,6 +198,10 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         const Segs &g, const Tree &t, bool integrate_end,
                         unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+// heat exchange: node temperature sums bottom-up in the reference's order and
+// the walk's temperature entries (after launch_build)
+cudaError_t launch_node_temps(int dims, const State &s, const StepParams &p, Tree &t,
+                              int num_sms, cudaStream_t st);
 // GE_PREC_MIXED: FP64 mass, centre of mass and second moments of every node,
 // bottom-up from the particles, written into the walk entries with the
 // offset-corrected opening radius (after launch_build)

@@ -250,6 +250,7 @@ __global__ void k_permute(const uint64_t *__restrict__ keys, const uint32_t *__r
             if (D == 3) out.pvz[k] = in.pvz[j];
         }
         if (in.pinned) out.pinned[k] = in.pinned[j];
+        if (in.temp) out.temp[k] = in.temp[j];
         if (in.kx) {
             out.kx[k] = in.kx[j]; out.ky[k] = in.ky[j];
             out.kvx[k] = in.kvx[j]; out.kvy[k] = in.kvy[j];

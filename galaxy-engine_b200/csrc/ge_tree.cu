@@ -866,12 +866,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
         const bool massless = nm <= 0.0f;
         if (massless) {
             // gridMass <= 0: the reference skips the whole subtree.  As a source
-            // it is accepted by every test (size^2 = -1), carries no mass (the
-            // walk makes no interaction with a massless source) and leads to
-            // its successor.
-            t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -1.0f) : make_float4(w.x, w.y, w.z, 0.0f);
+            // it is accepted by every test (size^2 = -2; particles have -1),
+            // carries no mass (the walk makes no interaction with a massless
+            // node) and leads to its successor.
+            t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -2.0f) : make_float4(w.x, w.y, w.z, 0.0f);
             if (D == 2) ((uint32_t *)t.link)[me] = skip;
-            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-1.0f));
+            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
         } else {
             t.src[me] = w;
             if (D == 2) ((uint32_t *)t.link)[me] = skip;

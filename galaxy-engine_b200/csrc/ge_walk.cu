@@ -60,12 +60,12 @@ template <int D> struct LinkOf;
 template <> struct LinkOf<2> { using T = uint32_t; };
 template <> struct LinkOf<3> { using T = uint2; };
 
-template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
+template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS, bool TEMP = false>
 __global__ void __launch_bounds__(kWalkThreads)
 k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
     using LT = typename LinkOf<D>::T;
-    constexpr bool kSelfTest = MODE != GE_PREC_FAST || COUNT || !POS_EPS;
+    constexpr bool kSelfTest = MODE != GE_PREC_FAST || COUNT || !POS_EPS || TEMP;
     const LT *__restrict__ link = (const LT *)t.link;
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
@@ -81,6 +81,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         const uint32_t self = kSelfTest ? __ldg(&t.slot_of[i]) : kEmpty;
         float f[3] = {0.f, 0.f, 0.f};
         float fc[3] = {0.f, 0.f, 0.f};   // Kahan compensation (MIXED)
+        float ti = TEMP ? __ldg(&t.tv[self]) : 0.0f;   // own temperature, accumulated in walk order
         // the walk of the particle's own segment: its root to the root's successor
         const uint32_t sg = g.seg_of ? __ldg(&g.seg_of[i]) : 0u;
         uint32_t k = __ldg(&g.root_begin[sg]);
@@ -106,6 +107,19 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
             // includes 1 / theta
             const bool acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
             if (kSelfTest) {
+                // heat exchange (physics.cpp:145-158, 183-191): an accepted node
+                // with mass, or any other particle of an opened leaf (massless
+                // ones included); the others' temperatures as before the walk
+                if (TEMP && acc && k != self && (m != 0.0f || s2 == -1.0f)) {
+                    float inv;
+                    if (MODE == GE_PREC_EXACT) inv = fdiv(1.0f, __fsqrt_rn(r2));
+                    else inv = rsqrt_approx(r2);
+                    const float dist = r2 > 1e-16f ? fdiv(1.0f, inv) : 0.0f;
+                    if (dist > 1e-8f) {
+                        const float diff = fsub(__ldg(&t.tv[k]), ti);
+                        ti = fadd(ti, fmul(fdiv(fmul(p.heat_cond, diff), dist), p.dt));
+                    }
+                }
                 if (acc && m != 0.0f && k != self) {
                     if (MODE == GE_PREC_MIXED) {
                         float term[3];
@@ -189,6 +203,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
                   : MODE == GE_PREC_MIXED ? G * fsub(f[a], fc[a]) : G * f[a];
         s.ax[i] = a3[0]; s.ay[i] = a3[1];
         if (D == 3) s.az[i] = a3[2];
+        if (TEMP) s.temp[i] = ti;
         if (integrate_end && !(s.pinned && s.pinned[i])) {
             if (MODE == GE_PREC_MIXED && s.kvx) {
                 float *vel[3] = {s.vx, s.vy, s.vz}, *kv[3] = {s.kvx, s.kvy, s.kvz};
@@ -208,11 +223,11 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
     }
 }
 
-template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS>
+template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS, bool TEMP = false>
 static cudaError_t walk_one(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
     const int blocks = (p.n + kWalkThreads - 1) / kWalkThreads;
-    k_walk<D, MODE, COUNT, PER, POS_EPS>
+    k_walk<D, MODE, COUNT, PER, POS_EPS, TEMP>
         <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, g, t, ie, inter, err);
     return cudaGetLastError();
 }
@@ -220,6 +235,11 @@ static cudaError_t walk_one(const State &s, const StepParams &p, const Segs &g, 
 template <int D, int MODE, bool PER>
 static cudaError_t walk_eps(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
+    if constexpr (MODE != GE_PREC_MIXED)
+        if (s.temp && t.tv) {   // heat exchange (counting included)
+            if (inter) return walk_one<D, MODE, true, PER, false, true>(s, p, g, t, ie, inter, err, st);
+            return walk_one<D, MODE, false, PER, false, true>(s, p, g, t, ie, nullptr, err, st);
+        }
     if (inter) return walk_one<D, MODE, true, PER, false>(s, p, g, t, ie, inter, err, st);
     if constexpr (MODE != GE_PREC_MIXED)   // MIXED always tests for the particle itself
         if (p.eps2 > 0.0f)

@@ -74,7 +74,10 @@ typedef struct {
     int32_t track_prev_vel;  /* keep prevVel as the reference does (integrateStart) */
     int32_t group_size;      /* GE_PREC_MIXED walk: particles that share one traversal
                                 (32, 64 or 128; 0 = every particle walks alone) */
-    int32_t reserved[6];
+    int32_t temp_enabled;    /* heat exchange in the walk (myVar.isTempEnabled, default off;
+                                GE_PREC_EXACT / GE_PREC_FAST); temperatures via ge_upload_temp */
+    float heat_cond;         /* myVar.globalHeatConductivity (parameters.h:120) */
+    int32_t reserved[4];
 } ge_params;
 
 typedef struct {
@@ -120,6 +123,16 @@ int ge_download(ge_ctx *ctx, float *x, float *y, float *z, float *vx, float *vy,
    in the current particle order; NULL clears them */
 int ge_upload_pinned(ge_ctx *ctx, const uint8_t *pinned);
 int ge_download_prev_vel(ge_ctx *ctx, float *pvx, float *pvy, float *pvz);
+/* particle temperatures (ParticlePhysics::temp), in the current particle
+   order; with temp_enabled each step's walk exchanges heat as the reference
+   does (physics.cpp:145-158, 183-191; physics3D.cpp:190-201, 230-237): an
+   accepted node by its average temperature, a leaf's particles one by one,
+   temp_i += heat_cond * (T - temp_i) / distance * dt.  The reference changes
+   temp_i in place while other threads read it; here every particle reads the
+   others' temperatures (and the node averages) as they were before the walk
+   and accumulates its own in walk order. */
+int ge_upload_temp(ge_ctx *ctx, const float *temp);
+int ge_download_temp(ge_ctx *ctx, float *temp);
 
 /* --- the fused step ---------------------------------------------------- */
 /* nsteps full frames on the resident state (globalLogic.cpp:1155-1370 /

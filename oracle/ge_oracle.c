@@ -346,10 +346,16 @@ void or_walk2d(int64_t n, const float *x, const float *y, const float *m, float 
     const float dx_dom = p->domain[0], dy_dom = p->domain[1];
     const float hx = dx_dom * 0.5f, hy = dy_dom * 0.5f;
     const int use_temp = p->temp_enabled && temp;
+    /* other particles' temperatures (and the nodes' sums, taken at build
+       time) are read as they were before the walk; each particle accumulates
+       its own in walk order (see the header) */
+    float *told = use_temp ? (float *)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1)) : NULL;
+    if (told) memcpy(told, temp, sizeof(float) * (size_t)n);
 #pragma omp parallel for schedule(dynamic) num_threads(nthreads)
     for (int64_t i = 0; i < n; i++) {
         float fx = 0.0f, fy = 0.0f;
         double absf = 0.0;
+        float ti = told ? told[i] : 0.0f;
         uint32_t cnt = 0;
         const float pm = m[i], xi = x[i], yi = y[i];
         uint32_t k = 0;
@@ -373,10 +379,10 @@ void or_walk2d(int64_t n, const float *x, const float *y, const float *m, float 
                     uint32_t c = t->end[k] - t->start[k];
                     if (c > 0) {
                         float avg = t->temp[k] / (float)c;
-                        float diff = avg - temp[i];
+                        float diff = avg - ti;
                         float dist = 0.0f;
                         if (r2 > 1e-16f) dist = 1.0f / inv;
-                        if (dist > 1e-8f) temp[i] += p->heat_cond * diff / dist * p->dt;
+                        if (dist > 1e-8f) ti += p->heat_cond * diff / dist * p->dt;
                     }
                 }
                 k += t->next[k] + 1;
@@ -394,10 +400,10 @@ void or_walk2d(int64_t n, const float *x, const float *y, const float *m, float 
                     absf += sqrt((double)(ddx * fm) * (ddx * fm) + (double)(ddy * fm) * (ddy * fm));
                     cnt++;
                     if (use_temp) {
-                        float diff = temp[j] - temp[i];
+                        float diff = told[j] - ti;
                         float dist = 0.0f;
                         if (rr > 1e-16f) dist = 1.0f / inv;
-                        if (dist > 1e-8f) temp[i] += p->heat_cond * diff / dist * p->dt;
+                        if (dist > 1e-8f) ti += p->heat_cond * diff / dist * p->dt;
                     }
                 }
                 k += t->next[k] + 1;
@@ -407,12 +413,14 @@ void or_walk2d(int64_t n, const float *x, const float *y, const float *m, float 
         }
         ax[i] = fx / m[i];
         ay[i] = fy / m[i];
+        if (told) temp[i] = ti;
         if (inter) inter[i] = cnt;
         if (cond) {
             double net = sqrt((double)fx * fx + (double)fy * fy);
             cond[i] = net > 0 ? (float)(absf / net) : INFINITY;
         }
     }
+    free(told);
 }
 
 void or_walk3d(int64_t n, const float *x, const float *y, const float *z, const float *m,
@@ -425,10 +433,13 @@ void or_walk3d(int64_t n, const float *x, const float *y, const float *z, const 
     const int per = p->periodic;
     const float hx = p->domain[0] * 0.5f, hy = p->domain[1] * 0.5f, hz = p->domain[2] * 0.5f;
     const int use_temp = p->temp_enabled && temp;
+    float *told = use_temp ? (float *)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1)) : NULL;
+    if (told) memcpy(told, temp, sizeof(float) * (size_t)n);
 #pragma omp parallel for schedule(dynamic) num_threads(nthreads)
     for (int64_t i = 0; i < n; i++) {
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         double absf = 0.0;
+        float ti = told ? told[i] : 0.0f;
         uint32_t cnt = 0;
         const float pm = m[i], xi = x[i], yi = y[i], zi = z[i];
         uint32_t k = 0;
@@ -456,10 +467,10 @@ void or_walk3d(int64_t n, const float *x, const float *y, const float *z, const 
                     uint32_t c = t->end[k] - t->start[k];
                     if (c > 0) {
                         float avg = t->temp[k] / (float)c;
-                        float diff = avg - temp[i];
+                        float diff = avg - ti;
                         float dist = 0.0f;
                         if (r2 > 1e-16f) dist = 1.0f / inv;
-                        if (dist > 1e-8f) temp[i] += p->heat_cond * diff / dist * p->dt;
+                        if (dist > 1e-8f) ti += p->heat_cond * diff / dist * p->dt;
                     }
                 }
                 k += t->next[k] + 1;
@@ -480,10 +491,10 @@ void or_walk3d(int64_t n, const float *x, const float *y, const float *z, const 
                     absf += fabs((double)fm) * sqrt((double)ddx * ddx + (double)ddy * ddy + (double)ddz * ddz);
                     cnt++;
                     if (use_temp) {
-                        float diff = temp[j] - temp[i];
+                        float diff = told[j] - ti;
                         float dist = 0.0f;
                         if (rr > 1e-16f) dist = 1.0f / inv;
-                        if (dist > 1e-8f) temp[i] += p->heat_cond * diff / dist * p->dt;
+                        if (dist > 1e-8f) ti += p->heat_cond * diff / dist * p->dt;
                     }
                 }
                 k += t->next[k] + 1;
@@ -494,12 +505,14 @@ void or_walk3d(int64_t n, const float *x, const float *y, const float *z, const 
         ax[i] = fx / m[i];
         ay[i] = fy / m[i];
         az[i] = fz / m[i];
+        if (told) temp[i] = ti;
         if (inter) inter[i] = cnt;
         if (cond) {
             double net = sqrt((double)fx * fx + (double)fy * fy + (double)fz * fz);
             cond[i] = net > 0 ? (float)(absf / net) : INFINITY;
         }
     }
+    free(told);
 }
 
 /* ------------------------------------------------------------------ */

@@ -98,6 +98,12 @@ int or_build_octree(or_tree *t, int64_t n, const float *x, const float *y, const
                     uint32_t leaf_cap, float size_gate, float min_size);
 
 /* --- force ------------------------------------------------------------ */
+/* Temperature (temp_enabled): the reference updates temp[i] in place inside
+ * an OpenMP-parallel loop while other threads read it as their temp[j]
+ * (physics.cpp:145-158, 183-191), so its result depends on thread timing.
+ * The oracle fixes one order: every particle reads the other particles'
+ * temperatures, and the nodes' sums, as they were before the walk, and
+ * accumulates its own in its walk order; the device walk does the same. */
 /* scalar walk (parity oracle).  temp may be NULL when temp_enabled == 0.
  * inter (optional, [n]) receives the per-particle interaction count:
  * accepted monopoles + leaf pairs j != i.  cond (optional, [n]) receives

@@ -46,8 +46,9 @@ def test_abi_version_and_defaults(ge):
 
 
 def test_struct_layouts_match_header(ge):
-    # ge_params: 11 scalars + domain[3] + track_prev_vel + group_size + reserved[6]
-    assert C.sizeof(ge.Params) == 4 * (11 + 3 + 1 + 1 + 6)
+    # ge_params: 11 scalars + domain[3] + track_prev_vel, group_size, temp_enabled,
+    # heat_cond + reserved[4]
+    assert C.sizeof(ge.Params) == 4 * (11 + 3 + 1 + 1 + 2 + 4)
     # ge_stats: 84 bytes of fields, padded to the 8-byte alignment of its int64 members
     assert C.sizeof(ge.Stats) == 88
 
