@@ -114,6 +114,8 @@ SIGNATURES = {
     "ge_upload_pinned": ([_vp, _vp], C.c_int),
     "ge_download_prev_vel": ([_vp, _vp, _vp, _vp], C.c_int),
     "ge_upload_temp": ([_vp, _vp], C.c_int),
+    "ge_predict_trajectory": ([_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_float, C.c_int32,
+                               _vp], C.c_int),
     "ge_download_temp": ([_vp, _vp], C.c_int),
     "ge_step": ([_vp, C.c_int32], C.c_int),
     "ge_profile_step": ([_vp], C.c_int),
@@ -359,6 +361,18 @@ class Simulation:
         out, ptrs = self._host_state(n)
         self._check(lib().ge_batch_download_sim(self._h, int(sim), *ptrs))
         return out
+
+    def predict_trajectory(self, pos, vel, mass, steps, eps2, sim=0):
+        """predictTrajectory (particlesSpawning.cpp:443-500): probe paths on the
+        tree of the last step; returns [nprobes, steps, dims]."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, self.dims)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, self.dims)
+        mass = np.ascontiguousarray(mass, np.float32).ravel()
+        path = np.zeros((len(mass), int(steps), self.dims), np.float32)
+        self._check(lib().ge_predict_trajectory(self._h, int(sim), len(mass), _ptr(pos),
+                                                _ptr(vel), _ptr(mass), float(eps2), int(steps),
+                                                _ptr(path)))
+        return path
 
     def upload_temp(self, temp):
         t = np.ascontiguousarray(temp, np.float32)

@@ -1214,6 +1214,42 @@ int ge_direct_sum_f64(ge_ctx *c, int64_t nt, const uint32_t *idx, double *ax, do
     return GE_OK;
 }
 
+int ge_predict_trajectory(ge_ctx *c, int32_t sim, int32_t nprobes, const float *pos,
+                          const float *vel, const float *mass, float eps2, int32_t steps,
+                          float *path) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (nprobes < 0 || steps < 0 || (nprobes > 0 && (!pos || !vel || !mass || !path)))
+        return fail(c, GE_ERR_ARG, "bad probes");
+    if (nprobes == 0 || steps == 0) return GE_OK;
+    if (c->p.precision == GE_PREC_MIXED)
+        return fail(c, GE_ERR_UNSUPPORTED, "trajectory preview needs GE_PREC_EXACT or GE_PREC_FAST");
+    if (!c->tree_valid) return fail(c, GE_ERR_STATE, "no tree: step or build first");
+    int r = 0;
+    if (sim != 0 && (r = find_sim(c, sim)) < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    const int D = c->p.dims;
+    uint32_t be[2];
+    GE_CHECK(c, cudaMemcpyAsync(&be[0], c->g.root_begin + r, sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(&be[1], c->g.root_end + r, sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, c->stream));
+    float *d = nullptr;
+    const size_t np = (size_t)nprobes, pn = np * (size_t)steps * D;
+    GE_CHECK(c, cudaMallocAsync((void **)&d, sizeof(float) * (np * (2 * D + 1) + pn), c->stream));
+    float *dpos = d, *dvel = d + np * D, *dm = d + 2 * np * D, *dpath = d + np * (2 * D + 1);
+    GE_CHECK(c, cudaMemcpyAsync(dpos, pos, sizeof(float) * np * D, cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(dvel, vel, sizeof(float) * np * D, cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(dm, mass, sizeof(float) * np, cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    StepParams p = step_params(c);
+    GE_CHECK(c, launch_predict(D, c->b.tree, p, be[0], be[1], eps2, nprobes, dpos, dvel, dm, steps,
+                               dpath, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(path, dpath, sizeof(float) * pn, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaFreeAsync(d, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    return GE_OK;
+}
+
 int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
     int rc = require_state(c);
     if (rc) return rc;

@@ -198,6 +198,12 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         const Segs &g, const Tree &t, bool integrate_end,
                         unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+// trajectory preview: probes stepped against the walk layout of the last
+// build, entries [begin, end) (one simulation's tree)
+cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, uint32_t begin,
+                           uint32_t end, float eps2, int nprobes, const float *pos,
+                           const float *vel, const float *mass, int steps, float *path,
+                           cudaStream_t st);
 // heat exchange: node temperature sums bottom-up in the reference's order and
 // the walk's temperature entries (after launch_build)
 cudaError_t launch_node_temps(int dims, const State &s, const StepParams &p, Tree &t,

@@ -194,6 +194,21 @@ int ge_integrate_end(ge_ctx *ctx);
 /* enable per-particle interaction counting in ge_compute_forces (stats) */
 int ge_set_count_interactions(ge_ctx *ctx, int32_t enable);
 
+/* --- trajectory preview ------------------------------------------------
+ * ParticlesSpawning::predictTrajectory (particlesSpawning.cpp:443-500, 3D
+ * :1000-1060): nprobes probe particles (pos, vel: [nprobes * dims] host
+ * arrays; mass [nprobes]) are each stepped `steps` times against the tree of
+ * the last step, which is not rebuilt, with the older walk the preview uses
+ * (Physics::calculateForceFromGridOld, physics.cpp:4-90 / physics3D.cpp:
+ * 49-120: leaves taken whole, a one-particle leaf within 0.001 of the probe
+ * skipped).  eps2 is the value that walk adds to r^2: softening^2 in both 2D
+ * and 3D.  path [nprobes * steps * dims] receives each step's position.
+ * sim: the simulation's handle (0: the context's first simulation).  Needs
+ * GE_PREC_EXACT or GE_PREC_FAST (the walk layout holds node sizes). */
+int ge_predict_trajectory(ge_ctx *ctx, int32_t sim, int32_t nprobes, const float *pos,
+                          const float *vel, const float *mass, float eps2, int32_t steps,
+                          float *path);
+
 /* --- FP64 diagnostics (accuracy reference; not on the step path) ------- */
 /* Direct-sum accelerations in FP64 of the particles at indices idx[0..nt) of
    the current order: sum over j != i of G m_j d / (|d|^2 + eps2)^(3/2), j over

@@ -861,3 +861,88 @@ int or_frame(const or_params *p, int64_t n, float *x, float *y, float *z,
     free(keys); free(perm); free(tmp);
     return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* trajectory preview: ParticlesSpawning::predictTrajectory            */
+/* (particlesSpawning.cpp:443-500, 3D :1000-1060) with the walk it     */
+/* calls, Physics::calculateForceFromGridOld (physics.cpp:4-90, 3D     */
+/* physics3D.cpp:49-120): leaves are taken whole (never opened), a     */
+/* one-particle leaf within 0.001 of the probe on every axis is        */
+/* skipped, softening is added squared in 2D and 3D (eps2 here).       */
+/* ------------------------------------------------------------------ */
+static void old_force(const or_tree *t, const float *pp[3], const or_params *p, float eps2,
+                      const float pos[3], float pmass, float F[3]) {
+    const int D = t->dims;
+    const float thetaSq = p->theta * p->theta;
+    F[0] = F[1] = F[2] = 0.0f;
+    uint32_t k = 0;
+    const uint32_t count = (uint32_t)t->count;
+    while (k < count) {
+        const float gm = t->mass[k];
+        if (gm <= 0.0f) { k += t->next[k] + 1; continue; }
+        float d[3] = {0, 0, 0};
+        for (int a = 0; a < D; a++) {
+            d[a] = t->com[(int64_t)k * D + a] - pos[a];
+            if (p->periodic) {
+                const float h = p->domain[a] * 0.5f;
+                d[a] -= p->domain[a] * (float)((d[a] > h) - (d[a] < -h));
+            }
+        }
+        float r2 = d[0] * d[0] + d[1] * d[1];
+        if (D == 3) r2 = r2 + d[2] * d[2];
+        r2 = r2 + eps2;
+        const int leaf = node_is_leaf(t, k);
+        const float sz = t->size[k];
+        if ((sz * sz < thetaSq * r2) || leaf) {
+            if (t->end[k] - t->start[k] == 1) {
+                const uint32_t j = t->start[k];
+                int near = 1;
+                for (int a = 0; a < D; a++) near = near && fabsf(pp[a][j] - pos[a]) < 0.001f;
+                if (near) { k += t->next[k] + 1; continue; }
+            }
+            const float inv = 1.0f / sqrtf(r2);
+            const float inv3 = inv * inv * inv;
+            const float fm = p->G * pmass * gm * inv3;
+            for (int a = 0; a < D; a++) F[a] += d[a] * fm;
+            k += t->next[k] + 1;
+        } else {
+            ++k;
+        }
+    }
+}
+
+void or_predict_trajectory(const or_tree *t, const float *x, const float *y, const float *z,
+                           const or_params *p, float eps2, int64_t nprobes, const float *pos,
+                           const float *vel, const float *mass, int32_t steps, float *path,
+                           int nthreads) {
+    const int D = t->dims;
+    const float *pp[3] = {x, y, z};
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int64_t q = 0; q < nprobes; q++) {
+        float ps[3] = {0, 0, 0}, v[3] = {0, 0, 0}, F[3], acc[3];
+        for (int a = 0; a < D; a++) { ps[a] = pos[q * D + a]; v[a] = vel[q * D + a]; }
+        const float m = mass[q], h = p->dt * 0.5f;
+        for (int32_t s = 0; s < steps; s++) {
+            old_force(t, pp, p, eps2, ps, m, F);
+            for (int a = 0; a < D; a++) {
+                acc[a] = F[a] / m;
+                v[a] += acc[a] * h;
+            }
+            for (int a = 0; a < D; a++) ps[a] += v[a] * p->dt;
+            if (p->periodic) {
+                for (int a = 0; a < D; a++) {
+                    const float lo = D == 2 ? 0.0f : -p->domain[a] * 0.5f;
+                    const float hi = D == 2 ? p->domain[a] : p->domain[a] * 0.5f;
+                    if (ps[a] < lo) ps[a] += p->domain[a];
+                    else if (ps[a] >= hi) ps[a] -= p->domain[a];
+                }
+            }
+            old_force(t, pp, p, eps2, ps, m, F);
+            for (int a = 0; a < D; a++) {
+                acc[a] = F[a] / m;
+                v[a] += acc[a] * h;
+            }
+            for (int a = 0; a < D; a++) path[((int64_t)q * steps + s) * D + a] = ps[a];
+        }
+    }
+}

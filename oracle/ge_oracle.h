@@ -146,6 +146,17 @@ void or_walk_group(int64_t n, const float *x, const float *y, const float *z, co
                    const or_tree *t, const or_params *p, int group_size, double *ax, double *ay,
                    double *az, uint32_t *inter, int nthreads);
 
+/* --- trajectory preview (particlesSpawning.cpp:443-500, :1000-1060) ----
+ * nprobes probe particles (pos/vel [nprobes*dims], mass [nprobes]) stepped
+ * `steps` times against the fixed tree t built over particles x, y, z, with
+ * the older walk (physics.cpp:4-90, physics3D.cpp:49-120); eps2 is the
+ * softening added to r^2 (squared in both 2D and 3D in that walk).
+ * path [nprobes*steps*dims] receives each step's position. */
+void or_predict_trajectory(const or_tree *t, const float *x, const float *y, const float *z,
+                           const or_params *p, float eps2, int64_t nprobes, const float *pos,
+                           const float *vel, const float *mass, int32_t steps, float *path,
+                           int nthreads);
+
 /* --- leapfrog --------------------------------------------------------- */
 void or_integrate_start(int dims, int64_t n, float *x, float *y, float *z,
                         float *vx, float *vy, float *vz, const float *ax, const float *ay,

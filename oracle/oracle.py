@@ -93,6 +93,9 @@ def _load(strict=True):
                                _f32p, _f32p, _f32p, C.c_int]
     lib.or_direct_f64.argtypes = [C.c_int, C.c_int64, _f32p, _f32p, _vp, _f32p, C.c_double,
                                   C.c_double, C.c_int64, _i64p, _f64p, _f64p, _vp, C.c_int]
+    lib.or_predict_trajectory.argtypes = [C.POINTER(Tree), _f32p, _f32p, _vp, C.POINTER(Params),
+                                          C.c_float, C.c_int64, _f32p, _f32p, _f32p, C.c_int32,
+                                          _f32p, C.c_int]
     lib.or_walk_mixed.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
                                   C.POINTER(Params), _f64p, _f64p, _vp, _vp, C.c_int]
     lib.or_walk_group.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
@@ -246,6 +249,22 @@ def walk(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False, wa
     if want_cond:
         out.append(cond)
     return out
+
+
+def predict_trajectory(x, y, tree_holder, params, eps2, pos, vel, mass, steps, z=None,
+                       nthreads=8):
+    """predictTrajectory (particlesSpawning.cpp:443-500): probe paths against
+    the fixed tree; returns [nprobes, steps, dims]."""
+    x, y = _f32(x), _f32(y)
+    pos, vel, mass = _f32(pos), _f32(vel), _f32(mass)
+    dims = 2 if z is None else 3
+    nprobes = len(mass)
+    path = np.zeros(nprobes * steps * dims, np.float32)
+    zz = None if z is None else _f32(z)
+    lib().or_predict_trajectory(C.byref(tree_holder.t), x, y, _ptr(zz), C.byref(params), eps2,
+                                nprobes, pos.ravel(), vel.ravel(), mass, int(steps), path,
+                                nthreads)
+    return path.reshape(nprobes, steps, dims)
 
 
 def walk_mixed(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False):
