@@ -93,6 +93,13 @@ class TuneResult(C.Structure):
                 ("reserved", C.c_int32), ("ms", C.c_float * 12)]
 
 
+class SaveInfo(C.Structure):
+    """ge_save_info (include/ge_bh.h)."""
+    _fields_ = [("version", C.c_uint32), ("dims", C.c_int32), ("n", C.c_int64),
+                ("global_id", C.c_uint32), ("global_shape_id", C.c_uint32),
+                ("global_wall_id", C.c_uint32), ("record_bytes", C.c_int32)]
+
+
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 _vp = C.c_void_p
@@ -114,6 +121,8 @@ SIGNATURES = {
     "ge_upload_pinned": ([_vp, _vp], C.c_int),
     "ge_download_prev_vel": ([_vp, _vp, _vp, _vp], C.c_int),
     "ge_upload_temp": ([_vp, _vp], C.c_int),
+    "ge_save_read_info": ([C.c_char_p, C.POINTER(SaveInfo)], C.c_int),
+    "ge_save_read": ([C.c_char_p, C.c_int64] + [_vp] * 13, C.c_int),
     "ge_predict_trajectory": ([_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_float, C.c_int32,
                                _vp], C.c_int),
     "ge_download_temp": ([_vp, _vp], C.c_int),
@@ -581,3 +590,26 @@ class Server:
         s = ServerStats()
         self._check(lib().ge_server_get_stats(self._h, C.byref(s)))
         return s
+
+
+def load_save(path):
+    """A Galaxy Engine scene file (SaveSystem, versions 190 / 180) as a dict of
+    arrays for Simulation.upload (+ "temp", "pinned"), plus "dims"."""
+    info = SaveInfo()
+    p = os.fsencode(path)
+    rc = lib().ge_save_read_info(p, C.byref(info))
+    if rc != 0:
+        raise GeError(rc, f"cannot read scene file {path}")
+    n, d = int(info.n), int(info.dims)
+    keys = ["x", "y", "vx", "vy", "ax", "ay", "m", "temp"] + (["z", "vz", "az"] if d == 3 else [])
+    out = {k: np.zeros(n, np.float32) for k in keys}
+    out["id"] = np.zeros(n, np.uint32)
+    out["pinned"] = np.zeros(n, np.uint8)
+    g = out.get
+    rc = lib().ge_save_read(p, n, *[_ptr(g(k)) for k in ("x", "y", "z", "vx", "vy", "vz", "ax",
+                                                          "ay", "az", "m", "temp", "id",
+                                                          "pinned")])
+    if rc != 0:
+        raise GeError(rc, f"cannot read scene file {path}")
+    out["dims"] = d
+    return out

@@ -209,6 +209,30 @@ int ge_predict_trajectory(ge_ctx *ctx, int32_t sim, int32_t nprobes, const float
                           const float *vel, const float *mass, float eps2, int32_t steps,
                           float *path);
 
+/* --- scene files -------------------------------------------------------
+ * Reader of the reference's save files (SaveSystem, src/UX/saveSystem.cpp:
+ * 285-362; include/UX/saveSystem.h:120-290; versions 190 and 180): the YAML
+ * parameter block (is3DMode decides the dimension), then per particle the
+ * binary ParticlePhysics(3D) / ParticleRendering(3D) members
+ * (include/Particles/particle.h).  Host code only; no context or GPU needed.
+ * ge_save_read_info gives the header; ge_save_read copies the members the
+ * gravity step uses into caller arrays of at least `cap` particles, in the
+ * file's order (any pointer may be NULL; z/vz/az ignored in 2D):
+ * positions, velocities, accelerations, mass, temperature, id, isPinned.
+ * GE_ERR_UNSUPPORTED for other versions, GE_ERR_ARG for a missing,
+ * malformed or truncated file, GE_ERR_CAPACITY when cap is too small. */
+typedef struct {
+    uint32_t version;
+    int32_t dims;
+    int64_t n;
+    uint32_t global_id, global_shape_id, global_wall_id;
+    int32_t record_bytes;      /* bytes per particle record (180 in 2D, 208 in 3D) */
+} ge_save_info;
+int ge_save_read_info(const char *path, ge_save_info *info);
+int ge_save_read(const char *path, int64_t cap, float *x, float *y, float *z, float *vx,
+                 float *vy, float *vz, float *ax, float *ay, float *az, float *m, float *temp,
+                 uint32_t *id, uint8_t *pinned);
+
 /* --- FP64 diagnostics (accuracy reference; not on the step path) ------- */
 /* Direct-sum accelerations in FP64 of the particles at indices idx[0..nt) of
    the current order: sum over j != i of G m_j d / (|d|^2 + eps2)^(3/2), j over
