@@ -93,6 +93,14 @@ class TuneResult(C.Structure):
                 ("reserved", C.c_int32), ("ms", C.c_float * 12)]
 
 
+class FieldParams(C.Structure):
+    """ge_field_params (include/ge_bh.h)."""
+    _fields_ = [("res", C.c_int32), ("softness", C.c_float), ("threshold", C.c_float),
+                ("stretch", C.c_float), ("exposure", C.c_float), ("two_color", C.c_int32),
+                ("color_low", C.c_float * 3), ("color_high", C.c_float * 3),
+                ("reserved", C.c_int32 * 4)]
+
+
 class SaveInfo(C.Structure):
     """ge_save_info (include/ge_bh.h)."""
     _fields_ = [("version", C.c_uint32), ("dims", C.c_int32), ("n", C.c_int64),
@@ -122,6 +130,9 @@ SIGNATURES = {
     "ge_download_prev_vel": ([_vp, _vp, _vp, _vp], C.c_int),
     "ge_upload_temp": ([_vp, _vp], C.c_int),
     "ge_save_read_info": ([C.c_char_p, C.POINTER(SaveInfo)], C.c_int),
+    "ge_field_params_default": ([C.POINTER(FieldParams)], None),
+    "ge_gravity_field": ([_vp, C.c_int32, C.POINTER(FieldParams), C.c_int64, _vp, _vp,
+                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "ge_save_read": ([C.c_char_p, C.c_int64] + [_vp] * 13, C.c_int),
     "ge_predict_trajectory": ([_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_float, C.c_int32,
                                _vp], C.c_int),
@@ -382,6 +393,30 @@ class Simulation:
                                                 _ptr(vel), _ptr(mass), float(eps2), int(steps),
                                                 _ptr(path)))
         return path
+
+    def gravity_field(self, sim=0, colors=True, **kw):
+        """The field view (field.h): cell strengths [amount_x, amount_y] and,
+        with colors, RGBA8 pixels [amount_x, amount_y, 4]."""
+        fp = FieldParams()
+        lib().ge_field_params_default(C.byref(fp))
+        for k, v in kw.items():
+            if k in ("color_low", "color_high"):
+                for a in range(3):
+                    getattr(fp, k)[a] = v[a]
+            else:
+                setattr(fp, k, v)
+        ax, ay = C.c_int32(0), C.c_int32(0)
+        rc = lib().ge_gravity_field(self._h, int(sim), C.byref(fp), 0, None, None, C.byref(ax),
+                                    C.byref(ay))
+        if rc not in (0, 4):
+            self._check(rc)
+        n = ax.value * ay.value
+        st = np.zeros(n, np.float32)
+        px = np.zeros(n * 4, np.uint8) if colors else None
+        self._check(lib().ge_gravity_field(self._h, int(sim), C.byref(fp), n, _ptr(st), _ptr(px),
+                                           C.byref(ax), C.byref(ay)))
+        st = st.reshape(ax.value, ay.value)
+        return (st, px.reshape(ax.value, ay.value, 4)) if colors else st
 
     def upload_temp(self, temp):
         t = np.ascontiguousarray(temp, np.float32)

@@ -1250,6 +1250,58 @@ int ge_predict_trajectory(ge_ctx *c, int32_t sim, int32_t nprobes, const float *
     return GE_OK;
 }
 
+void ge_field_params_default(ge_field_params *fp) {
+    if (!fp) return;
+    std::memset(fp, 0, sizeof(*fp));
+    fp->res = 150;            // field.h:20
+    fp->softness = 0.85f;     // field.h:30
+    fp->threshold = 1000.0f;  // field.h:26
+    fp->stretch = 90.0f;      // field.h:433
+    fp->exposure = 3.0f;      // field.h:437
+    // colorVisuals.pColor {0, 40, 68} and sColor {155, 80, 40} (particleColorVisuals.h:25-26)
+    const float lo[3] = {0.0f, 40.0f, 68.0f}, hi[3] = {155.0f, 80.0f, 40.0f};
+    for (int a = 0; a < 3; a++) {
+        fp->color_low[a] = lo[a] / 255.0f;
+        fp->color_high[a] = hi[a] / 255.0f;
+    }
+}
+
+int ge_gravity_field(ge_ctx *c, int32_t sim, const ge_field_params *fp, int64_t cap,
+                     float *strength, uint8_t *rgba, int32_t *amount_x, int32_t *amount_y) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!fp || fp->res < 1 || !(fp->threshold > 0.0f)) return fail(c, GE_ERR_ARG, "bad field parameters");
+    if (c->p.dims != 2) return fail(c, GE_ERR_UNSUPPORTED, "the field view is 2D");
+    if (!(c->p.domain[0] > 0.0f) || !(c->p.domain[1] > 0.0f))
+        return fail(c, GE_ERR_ARG, "the field view needs a positive domain");
+    int r = 0;
+    if (sim != 0 && (r = find_sim(c, sim)) < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    // Field::initializeCells (field.h:59-80)
+    const float dx = c->p.domain[0], dy = c->p.domain[1];
+    const float cell = (dx >= dy ? dy : dx) / (float)fp->res;
+    const int ax = (int)(dx / cell), ay = (int)(dy / cell);
+    if (amount_x) *amount_x = ax;
+    if (amount_y) *amount_y = ay;
+    const int64_t cells = (int64_t)ax * ay;
+    if (cells > cap) return fail(c, GE_ERR_CAPACITY, "field arrays smaller than the cell count");
+    if (cells < 1) return GE_OK;
+    float *d = nullptr;
+    GE_CHECK(c, cudaMallocAsync((void **)&d, sizeof(float) * 2 * (size_t)cells, c->stream));
+    float *ds = d;
+    uint32_t *dc = reinterpret_cast<uint32_t *>(d + cells);
+    const uint32_t lo = c->h_off[(size_t)r], hi = c->h_off[(size_t)r + 1];
+    GE_CHECK(c, launch_field(cur_state(c), lo, hi, ax, ay, cell, c->p.G, fp->softness * fp->softness,
+                             c->p.periodic, dx, dy, *fp, ds, rgba ? dc : nullptr, c->stream));
+    if (strength)
+        GE_CHECK(c, cudaMemcpyAsync(strength, ds, sizeof(float) * (size_t)cells,
+                                    cudaMemcpyDeviceToHost, c->stream));
+    if (rgba)
+        GE_CHECK(c, cudaMemcpyAsync(rgba, dc, 4 * (size_t)cells, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaFreeAsync(d, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    return GE_OK;
+}
+
 int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
     int rc = require_state(c);
     if (rc) return rc;

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "ge_bh.h"
+
 namespace ge {
 
 // Particle state, structure-of-arrays, in Morton order.  z/vz/az are unused
@@ -198,6 +200,11 @@ cudaError_t launch_walk(int dims, int precision, const State &s, const StepParam
                         const Segs &g, const Tree &t, bool integrate_end,
                         unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
+// gravity field display: strength (and RGBA8 colour) of every cell
+cudaError_t launch_field(const State &s, uint32_t lo, uint32_t hi, int amount_x, int amount_y,
+                         float cell, float G, float soft2, int periodic, float dom_x, float dom_y,
+                         const ge_field_params &fp, float *strength, uint32_t *rgba,
+                         cudaStream_t st);
 // trajectory preview: probes stepped against the walk layout of the last
 // build, entries [begin, end) (one simulation's tree)
 cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, uint32_t begin,

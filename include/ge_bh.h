@@ -209,6 +209,33 @@ int ge_predict_trajectory(ge_ctx *ctx, int32_t sim, int32_t nprobes, const float
                           const float *vel, const float *mass, float eps2, int32_t steps,
                           float *path);
 
+/* --- gravity field display ----------------------------------------------
+ * The reference's field view (include/Physics/field.h: cells of
+ * initializeCells :59-80, compute shader fieldGravityCompute :106-160,
+ * fragment shader fieldFragmentShader :165-222), run as CUDA on the resident
+ * particles of one simulation (2D): each cell's strength
+ * sum_j G * (10 m_j) / (|p_j - corner|^2 + softness^2) (minimum image when
+ * periodic, terms with distance <= 1e-4 left out) and, when rgba is not NULL,
+ * its colour as RGBA8 (one pixel per cell; no window on this library's
+ * side).  Cells: size = min(domain) / res, amount_x x amount_y of them,
+ * index j + i * amount_y for the cell with corner (i, j) * size.  Arrays
+ * hold cap cells; GE_ERR_CAPACITY (with *amount_x, *amount_y set) when
+ * they are too small.  sim: handle, 0 = the first simulation. */
+typedef struct {
+    int32_t res;              /* Field::res (150) */
+    float softness;           /* gravityDisplaySoftness (0.85) */
+    float threshold;          /* gravityDisplayThreshold (1000) */
+    float stretch;            /* gravityStretchFactor (90) */
+    float exposure;           /* gravityExposure (3) */
+    int32_t two_color;        /* gravityCustomColors (0: HSV ramp) */
+    float color_low[3];       /* colorVisuals.pColor / 255 */
+    float color_high[3];      /* colorVisuals.sColor / 255 */
+    int32_t reserved[4];
+} ge_field_params;
+void ge_field_params_default(ge_field_params *fp);
+int ge_gravity_field(ge_ctx *ctx, int32_t sim, const ge_field_params *fp, int64_t cap,
+                     float *strength, uint8_t *rgba, int32_t *amount_x, int32_t *amount_y);
+
 /* --- scene files -------------------------------------------------------
  * Reader of the reference's save files (SaveSystem, src/UX/saveSystem.cpp:
  * 285-362; include/UX/saveSystem.h:120-290; versions 190 and 180): the YAML

@@ -946,3 +946,67 @@ void or_predict_trajectory(const or_tree *t, const float *x, const float *y, con
         }
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* gravity field display (include/Physics/field.h): cells of           */
+/* initializeCells (:59-80), the compute shader fieldGravityCompute    */
+/* (:106-160) and the fragment shader's colour map (:165-222), in      */
+/* single precision, each operation rounded on its own, GLSL round()   */
+/* taken as roundf (halves away from zero).                            */
+/* ------------------------------------------------------------------ */
+static uint32_t unorm8(float v) {
+    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+    return (uint32_t)lrintf(v * 255.0f);
+}
+
+int or_gravity_field(int64_t n, const float *x, const float *y, const float *m, float G,
+                     float dom_x, float dom_y, int periodic, int res, float softness,
+                     float threshold, float stretch, float exposure, int two_color,
+                     const float low[3], const float high[3], float *strength, uint32_t *rgba,
+                     int *amount_x, int *amount_y, int nthreads) {
+    const float cell = (dom_x >= dom_y ? dom_y : dom_x) / (float)res;
+    const int ax = (int)(dom_x / cell), ay = (int)(dom_y / cell);
+    *amount_x = ax;
+    *amount_y = ay;
+    const float soft2 = softness * softness;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int c = 0; c < ax * ay; c++) {
+        const int i = c / ay, j = c % ay;
+        const float cx = (float)i * cell, cy = (float)j * cell;
+        float force = 0.0f;
+        for (int64_t k = 0; k < n; k++) {
+            float dx = x[k] - cx, dy = y[k] - cy;
+            if (periodic) {
+                dx = dx - dom_x * roundf(dx / dom_x);
+                dy = dy - dom_y * roundf(dy / dom_y);
+            }
+            const float d2 = dx * dx + dy * dy + soft2;
+            const float dist = sqrtf(d2);
+            if (dist > 0.0001f) force = force + G * (m[k] * 10.0f) / (dist * dist);
+        }
+        if (strength) strength[c] = force;
+        if (!rgba) continue;
+        const float cl = fminf(fmaxf(force, 0.0f), threshold);
+        const float nrm = cl / threshold;
+        const float s = logf(1.0f + nrm * stretch) / logf(1.0f + stretch);
+        float col[3];
+        if (two_color) {
+            for (int a = 0; a < 3; a++) {
+                const float base = low[a] * (1.0f - s) + high[a] * s;
+                col[a] = base * s * exposure;
+            }
+        } else {
+            const float h = (1.0f - s) * 240.0f / 360.0f;
+            const float K[3] = {1.0f, 2.0f / 3.0f, 1.0f / 3.0f};
+            for (int a = 0; a < 3; a++) {
+                const float f = h + K[a];
+                const float pp = fabsf((f - floorf(f)) * 6.0f - 3.0f);
+                float t = pp - 1.0f;
+                t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+                col[a] = s * t;
+            }
+        }
+        rgba[c] = unorm8(col[0]) | (unorm8(col[1]) << 8) | (unorm8(col[2]) << 16) | (255u << 24);
+    }
+    return 0;
+}

@@ -157,6 +157,15 @@ void or_predict_trajectory(const or_tree *t, const float *x, const float *y, con
                            const float *vel, const float *mass, int32_t steps, float *path,
                            int nthreads);
 
+/* --- gravity field display (include/Physics/field.h:59-80, 106-222) -----
+ * strength [amount_x * amount_y] (index j + i * amount_y) and rgba (RGBA8,
+ * one pixel per cell) of the field view over the 2D domain. */
+int or_gravity_field(int64_t n, const float *x, const float *y, const float *m, float G,
+                     float dom_x, float dom_y, int periodic, int res, float softness,
+                     float threshold, float stretch, float exposure, int two_color,
+                     const float low[3], const float high[3], float *strength, uint32_t *rgba,
+                     int *amount_x, int *amount_y, int nthreads);
+
 /* --- leapfrog --------------------------------------------------------- */
 void or_integrate_start(int dims, int64_t n, float *x, float *y, float *z,
                         float *vx, float *vy, float *vz, const float *ax, const float *ay,

@@ -96,6 +96,10 @@ def _load(strict=True):
     lib.or_predict_trajectory.argtypes = [C.POINTER(Tree), _f32p, _f32p, _vp, C.POINTER(Params),
                                           C.c_float, C.c_int64, _f32p, _f32p, _f32p, C.c_int32,
                                           _f32p, C.c_int]
+    lib.or_gravity_field.argtypes = [C.c_int64, _f32p, _f32p, _f32p, C.c_float, C.c_float,
+                                     C.c_float, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     C.c_float, C.c_float, C.c_int, _f32p, _f32p, _vp, _vp,
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
     lib.or_walk_mixed.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
                                   C.POINTER(Params), _f64p, _f64p, _vp, _vp, C.c_int]
     lib.or_walk_group.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
@@ -265,6 +269,26 @@ def predict_trajectory(x, y, tree_holder, params, eps2, pos, vel, mass, steps, z
                                 nprobes, pos.ravel(), vel.ravel(), mass, int(steps), path,
                                 nthreads)
     return path.reshape(nprobes, steps, dims)
+
+
+def gravity_field(x, y, m, G, domain, periodic=False, res=150, softness=0.85, threshold=1000.0,
+                  stretch=90.0, exposure=3.0, two_color=False, low=(0.0, 40 / 255, 68 / 255),
+                  high=(155 / 255, 80 / 255, 40 / 255), nthreads=8):
+    """The field view (field.h): strengths [ax, ay] and RGBA8 [ax, ay, 4]."""
+    x, y, m = _f32(x), _f32(y), _f32(m)
+    dx, dy = float(domain[0]), float(domain[1])
+    cell = np.float32(min(dx, dy)) / np.float32(res)
+    ax, ay = int(np.float32(dx) / cell) + 2, int(np.float32(dy) / cell) + 2
+    st = np.zeros(ax * ay, np.float32)
+    px = np.zeros(ax * ay, np.uint32)
+    oax, oay = C.c_int(0), C.c_int(0)
+    lib().or_gravity_field(len(x), x, y, m, G, dx, dy, int(bool(periodic)), res, softness,
+                           threshold, stretch, exposure, int(bool(two_color)),
+                           np.array(low, np.float32), np.array(high, np.float32), _ptr(st),
+                           _ptr(px), C.byref(oax), C.byref(oay), nthreads)
+    n = oax.value * oay.value
+    rgba = px[:n].view(np.uint8).reshape(oax.value, oay.value, 4)
+    return st[:n].reshape(oax.value, oay.value), rgba
 
 
 def walk_mixed(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False):

@@ -62,7 +62,8 @@ def test_struct_layouts_match_c_compiler(ge, tmp_path):
         pytest.skip("no C compiler")
     structs = {"ge_params": ge.Params, "ge_stats": ge.Stats,
                "ge_server_config": ge.ServerConfig, "ge_server_stats": ge.ServerStats,
-               "ge_tune_result": ge.TuneResult, "ge_save_info": ge.SaveInfo}
+               "ge_tune_result": ge.TuneResult, "ge_save_info": ge.SaveInfo,
+               "ge_field_params": ge.FieldParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ge_bh.h"', 'int main(void) {']
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
