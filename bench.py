@@ -266,6 +266,47 @@ def bench_mixed(ge, torch, stream, st, n, flush, K=10):
                                   "p99": float(np.percentile(err, 99)), "sample": int(len(idx))}}
 
 
+def bench_plummer3d(ge, ics, torch, n=1 << 22, K=20):
+    """The mixed-precision 3D workload: a Plummer sphere of 4,194,304 particles,
+    theta 0.5, softening 0.01 (added to r^2 as the 3D walk does), dt 5e-4,
+    group walk; throughput over K steps, the median error against the FP64
+    direct sum on 32,768 sampled particles, and the drift of the total energy
+    and of the momentum over the K steps (all in FP64)."""
+    st = ics.plummer3d(n, seed=0)
+    p = ge.default_params(3, G=1.0, theta=0.5, eps2=0.01, dt=5e-4, leaf_cap=LEAF,
+                          precision=ge.PREC_MIXED, group_size=32)
+    stream = torch.cuda.Stream()
+    with ge.Simulation(p) as sim:
+        sim.set_stream(stream.cuda_stream)
+        sim.upload(st)
+        sim.step(2)
+        e0 = sim.energy_f64()
+        m0 = sim.sums_f64()
+        times = _timed_steps(torch, stream, sim, K)
+        e1 = sim.energy_f64()
+        m1 = sim.sums_f64()
+        out = sim.download()
+        idx = np.sort(np.random.Generator(np.random.PCG64(1)).choice(
+            n, size=32768, replace=False)).astype(np.uint32)
+        ref = sim.direct_sum_f64(idx)
+        err = _err([out["ax"][idx], out["ay"][idx], out["az"][idx]], ref)
+        stage = np.array(sim.profile_step())
+    p_scale = float(np.sqrt(2.0 * m0[4] * abs(m0[0])))   # M |v|, the momentum scale
+    return {"workload": f"3D Plummer sphere, N={n}, theta 0.5, softening 0.01, dt 5e-4",
+            "precision": "mixed", "group_size": 32, "value": n / (times.mean() * 1e-3),
+            "unit": UNIT, "ms_per_step": float(times.mean()),
+            "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+            "steps": K,
+            "stage_ms": {"kick_drift_bbox": stage[0], "keys": stage[1], "sort": stage[2],
+                         "permute": stage[3], "build_and_moments": stage[4], "walk": stage[5]},
+            "force_err_vs_fp64": {"median": float(np.median(err)),
+                                  "p99": float(np.percentile(err, 99)), "sample": int(len(idx))},
+            "energy": {"start": list(e0), "end": list(e1), "steps_between": K,
+                       "relative_drift": (e1[2] - e0[2]) / abs(e0[2])},
+            "momentum_drift_over_scale": float(np.sqrt((m1[1] - m0[1]) ** 2 + (m1[2] - m0[2]) ** 2
+                                                       + (m1[3] - m0[3]) ** 2)) / p_scale}
+
+
 def bench_batched(ge, ics, torch, count, K=5, Kp=2):
     """512 independent 2D disks, N log-uniform in [1024, 262144] (seed 2), theta
     0.7, softening 0.01: one context stepping all of them (batched) against one
@@ -559,6 +600,8 @@ def run_ours(args, world, rank, local):
         del flush
         torch.cuda.empty_cache()
         line["batched"] = bench_batched(ge, ics, torch, args.batch_sims)
+        torch.cuda.empty_cache()
+        line["plummer3d"] = bench_plummer3d(ge, ics, torch)
         line["serving"] = bench_serving(ge, ics, args.serve_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)

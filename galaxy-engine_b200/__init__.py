@@ -151,6 +151,7 @@ SIGNATURES = {
     "ge_export_tree": ([_vp, C.c_int64, _vp] + [_vp] * 8, C.c_int),
     "ge_direct_sum_f64": ([_vp, C.c_int64, _vp, _vp, _vp, _vp], C.c_int),
     "ge_sums_f64": ([_vp, _vp], C.c_int),
+    "ge_energy_f64": ([_vp, _vp], C.c_int),
     "ge_build_timeline": ([_vp, C.c_int32, _vp, _vp], C.c_int),
     "ge_morton_sort_2d_noalloc": ([C.c_int64, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "ge_batch_create": ([C.POINTER(Params), C.POINTER(_vp)], C.c_int),
@@ -501,6 +502,12 @@ class Simulation:
         cnt = C.c_int32(0)
         self._check(lib().ge_build_timeline(self._h, 256, _ptr(ns), C.byref(cnt)))
         return ns[: cnt.value].copy()
+
+    def energy_f64(self):
+        """(kinetic, potential, total) in FP64 (mixed mode, group walk)."""
+        out = np.zeros(3, np.float64)
+        self._check(lib().ge_energy_f64(self._h, _ptr(out)))
+        return tuple(float(v) for v in out)
 
     def sums_f64(self):
         """{kinetic energy, p_x, p_y, p_z, total mass} in FP64."""

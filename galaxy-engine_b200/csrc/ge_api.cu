@@ -1317,6 +1317,37 @@ int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
     return GE_OK;
 }
 
+int ge_energy_f64(ge_ctx *c, double *out) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!out) return fail(c, GE_ERR_ARG, "out is NULL");
+    if (!group_walk_on(c))
+        return fail(c, GE_ERR_UNSUPPORTED, "the energy pass needs the mixed mode's group walk");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    if (!c->tree_valid) {
+        if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_keys(c)) || (rc = enqueue_sort(c)) ||
+            (rc = enqueue_permute(c, true)) || (rc = enqueue_bbox(c, false)) ||
+            (rc = enqueue_build(c)))
+            return rc;
+        if ((rc = check_device(c))) return rc;
+        c->tree_valid = true;
+    }
+    double *d = nullptr;
+    GE_CHECK(c, cudaMallocAsync((void **)&d, sizeof(double) * 6, c->stream));
+    StepParams p = step_params(c);
+    GE_CHECK(c, launch_group_potential(c->p.dims, cur_state(c), p, c->g, mixed_view(c),
+                                       c->b.tree.meta + 10, c->d_err, d, c->stream));
+    GE_CHECK(c, launch_sums_f64(c->p.dims, cur_state(c), (int)c->n, d + 1, c->stream));
+    double h[6];
+    GE_CHECK(c, cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaFreeAsync(d, c->stream));
+    if ((rc = check_device(c))) return rc;
+    out[0] = h[1];
+    out[1] = -0.5 * (double)c->p.G * h[0];
+    out[2] = out[0] + out[1];
+    return GE_OK;
+}
+
 int ge_sums_f64(ge_ctx *c, double *out) {
     int rc = require_state(c);
     if (rc) return rc;

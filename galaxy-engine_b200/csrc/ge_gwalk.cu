@@ -57,20 +57,24 @@ template <int D, int PPL>
 struct GroupState {
     float x[PPL][3];
     float f[PPL][3], fc[PPL][3];   // running sums and their Kahan compensation
+    float u[PPL], uc[PPL];         // potential pass: sum of m / r terms (phi = -G u)
     uint32_t idx[PPL];
     bool act[PPL];
     unsigned long long count;
 };
 
-// accepted nodes: monopole + quadrupole of the softened kernel
-template <int D, int PPL>
+// accepted nodes: monopole + quadrupole of the softened kernel (with POT,
+// the potential instead: M / r + 1.5 (d.I.d) / r^5 - 0.5 tr(I) / r^3)
+template <int D, int PPL, bool POT = false>
 __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupState<D, PPL> &g,
                                             float eps2, bool count) {
-    float acc[PPL][3];
+    float acc[PPL][3], pu[PPL];
 #pragma unroll
-    for (int k = 0; k < PPL; k++)
+    for (int k = 0; k < PPL; k++) {
+        pu[k] = 0.0f;
 #pragma unroll
         for (int a = 0; a < 3; a++) acc[k][a] = 0.0f;
+    }
     for (int j = 0; j < nl; j++) {
         const float4 A = sm.nA[j], B = sm.nB[j];
         const float4 C = D == 3 ? sm.nC[j] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -104,6 +108,10 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
             }
             float dId = d[0] * Id[0] + d[1] * Id[1];
             if (D == 3) dId += d[2] * Id[2];
+            if (POT) {
+                pu[k] += m * inv + 1.5f * dId * inv5 - 0.5f * tr * inv3;
+                continue;
+            }
             const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
             const float ci = -3.0f * inv5;
 #pragma unroll
@@ -112,22 +120,27 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
     }
 #pragma unroll
     for (int k = 0; k < PPL; k++) {
+        if (POT) kahan_add(g.u[k], g.uc[k], pu[k]);
 #pragma unroll
-        for (int a = 0; a < D; a++) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
+        for (int a = 0; a < D; a++)
+            if (!POT) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
         if (count && g.act[k]) g.count += (unsigned long long)nl;
     }
 }
 
-// particles of opened leaves: the softened pair force, the particle itself skipped
-template <int D, int PPL>
+// particles of opened leaves: the softened pair force (with POT, m / r), the
+// particle itself skipped
+template <int D, int PPL, bool POT = false>
 __device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupState<D, PPL> &g,
                                             float eps2, bool count) {
-    float acc[PPL][3];
+    float acc[PPL][3], pu[PPL];
     uint32_t self_hits = 0;
 #pragma unroll
-    for (int k = 0; k < PPL; k++)
+    for (int k = 0; k < PPL; k++) {
+        pu[k] = 0.0f;
 #pragma unroll
         for (int a = 0; a < 3; a++) acc[k][a] = 0.0f;
+    }
     for (int j = 0; j < pl; j++) {
         const float4 P = sm.pA[j];
         const uint32_t pj = sm.pI[j];
@@ -142,6 +155,10 @@ __device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupSt
             const float inv = rsqrt_fast(rr);
             const bool self = pj == g.idx[k];
             self_hits += (self && g.act[k]) ? 1u : 0u;
+            if (POT) {
+                pu[k] += self ? 0.0f : P.w * inv;
+                continue;
+            }
             const float fm = self ? 0.0f : P.w * (inv * inv * inv);
 #pragma unroll
             for (int a = 0; a < D; a++) acc[k][a] += d[a] * fm;
@@ -149,8 +166,10 @@ __device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupSt
     }
 #pragma unroll
     for (int k = 0; k < PPL; k++) {
+        if (POT) kahan_add(g.u[k], g.uc[k], pu[k]);
 #pragma unroll
-        for (int a = 0; a < D; a++) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
+        for (int a = 0; a < D; a++)
+            if (!POT) kahan_add(g.f[k][a], g.fc[k][a], acc[k][a]);
         if (count && g.act[k]) g.count += (unsigned long long)pl;
     }
     if (count) g.count -= self_hits;
@@ -206,10 +225,10 @@ __global__ void k_make_groups(Tree t, uint32_t GS) {
     }
 }
 
-template <int D, int PPL, bool COUNT>
+template <int D, int PPL, bool COUNT, bool POT = false>
 __global__ void __launch_bounds__(kGWThreads)
 k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
-             unsigned long long *inter, uint32_t *err) {
+             unsigned long long *inter, uint32_t *err, double *epot = nullptr) {
     __shared__ GWSmem<D> smem[kGWWarps];
     GWSmem<D> &sm = smem[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31u;
@@ -241,6 +260,8 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 g.f[k][a] = 0.0f;
                 g.fc[k][a] = 0.0f;
             }
+            g.u[k] = 0.0f;
+            g.uc[k] = 0.0f;
             if (g.act[k]) {
 #pragma unroll
                 for (int a = 0; a < D; a++) {
@@ -287,7 +308,7 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
             // 1. accepted nodes into the node list
             const unsigned accb = __ballot_sync(0xffffffffu, kind == 1);
             if (nl + __popc(accb) > kGWNodes) {
-                flush_nodes<D, PPL>(sm, nl, g, eps2, COUNT);
+                flush_nodes<D, PPL, POT>(sm, nl, g, eps2, COUNT);
                 nl = 0;
                 __syncwarp();
             }
@@ -339,7 +360,7 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 // does not fit: flush, then move the first pending leaf in
                 // list-sized chunks
                 __syncwarp();
-                flush_parts<D, PPL>(sm, pl, g, eps2, COUNT);
+                flush_parts<D, PPL, POT>(sm, pl, g, eps2, COUNT);
                 __syncwarp();
                 const int L = __ffs(pend) - 1;
                 const uint32_t lb = __shfl_sync(0xffffffffu, pbeg, L);
@@ -366,9 +387,18 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
             pl = 0;
         }
         __syncwarp();
-        if (nl) flush_nodes<D, PPL>(sm, nl, g, eps2, COUNT);
-        if (pl) flush_parts<D, PPL>(sm, pl, g, eps2, COUNT);
+        if (nl) flush_nodes<D, PPL, POT>(sm, nl, g, eps2, COUNT);
+        if (pl) flush_parts<D, PPL, POT>(sm, pl, g, eps2, COUNT);
         __syncwarp();
+        if (POT) {   // potential pass: sum_i m_i u_i in FP64, nothing written to the state
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < PPL; k++)
+                if (g.act[k]) v += (double)s.m[g.idx[k]] * ((double)g.u[k] - (double)g.uc[k]);
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(epot, v);
+            continue;
+        }
         // results and the fused second half kick
 #pragma unroll
         for (int k = 0; k < PPL; k++) {
@@ -460,6 +490,31 @@ static cudaError_t gw_dims(const State &s, const StepParams &p, const Segs &g, c
     if (p.group_size >= 128) return gw_launch<D, 4, false>(s, p, g, t, ie, inter, err, st);
     if (p.group_size >= 64) return gw_launch<D, 2, false>(s, p, g, t, ie, inter, err, st);
     return gw_launch<D, 1, false>(s, p, g, t, ie, inter, err, st);
+}
+
+template <int D, int PPL>
+static cudaError_t gw_pot(const State &s, const StepParams &p, const Segs &g, const Tree &t,
+                          uint32_t *err, double *epot, cudaStream_t st) {
+    k_make_groups<<<grid_blocks(p.n), 256, 0, st>>>(t, 32u * PPL);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int blocks = (int)(t.wl_warps / kGWWarps);
+    const int64_t want = ((int64_t)p.n + kGWWarps - 1) / kGWWarps;
+    if (blocks > want) blocks = (int)want;
+    if (blocks < 1) blocks = 1;
+    k_group_walk<D, PPL, false, true><<<blocks, kGWThreads, 0, st>>>(s, p, g, t, 0, nullptr, err,
+                                                                     epot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_potential(int dims, const State &s, const StepParams &p, const Segs &g,
+                                   const Tree &t, uint32_t *counter, uint32_t *err, double *epot,
+                                   cudaStream_t st) {
+    if (!t.wl || !t.grp || t.wl_warps < (uint32_t)kGWWarps) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(epot, 0, sizeof(double), st)) != cudaSuccess) return e;
+    return dims == 2 ? gw_pot<2, 1>(s, p, g, t, err, epot, st) : gw_pot<3, 1>(s, p, g, t, err, epot, st);
 }
 
 cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, const Segs &g,

@@ -191,6 +191,12 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Se
 // GE_PREC_MIXED group walk (ge_gwalk.cu): warps walk for groups of
 // p.group_size consecutive particles of one simulation; counter = one word
 int group_walk_warps(int dims, int num_sms);
+// the group walk's potential pass: *epot = sum_i m_i u_i, phi_i = -G u_i
+// (monopole + quadrupole of the softened kernel), groups of 32; no state
+// is written
+cudaError_t launch_group_potential(int dims, const State &s, const StepParams &p, const Segs &g,
+                                   const Tree &t, uint32_t *counter, uint32_t *err, double *epot,
+                                   cudaStream_t st);
 uint32_t group_walk_stack_entries();
 cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, const Segs &g,
                               const Tree &t, bool integrate_end, unsigned long long *inter_count,

@@ -269,6 +269,14 @@ int ge_direct_sum_f64(ge_ctx *ctx, int64_t nt, const uint32_t *idx, double *ax, 
                       double *az);
 /* FP64 sums over the state: out = {kinetic energy, p_x, p_y, p_z, total mass} */
 int ge_sums_f64(ge_ctx *ctx, double *out);
+/* Energy of the current state (no counterpart in the reference):
+   out = {kinetic, potential, total}, kinetic summed in FP64 over the
+   particles, potential = 1/2 sum_i m_i phi_i with phi_i from the mixed
+   mode's group walk (monopole + quadrupole of the softened kernel, the
+   particle itself left out) summed in FP64; over all simulations of the
+   context.  Needs GE_PREC_MIXED with the group walk (group_size > 0, not
+   periodic); builds the tree when the last step's is not current. */
+int ge_energy_f64(ge_ctx *ctx, double *out);
 /* Timeline of the last tree build: device time (ns, from the first entry) at
    each of its grid-wide barriers, in order (one per level of the large-node
    phase, then the subtree phase, then the three layout steps).  Profiling aid

@@ -1010,3 +1010,24 @@ int or_gravity_field(int64_t n, const float *x, const float *y, const float *m, 
     }
     return 0;
 }
+
+
+/* FP64 potential energy by direct summation: -1/2 G sum_i sum_{j != i}
+ * m_i m_j / sqrt(|x_i - x_j|^2 + eps2) (the accuracy reference of the energy
+ * pass; not in the reference). */
+double or_potential_f64(int dims, int64_t n, const float *x, const float *y, const float *z,
+                        const float *m, double G, double eps2, int nthreads) {
+    double e = 0.0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : e) num_threads(nthreads)
+    for (int64_t i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int64_t j = 0; j < n; j++) {
+            if (j == i) continue;
+            const double dx = (double)x[j] - x[i], dy = (double)y[j] - y[i];
+            const double dz = dims == 3 ? (double)z[j] - z[i] : 0.0;
+            s += (double)m[j] / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+        }
+        e += (double)m[i] * s;
+    }
+    return -0.5 * G * e;
+}

@@ -166,6 +166,10 @@ int or_gravity_field(int64_t n, const float *x, const float *y, const float *m, 
                      const float low[3], const float high[3], float *strength, uint32_t *rgba,
                      int *amount_x, int *amount_y, int nthreads);
 
+/* FP64 potential energy by direct summation (energy pass reference) */
+double or_potential_f64(int dims, int64_t n, const float *x, const float *y, const float *z,
+                        const float *m, double G, double eps2, int nthreads);
+
 /* --- leapfrog --------------------------------------------------------- */
 void or_integrate_start(int dims, int64_t n, float *x, float *y, float *z,
                         float *vx, float *vy, float *vz, const float *ax, const float *ay,

@@ -100,6 +100,9 @@ def _load(strict=True):
                                      C.c_float, C.c_int, C.c_int, C.c_float, C.c_float,
                                      C.c_float, C.c_float, C.c_int, _f32p, _f32p, _vp, _vp,
                                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
+    lib.or_potential_f64.argtypes = [C.c_int, C.c_int64, _f32p, _f32p, _vp, _f32p, C.c_double,
+                                     C.c_double, C.c_int]
+    lib.or_potential_f64.restype = C.c_double
     lib.or_walk_mixed.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
                                   C.POINTER(Params), _f64p, _f64p, _vp, _vp, C.c_int]
     lib.or_walk_group.argtypes = [C.c_int64, _f32p, _f32p, _vp, _f32p, C.POINTER(Tree),
@@ -289,6 +292,13 @@ def gravity_field(x, y, m, G, domain, periodic=False, res=150, softness=0.85, th
     n = oax.value * oay.value
     rgba = px[:n].view(np.uint8).reshape(oax.value, oay.value, 4)
     return st[:n].reshape(oax.value, oay.value), rgba
+
+
+def potential_f64(x, y, m, G, eps2, z=None, nthreads=8):
+    """FP64 direct-sum potential energy."""
+    zz = None if z is None else _f32(z)
+    return lib().or_potential_f64(2 if z is None else 3, len(x), _f32(x), _f32(y), _ptr(zz),
+                                  _f32(m), G, eps2, nthreads)
 
 
 def walk_mixed(x, y, m, tree_holder, params, z=None, nthreads=8, want_counts=False):

@@ -203,3 +203,21 @@ def test_autotune_refused_outside_mixed(ge, ics):
         with pytest.raises(ge.GeError) as ei:
             s.autotune()
         assert ei.value.code == 5
+
+
+@pytest.mark.parametrize("dims,n,theta,eps2", [(2, 12000, 0.7, 1e-4), (3, 8192, 0.5, 0.01)])
+def test_energy_pass_against_direct_sum(ge, ics, O, dims, n, theta, eps2):
+    """Potential energy from the group walk's potential pass against the FP64
+    direct sum; kinetic energy against the FP64 sums of the state."""
+    st = ics.disk2d(n, seed=6) if dims == 2 else ics.plummer3d(n, seed=6)
+    p = ge.default_params(dims, G=1.0, theta=theta, eps2=eps2, dt=1e-3, precision=MIXED)
+    with ge.Simulation(p) as s:
+        s.upload(st)
+        s.step(2)
+        kin, pot, tot = s.energy_f64()
+        sums = s.sums_f64()
+        out = s.download()
+    ref = O.potential_f64(out["x"], out["y"], out["m"], 1.0, eps2, z=out.get("z"))
+    assert abs(pot - ref) <= 2e-4 * abs(ref)
+    # FP64 atomic sums: equal up to the order of their additions
+    assert abs(kin - sums[0]) <= 1e-12 * abs(sums[0]) and tot == kin + pot
