@@ -53,7 +53,7 @@ class Params(C.Structure):
         ("size_gate", C.c_float), ("min_size", C.c_float), ("node_cap_factor", C.c_float),
         ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
         ("group_size", C.c_int32), ("temp_enabled", C.c_int32), ("heat_cond", C.c_float),
-        ("reserved", C.c_int32 * 4),
+        ("direct_below", C.c_int32), ("direct_eps2", C.c_float), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -203,12 +203,14 @@ def lib():
 
 def default_params(dims=2, **kw):
     """ge_params_default, then keyword overrides (softening= sets eps2 the
-    way the reference walk uses it: squared in 2D, as-is in 3D)."""
+    way the reference walk uses it: squared in 2D, as-is in 3D; and
+    direct_eps2 the way its direct sum does: as-is in both)."""
     p = Params()
     lib().ge_params_default(C.byref(p), dims)
     soft = kw.pop("softening", None)
     if soft is not None:
         p.eps2 = soft * soft if dims == 2 else soft
+        p.direct_eps2 = soft
     for k, v in kw.items():
         if k == "domain":
             for a in range(3):

@@ -62,6 +62,9 @@ struct SegBuffers {
     float4 *box = nullptr;
     uint32_t *boxmm = nullptr, *root_begin = nullptr, *root_end = nullptr;
     uint32_t *hist = nullptr, *status = nullptr;
+    uint2 *dtiles = nullptr;    // direct sum: {segment, first particle} of each tile
+    uint8_t *dflag = nullptr;   // direct sum: 1 for a segment that skips the walk
+    int64_t dtile_cap = 0;
     AllocList allocs;
 };
 
@@ -119,6 +122,11 @@ struct ge_ctx {
     int64_t total_steps = 0;
     int32_t pending_steps = 0;    // steps enqueued by ge_step_async, not yet waited for
     std::vector<uint32_t> h_off, h_tile_base;
+    // direct sum (params.direct_below): its tiles, and whether some segment
+    // takes the direct sum / the walk
+    std::vector<uint2> h_dtiles;
+    std::vector<uint8_t> h_dflag;
+    bool any_direct = false, any_walk = true;
     uint32_t *d_err = nullptr;
     uint32_t *h_meta = nullptr;   // pinned copy of the tree meta words
     int64_t slots = 0;            // node slots of the last build (holes included)
@@ -179,6 +187,7 @@ StepParams step_params(const ge_ctx *c) {
     s.periodic = c->p.periodic ? 1 : 0;
     s.group_size = c->p.group_size;
     s.heat_cond = c->p.heat_cond;
+    s.direct_eps2 = c->p.direct_eps2;
     for (int a = 0; a < 3; a++) {
         s.domain[a] = c->p.domain[a];
         s.half_domain[a] = c->p.domain[a] * 0.5f;
@@ -198,6 +207,11 @@ int validate(ge_ctx *c, const ge_params *p) {
     if (!(p->node_cap_factor >= 1.0f)) return fail(c, GE_ERR_ARG, "node_cap_factor must be >= 1");
     if (p->temp_enabled && p->precision == GE_PREC_MIXED)
         return fail(c, GE_ERR_UNSUPPORTED, "heat exchange runs in GE_PREC_EXACT and GE_PREC_FAST");
+    if (p->direct_below < 0) return fail(c, GE_ERR_ARG, "direct_below must be >= 0");
+    if (p->direct_below > 0 && p->precision == GE_PREC_MIXED)
+        return fail(c, GE_ERR_UNSUPPORTED, "the direct sum runs in GE_PREC_EXACT and GE_PREC_FAST");
+    if (p->direct_below > 0 && !(p->direct_eps2 > 0.0f && p->direct_eps2 < INFINITY))
+        return fail(c, GE_ERR_ARG, "direct_eps2 must be positive and finite (the self term divides by it)");
     if (p->group_size != 0 && p->group_size != 32 && p->group_size != 64 && p->group_size != 128)
         return fail(c, GE_ERR_ARG, "group_size must be 0, 32, 64 or 128");
     if (p->periodic && (!(p->domain[0] > 0) || !(p->domain[1] > 0) ||
@@ -456,12 +470,50 @@ int alloc_segs(ge_ctx *c, SegBuffers &nb, int64_t seg_cap, int64_t n_cap, int64_
     GE_CHECK(c, dalloc(L, &nb.root_end, SC));
     GE_CHECK(c, dalloc(L, &nb.hist, (size_t)kMaxPasses * SC * 256));
     GE_CHECK(c, dalloc(L, &nb.status, (size_t)kMaxPasses * TC * 256));
+    nb.dtile_cap = nb.n_cap / kDirectTile + nb.seg_cap + 1;
+    GE_CHECK(c, dalloc(L, &nb.dtiles, (size_t)nb.dtile_cap));
+    GE_CHECK(c, dalloc(L, &nb.dflag, SC));
     if (!L.dry) {
         Segs all{};
         all.S = (int)nb.seg_cap;
         all.boxmm = nb.boxmm;
         GE_CHECK(c, launch_reset_boxes(all, c->stream));
     }
+    return GE_OK;
+}
+
+// Which simulations take the direct sum (fewer than params.direct_below
+// particles), the direct sum's tiles of kDirectTile particles over them, and
+// the per-segment flag the walk skips them by (bound to c->g only when both
+// kinds are present).
+int direct_tables(ge_ctx *c) {
+    const int64_t S = (int64_t)c->sims.size();
+    c->h_dtiles.clear();
+    c->h_dflag.assign((size_t)std::max<int64_t>(S, 1), 0u);
+    c->any_direct = false;
+    c->any_walk = S == 0;
+    for (int64_t s = 0; s < S; s++) {
+        const int64_t ns = c->sims[s].n;
+        if (ns < (int64_t)c->p.direct_below) {
+            c->h_dflag[s] = 1u;
+            c->any_direct = true;
+            for (int64_t o = 0; o < ns; o += kDirectTile)
+                c->h_dtiles.push_back(make_uint2((uint32_t)s, c->h_off[s] + (uint32_t)o));
+        } else {
+            c->any_walk = true;
+        }
+    }
+    c->g.direct = nullptr;
+    if (!c->any_direct) return GE_OK;
+    SegBuffers &sb = c->sb;
+    if ((int64_t)c->h_dtiles.size() > sb.dtile_cap || S > sb.seg_cap)
+        return fail(c, GE_ERR_STATE, "direct-sum tables exceed their capacity");
+    GE_CHECK(c, cudaMemcpyAsync(sb.dtiles, c->h_dtiles.data(), sizeof(uint2) * c->h_dtiles.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(sb.dflag, c->h_dflag.data(), (size_t)S, cudaMemcpyHostToDevice,
+                                c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));   // the host tables are reused
+    if (c->any_walk) c->g.direct = sb.dflag;
     return GE_OK;
 }
 
@@ -521,7 +573,7 @@ int sync_segments(ge_ctx *c) {
     c->b.ss.box_blocks = (int)bb;
     c->tree_valid = false;
     c->keys_valid = false;
-    return GE_OK;
+    return direct_tables(c);
 }
 
 // Reads back the error word and tree size; clears the error word.
@@ -625,6 +677,10 @@ int enqueue_walk(ge_ctx *c, bool integrate_end) {
         return GE_OK;
     }
     State s = cur_state(c);
+    if (c->any_direct)
+        GE_CHECK(c, launch_direct(c->p.dims, c->p.precision, s, p, c->g, c->sb.dtiles,
+                                  (int64_t)c->h_dtiles.size(), integrate_end, c->stream));
+    if (!c->any_walk) return GE_OK;
     if (!c->p.temp_enabled) s.temp = nullptr;
     GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, s, p, c->g, mixed_view(c), integrate_end,
                             cnt, c->d_err, c->stream));
@@ -762,6 +818,7 @@ void ge_params_default(ge_params *p, int dims) {
     p->domain[2] = 1300.0f;
     p->group_size = 32;
     p->heat_cond = 0.045f;      // globalHeatConductivity (parameters.h:120)
+    p->direct_eps2 = 1.5f;      // softening, added un-squared by naiveGravity
 }
 
 int ge_create(const ge_params *p, ge_ctx **out) {
@@ -823,7 +880,12 @@ int ge_set_params(ge_ctx *c, const ge_params *p) {
                                         (p->track_prev_vel != 0) != c->b.prev);
     if (realloc) return fail(c, GE_ERR_STATE, "node_cap_factor / track_prev_vel change needs a new upload");
     const bool to_mixed = p->precision == GE_PREC_MIXED && c->p.precision != GE_PREC_MIXED;
+    const bool new_direct = p->direct_below != c->p.direct_below;
     c->p = *p;
+    if (new_direct && c->sb.seg_cap) {
+        rc = direct_tables(c);
+        if (rc) return rc;
+    }
     if (to_mixed && c->b.mixed) {
         // the compensation terms were not carried in the other modes: restart them
         for (int k = 0; k < 2; k++) {

@@ -118,6 +118,8 @@ struct Segs {
     uint32_t *boxmm;            // [S * 6] order-preserving min/max words
     uint32_t *root_begin;       // [S] walk entry of each root
     uint32_t *root_end;         // [S] end of each root's walk
+    const uint8_t *direct;      // [S] 1: the segment takes the direct sum and the
+                                // walk skips it (nullptr: every segment walks)
 };
 
 __host__ __device__ __forceinline__ uint32_t seg_lo(const Segs &g, uint32_t s) {
@@ -147,11 +149,13 @@ struct StepParams {
     float domain[3], half_domain[3];
     int group_size;   // GE_PREC_MIXED: 0 = per-particle walk, else the group walk
     float heat_cond;  // heat exchange coefficient (used when State::temp is set)
+    float direct_eps2;   // value the direct sum adds to r^2
 };
 
 constexpr int kBBoxThreads = 256;
 constexpr int kSortTile = 4096;   // keys per look-back tile (256 threads x 16)
 constexpr int kTimeline = 256;    // build timeline entries
+constexpr int kDirectTile = 128;  // particles per block of the direct sum
 
 // --- launchers (each runs on `st`) ----------------------------------------
 // integrateStart (kick + drift) fused with the per-segment bounding-box
@@ -201,6 +205,12 @@ uint32_t group_walk_stack_entries();
 cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, const Segs &g,
                               const Tree &t, bool integrate_end, unsigned long long *inter_count,
                               uint32_t *counter, uint32_t *err, cudaStream_t st);
+// O(N^2) direct sum of the segments listed by tiles[ntiles] ({segment,
+// first particle}, kDirectTile particles each, inside one segment), fused
+// with integrateEnd like the walk
+cudaError_t launch_direct(int dims, int precision, const State &s, const StepParams &p,
+                          const Segs &g, const uint2 *tiles, int64_t ntiles, bool integrate_end,
+                          cudaStream_t st);
 // tree walk; integrate_end fuses integrateEnd (v += a*dt/2)
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
                         const Segs &g, const Tree &t, bool integrate_end,

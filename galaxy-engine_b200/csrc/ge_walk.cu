@@ -28,7 +28,8 @@
 //                   (ge_moments.cu): opening radius instead of size, the
 //                   double-float centre of mass, a quadrupole term, and
 //                   Kahan-compensated sums of the acceleration terms.
-// integrateEnd (physics.cpp:1114-1125) is fused into the epilogue.
+// integrateEnd (physics.cpp:1114-1125) is fused into the epilogue.  A
+// simulation below params.direct_below is skipped here (ge_direct.cu).
 #include "ge_bh.h"
 #include "ge_device.cuh"
 #include "ge_internal.h"
@@ -72,7 +73,9 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
-    if (i < n) {
+    // particles of simulations that take the direct sum are left to it
+    const bool walks = i < n && !(g.direct && __ldg(&g.direct[g.seg_of ? __ldg(&g.seg_of[i]) : 0u]));
+    if (walks) {
         float pi[3];
         pi[0] = s.x[i]; pi[1] = s.y[i];
         pi[2] = D == 3 ? s.z[i] : 0.0f;

@@ -77,7 +77,16 @@ typedef struct {
     int32_t temp_enabled;    /* heat exchange in the walk (myVar.isTempEnabled, default off;
                                 GE_PREC_EXACT / GE_PREC_FAST); temperatures via ge_upload_temp */
     float heat_cond;         /* myVar.globalHeatConductivity (parameters.h:120) */
-    int32_t reserved[4];
+    int32_t direct_below;    /* a simulation of fewer particles takes its accelerations
+                                from the O(N^2) direct sum instead of the walk, as the
+                                application does below 5000 (globalLogic.cpp:1321-1346,
+                                3D :1677-1702; naiveGravity physics.cpp:392-434, 3D
+                                physics3D.cpp:416-469); 0 = always walk, INT32_MAX =
+                                always direct (myVar.naive); no heat exchange there;
+                                GE_PREC_EXACT / GE_PREC_FAST */
+    float direct_eps2;       /* value the direct sum adds to r^2: softening, un-squared
+                                in 2D and 3D (physics.cpp:422, physics3D.cpp:455) */
+    int32_t reserved[2];
 } ge_params;
 
 typedef struct {
@@ -97,7 +106,8 @@ typedef struct ge_ctx ge_ctx;
 
 /* --- lifecycle -------------------------------------------------------- */
 /* Fills the reference defaults: theta 0.8, softening 1.5 (eps2 = 2.25 in 2D,
-   1.5 in 3D), dt 0.045, G 6.674e-11, leaf_cap 4, size_gate 2, min_size 1e-6. */
+   1.5 in 3D, direct_eps2 = 1.5), dt 0.045, G 6.674e-11, leaf_cap 4, size_gate 2,
+   min_size 1e-6; direct_below 0 (the application's own dispatch is 5000). */
 void ge_params_default(ge_params *p, int dims);
 int ge_create(const ge_params *p, ge_ctx **out);
 int ge_destroy(ge_ctx *ctx);

@@ -661,8 +661,9 @@ void or_walk3d_avx2(int64_t n, const float *x, const float *y, const float *z, c
 }
 
 /* ------------------------------------------------------------------ */
-/* direct sum: physics.cpp:392-434 (scalar form; softening un-squared,  */
-/* self term included since dx = dy = 0 contributes nothing)            */
+/* direct sum: physics.cpp:392-434, 3D physics3D.cpp:416-469 (scalar   */
+/* form; softening un-squared, self term included since d = 0 adds      */
+/* nothing; the result is the acceleration, no heat exchange)           */
 /* ------------------------------------------------------------------ */
 void or_naive2d(int64_t n, const float *x, const float *y, const float *m,
                 const or_params *p, float *ax, float *ay, int nthreads) {
@@ -697,6 +698,11 @@ void or_naive3d(int64_t n, const float *x, const float *y, const float *z, const
         const float xi = x[i], yi = y[i], zi = z[i];
         for (int64_t j = 0; j < n; j++) {
             float dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
+            if (p->periodic) {   /* physics3D.cpp:449-453 */
+                dx = wrap_d(dx, p->domain[0], p->domain[0] * 0.5f);
+                dy = wrap_d(dy, p->domain[1], p->domain[1] * 0.5f);
+                dz = wrap_d(dz, p->domain[2], p->domain[2] * 0.5f);
+            }
             float r2 = dx * dx + dy * dy + dz * dz + soft;
             float inv = 1.0f / sqrtf(r2);
             float f = G * m[j] * (inv * inv * inv);
@@ -834,7 +840,7 @@ int or_frame(const or_params *p, int64_t n, float *x, float *y, float *z,
     double t5 = now_ms();
     uint32_t *inter = interactions ? (uint32_t *)malloc(sizeof(uint32_t) * (size_t)n) : NULL;
     for (int64_t i = 0; i < n; i++) { ax[i] = 0.0f; ay[i] = 0.0f; if (d3) az[i] = 0.0f; }
-    if (walk == 2 && n < 5000) {
+    if ((walk == 2 && n < 5000) || (walk == 0 && n < (int64_t)p->direct_below)) {
         if (d3) or_naive3d(n, x, y, z, m, p, ax, ay, az, nthreads);
         else or_naive2d(n, x, y, m, p, ax, ay, nthreads);
     } else if (walk >= 1) {

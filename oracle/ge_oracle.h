@@ -56,6 +56,7 @@ typedef struct {
     int   temp_enabled;    /* isTempEnabled */
     float heat_cond;       /* globalHeatConductivity */
     float naive_soft;      /* softening added un-squared by the direct-sum path */
+    int   direct_below;    /* scalar frame (walk 0): direct sum below this many particles */
 } or_params;
 
 typedef struct {
@@ -183,8 +184,9 @@ void or_integrate_end(int dims, int64_t n, float *vx, float *vy, float *vz,
  * State arrays are in the current particle order and are permuted into
  * Morton order, exactly as the application's particle vectors are.  z, vz,
  * az, pvz are ignored in 2D; pvx..pvz, temp, pinned may be NULL.
- * walk: 0 = scalar tree walk, 1 = AVX2 tree walk, 2 = application dispatch
- * (direct sum below 5000 particles, AVX2 walk otherwise).
+ * walk: 0 = scalar tree walk (scalar direct sum below p->direct_below
+ * particles), 1 = AVX2 tree walk, 2 = application dispatch (direct sum below
+ * 5000 particles, AVX2 walk otherwise).
  * stage_ms (optional, [8]): integrateStart, bbox, keys, sort+gather, build,
  * walk, integrateEnd, total.  Returns 0, or -1 on allocation failure. */
 int or_frame(const or_params *p, int64_t n, float *x, float *y, float *z,

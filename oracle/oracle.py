@@ -32,12 +32,13 @@ class Params(C.Structure):
         ("dt", C.c_float), ("leaf_cap", C.c_uint32), ("size_gate", C.c_float),
         ("min_size", C.c_float), ("periodic", C.c_int), ("domain", C.c_float * 3),
         ("temp_enabled", C.c_int), ("heat_cond", C.c_float), ("naive_soft", C.c_float),
+        ("direct_below", C.c_int),
     ]
 
 
 def make_params(dims=2, G=1.0, theta=0.7, eps2=1e-4, dt=1e-3, leaf_cap=4, size_gate=2.0,
                 min_size=1e-6, periodic=False, domain=(0.0, 0.0, 0.0), temp_enabled=False,
-                heat_cond=0.045, naive_soft=None):
+                heat_cond=0.045, naive_soft=None, direct_below=0):
     p = Params()
     p.dims, p.G, p.theta, p.eps2, p.dt = dims, G, theta, eps2, dt
     p.leaf_cap, p.size_gate, p.min_size = leaf_cap, size_gate, min_size
@@ -46,6 +47,7 @@ def make_params(dims=2, G=1.0, theta=0.7, eps2=1e-4, dt=1e-3, leaf_cap=4, size_g
         p.domain[a] = domain[a]
     p.temp_enabled, p.heat_cond = int(bool(temp_enabled)), heat_cond
     p.naive_soft = eps2 if naive_soft is None else naive_soft
+    p.direct_below = int(direct_below)
     return p
 
 

@@ -41,14 +41,16 @@ def test_abi_version_and_defaults(ge):
     assert p.leaf_cap == 4 and p.size_gate == 2.0 and abs(p.dt - 0.045) < 1e-7
     p3 = ge.default_params(3)
     assert abs(p3.eps2 - 1.5) < 1e-6 and p3.node_cap_factor == 8.0
+    assert p3.direct_below == 0 and abs(p3.direct_eps2 - 1.5) < 1e-6
     p = ge.default_params(2, softening=0.01, theta=0.7)
     assert abs(p.eps2 - 1e-4) < 1e-10 and abs(p.theta - 0.7) < 1e-7
+    assert abs(p.direct_eps2 - 0.01) < 1e-9   # the direct sum adds softening un-squared
 
 
 def test_struct_layouts_match_header(ge):
     # ge_params: 11 scalars + domain[3] + track_prev_vel, group_size, temp_enabled,
-    # heat_cond + reserved[4]
-    assert C.sizeof(ge.Params) == 4 * (11 + 3 + 1 + 1 + 2 + 4)
+    # heat_cond, direct_below, direct_eps2 + reserved[2]
+    assert C.sizeof(ge.Params) == 4 * (11 + 3 + 1 + 1 + 2 + 2 + 2)
     # ge_stats: 84 bytes of fields, padded to the 8-byte alignment of its int64 members
     assert C.sizeof(ge.Stats) == 88
 
