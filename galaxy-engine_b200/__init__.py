@@ -134,6 +134,7 @@ SIGNATURES = {
     "ge_gravity_field": ([_vp, C.c_int32, C.POINTER(FieldParams), C.c_int64, _vp, _vp,
                           C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
     "ge_save_read": ([C.c_char_p, C.c_int64] + [_vp] * 13, C.c_int),
+    "ge_sph_grid": ([_vp, C.c_int32, C.c_float, C.c_uint32, C.c_int64] + [_vp] * 5, C.c_int),
     "ge_predict_trajectory": ([_vp, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_float, C.c_int32,
                                _vp], C.c_int),
     "ge_download_temp": ([_vp, _vp], C.c_int),
@@ -420,6 +421,24 @@ class Simulation:
                                            C.byref(ax), C.byref(ay)))
         st = st.reshape(ax.value, ay.value)
         return (st, px.reshape(ax.value, ay.value, 4)) if colors else st
+
+    def sph_grid(self, cell_size=3.0, table_size=16384, sim=0):
+        """SPH neighbour grid (SPH::newGridGPU): entries sorted by hashed
+        cell key (keys, index, cell_x, cell_y, one per particle of the
+        simulation) and offsets[table_size] (first entry of each key,
+        0xFFFFFFFF for none)."""
+        n = self.query(sim)[0] if sim else self._first_n()
+        out = {k: np.empty(n, np.uint32) for k in ("keys", "index")}
+        out.update({k: np.empty(n, np.int32) for k in ("cell_x", "cell_y")})
+        out["offsets"] = np.empty(int(table_size), np.uint32)
+        self._check(lib().ge_sph_grid(self._h, int(sim), float(cell_size), int(table_size), n,
+                                      *(_ptr(out[k]) for k in ("keys", "index", "cell_x",
+                                                                "cell_y", "offsets"))))
+        return out
+
+    def _first_n(self):
+        hs = self.sims()
+        return self.query(hs[0])[0] if hs else self.n
 
     def upload_temp(self, temp):
         t = np.ascontiguousarray(temp, np.float32)

@@ -1364,6 +1364,43 @@ int ge_gravity_field(ge_ctx *c, int32_t sim, const ge_field_params *fp, int64_t 
     return GE_OK;
 }
 
+int ge_sph_grid(ge_ctx *c, int32_t sim, float cell_size, uint32_t table_size, int64_t cap,
+                uint32_t *keys, uint32_t *index, int32_t *cell_x, int32_t *cell_y,
+                uint32_t *offsets) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (c->p.dims != 2) return fail(c, GE_ERR_UNSUPPORTED, "the SPH grid is 2D");
+    if (!(cell_size > 0.0f && cell_size < INFINITY))
+        return fail(c, GE_ERR_ARG, "cell_size must be positive and finite");
+    if (table_size < 1u || table_size > (1u << 24))
+        return fail(c, GE_ERR_ARG, "table_size must be in [1, 2^24]");
+    if (!keys || !index || !cell_x || !cell_y || !offsets)
+        return fail(c, GE_ERR_ARG, "every output array is required");
+    int r = 0;
+    if (sim != 0 && (r = find_sim(c, sim)) < 0) return fail(c, GE_ERR_ARG, "no such simulation");
+    const uint32_t lo = c->h_off[(size_t)r], hi = c->h_off[(size_t)r + 1];
+    const int64_t n = (int64_t)hi - lo;
+    if (n > cap) return fail(c, GE_ERR_CAPACITY, "output arrays smaller than the simulation");
+    if (n >= (int64_t(1) << 28)) return fail(c, GE_ERR_CAPACITY, "more than 2^28 particles");
+    if (n < 1) return GE_OK;
+    const size_t words = 4 * (size_t)n + table_size;
+    uint32_t *d = nullptr;
+    GE_CHECK(c, cudaMallocAsync((void **)&d, sizeof(uint32_t) * words, c->stream));
+    uint32_t *dk = d, *di = d + n, *dofs = d + 4 * n;
+    int32_t *dx = reinterpret_cast<int32_t *>(d + 2 * n), *dy = reinterpret_cast<int32_t *>(d + 3 * n);
+    c->keys_valid = false;   // the Morton sort scratch is reused
+    GE_CHECK(c, launch_sph_grid(cur_state(c), lo, (int)n, cell_size, table_size, c->b.ss, c->d_err,
+                                dk, di, dx, dy, dofs, c->num_sms, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(keys, dk, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(index, di, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(cell_x, dx, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(cell_y, dy, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    GE_CHECK(c, cudaMemcpyAsync(offsets, dofs, 4 * (size_t)table_size, cudaMemcpyDeviceToHost,
+                                c->stream));
+    GE_CHECK(c, cudaFreeAsync(d, c->stream));
+    return check_device(c);
+}
+
 int ge_build_timeline(ge_ctx *c, int32_t cap, uint64_t *ns, int32_t *count) {
     int rc = require_state(c);
     if (rc) return rc;

@@ -179,6 +179,19 @@ cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScra
 // ss.keys[0] (and vals[0])
 cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_t *err,
                         cudaStream_t st);
+// stable radix passes over bits [shift0, shift0 + 8 * passes) of the 64-bit
+// words in words[0] (one range, no segments); digit histograms in hist
+// [passes][256]; *result = the buffer that holds the sorted words
+cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int passes,
+                               const uint32_t *hist, uint32_t *status, uint32_t *tile_ctr,
+                               uint32_t *err, int *result, cudaStream_t st);
+// SPH neighbour grid of particles [lo, lo + n) (ge_sph.cu); outputs are device
+// arrays keys/index/cell_x/cell_y [n], offsets [table]
+int sph_grid_passes(uint32_t table);
+cudaError_t launch_sph_grid(const State &s, uint32_t lo, int n, float cell, uint32_t table,
+                            SortScratch &ss, uint32_t *err, uint32_t *keys, uint32_t *index,
+                            int32_t *cell_x, int32_t *cell_y, uint32_t *offsets, int num_sms,
+                            cudaStream_t st);
 // gather of the state into `out` by the sorted order
 cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
                            const State &out, bool with_acc, cudaStream_t st);

@@ -317,6 +317,24 @@ cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_
     return cudaSuccess;
 }
 
+cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int passes,
+                               const uint32_t *hist, uint32_t *status, uint32_t *tile_ctr,
+                               uint32_t *err, int *result, cudaStream_t st) {
+    const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+    const Segs one{};   // a single range [0, n)
+    int cur = 0;
+    for (int ps = 0; ps < passes; ps++) {
+        k_radix_pass<false><<<(unsigned)(tiles < 1 ? 1 : tiles), kSortThreads, 0, st>>>(
+            words[cur], words[cur ^ 1], nullptr, nullptr, n, shift0 + 8 * ps, one,
+            hist + (size_t)ps * kRadix, status + ps * tiles * kRadix, tile_ctr + ps, err);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        cur ^= 1;
+    }
+    *result = cur;
+    return cudaSuccess;
+}
+
 cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
                            const State &out, bool with_acc, cudaStream_t st) {
     int blocks = grid_for(n, 256, 148 * 16);

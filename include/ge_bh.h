@@ -246,6 +246,22 @@ void ge_field_params_default(ge_field_params *fp);
 int ge_gravity_field(ge_ctx *ctx, int32_t sim, const ge_field_params *fp, int64_t cap,
                      float *strength, uint8_t *rgba, int32_t *amount_x, int32_t *amount_y);
 
+/* --- SPH neighbour grid (2D) -------------------------------------------
+ * Replaces SPH::newGridGPU (GalaxyEngine/include/Physics/SPH.h:533-590 with
+ * its shaders :101-152, :247-296, :369-400, :455-470).  For one simulation's
+ * particles in their current order (sim 0 = the first or only one):
+ * cell (cx, cy) = floor(position / cell_size); key = (uint32(cx * 73856093) ^
+ * uint32(cy * 19349663)) % table_size with wrapping 32-bit products; the
+ * entries {key, particle, cx, cy} sorted by key (stable: a key's particles in
+ * increasing order; the reference's bitonic network leaves ties in an order
+ * of its own); offsets[key] = the key's first entry, UINT32_MAX for a key no
+ * particle has.  keys/index/cell_x/cell_y hold n entries (cap >= n), offsets
+ * table_size entries.  The reference uses hashTableSize 16384 and cellSize =
+ * radiusMultiplier = 3 (SPH.h:16,28,97).  table_size in [1, 2^24]. */
+int ge_sph_grid(ge_ctx *ctx, int32_t sim, float cell_size, uint32_t table_size, int64_t cap,
+                uint32_t *keys, uint32_t *index, int32_t *cell_x, int32_t *cell_y,
+                uint32_t *offsets);
+
 /* --- scene files -------------------------------------------------------
  * Reader of the reference's save files (SaveSystem, src/UX/saveSystem.cpp:
  * 285-362; include/UX/saveSystem.h:120-290; versions 190 and 180): the YAML

@@ -869,6 +869,63 @@ int or_frame(const or_params *p, int64_t n, float *x, float *y, float *z,
 }
 
 /* ------------------------------------------------------------------ */
+/* SPH neighbour grid: SPH::newGridGPU (SPH.h:533-590)                  */
+/* ------------------------------------------------------------------ */
+/* int(floor(v)) of the shader; out of the int range (undefined there)  */
+/* it saturates, NaN gives 0                                            */
+static int32_t floor_to_i32(float v) {
+    if (v != v) return 0;
+    const double f = floor((double)v);
+    if (f >= 2147483647.0) return INT32_MAX;
+    if (f <= -2147483648.0) return INT32_MIN;
+    return (int32_t)f;
+}
+
+void or_sph_grid(int64_t n, const float *x, const float *y, float cell, uint32_t table,
+                 uint32_t *keys, uint32_t *index, int32_t *cell_x, int32_t *cell_y,
+                 uint32_t *offsets) {
+    /* neighborSearchCompute (:130-151): posToCellCoord, hashCell; the int
+       products wrap modulo 2^32 */
+    for (int64_t i = 0; i < n; i++) {
+        const int32_t cx = floor_to_i32(x[i] / cell), cy = floor_to_i32(y[i] / cell);
+        keys[i] = (((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u)) % table;
+        index[i] = (uint32_t)i;
+        cell_x[i] = cx;
+        cell_y[i] = cy;
+    }
+    /* gpuBitonicSort (:337-367) with bitonicSortCompute (:272-295): stages
+       over the next power of two; a compare-exchange whose right index is
+       past the end is skipped */
+    uint32_t p2 = 1;
+    while (p2 < (uint64_t)n) p2 <<= 1;
+    int stages = 0;
+    while ((1u << stages) < p2) stages++;
+    for (int stage = 0; stage < stages; stage++) {
+        for (int step = 0; step <= stage; step++) {
+            const uint32_t gw = 1u << (stage - step), gh = 2 * gw - 1;
+            for (uint32_t t = 0; t < p2 / 2; t++) {
+                const uint32_t h = t & (gw - 1);
+                const uint32_t l = h + (gh + 1) * (t / gw);
+                const uint32_t r = l + (step == 0 ? gh - 2 * h : (gh + 1) / 2);
+                if (r >= (uint64_t)n) continue;
+                if (keys[l] > keys[r]) {
+                    uint32_t tk = keys[l]; keys[l] = keys[r]; keys[r] = tk;
+                    uint32_t ti = index[l]; index[l] = index[r]; index[r] = ti;
+                    int32_t tx = cell_x[l]; cell_x[l] = cell_x[r]; cell_x[r] = tx;
+                    int32_t ty = cell_y[l]; cell_y[l] = cell_y[r]; cell_y[r] = ty;
+                }
+            }
+        }
+    }
+    /* offsetsResetCompute (:465-469) and offsetCompute (:386-399) */
+    for (uint32_t k = 0; k < table; k++) offsets[k] = 0xFFFFFFFFu;
+    for (int64_t i = 0; i < n; i++) {
+        const uint32_t prev = i == 0 ? table : keys[i - 1];
+        if (keys[i] != prev && keys[i] < table) offsets[keys[i]] = (uint32_t)i;
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* trajectory preview: ParticlesSpawning::predictTrajectory            */
 /* (particlesSpawning.cpp:443-500, 3D :1000-1060) with the walk it     */
 /* calls, Physics::calculateForceFromGridOld (physics.cpp:4-90, 3D     */

@@ -180,6 +180,15 @@ void or_integrate_end(int dims, int64_t n, float *vx, float *vy, float *vz,
                       const float *ax, const float *ay, const float *az,
                       const uint8_t *pinned, const or_params *p);
 
+/* SPH neighbour grid: SPH::newGridGPU (SPH.h:533-590) -- the cell-key
+ * shader (:101-152), the bitonic network as gpuBitonicSort drives it
+ * (:247-296, :337-367) and the offsets shaders (:369-400, :455-470).
+ * Outputs keys/index/cell_x/cell_y [n] in the network's order and
+ * offsets [table]. */
+void or_sph_grid(int64_t n, const float *x, const float *y, float cell, uint32_t table,
+                 uint32_t *keys, uint32_t *index, int32_t *cell_x, int32_t *cell_y,
+                 uint32_t *offsets);
+
 /* --- one full frame of the gravity path -------------------------------
  * State arrays are in the current particle order and are permuted into
  * Morton order, exactly as the application's particle vectors are.  z, vz,

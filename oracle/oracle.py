@@ -102,6 +102,7 @@ def _load(strict=True):
                                      C.c_float, C.c_int, C.c_int, C.c_float, C.c_float,
                                      C.c_float, C.c_float, C.c_int, _f32p, _f32p, _vp, _vp,
                                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
+    lib.or_sph_grid.argtypes = [C.c_int64, _f32p, _f32p, C.c_float, C.c_uint32] + [_vp] * 5
     lib.or_potential_f64.argtypes = [C.c_int, C.c_int64, _f32p, _f32p, _vp, _f32p, C.c_double,
                                      C.c_double, C.c_int]
     lib.or_potential_f64.restype = C.c_double
@@ -383,6 +384,22 @@ def frame(params, state, walk_kind=0, nthreads=8, strict=True):
     if rc != 0:
         raise RuntimeError("or_frame failed")
     return st, int(inter[0]), int(nodes[0])
+
+
+def sph_grid(x, y, cell=3.0, table=16384, strict=True):
+    """SPH neighbour grid (SPH::newGridGPU) as the reference's shaders compute
+    it, bitonic network included: dict of keys, index, cell_x, cell_y
+    (network order) and offsets."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n = len(x)
+    out = {k: np.empty(n, np.uint32) for k in ("keys", "index")}
+    out.update({k: np.empty(n, np.int32) for k in ("cell_x", "cell_y")})
+    out["offsets"] = np.empty(int(table), np.uint32)
+    lib(strict).or_sph_grid(n, x, y, float(cell), int(table),
+                            *(_ptr(out[k]) for k in ("keys", "index", "cell_x", "cell_y",
+                                                      "offsets")))
+    return out
 
 
 # --------------------------------------------------------------------------
