@@ -282,6 +282,16 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     GE_CHECK(c, dalloc(L, &t.lvl_alloc, kMaxLevels + 2));
     GE_CHECK(c, dalloc(L, &t.meta, 16));
     GE_CHECK(c, dalloc(L, &t.tl, kTimeline));
+    // key-prefix build
+    GE_CHECK(c, dalloc(L, &t.kdl, N));
+    GE_CHECK(c, dalloc(L, &t.klam, N));
+    GE_CHECK(c, dalloc(L, &t.kxr, N));
+    t.ksus_cap = (uint32_t)key_suspect_cap((int64_t)N);
+    GE_CHECK(c, dalloc(L, &t.ksus, (size_t)t.ksus_cap));
+    GE_CHECK(c, dalloc(L, &t.kroots, N + 1));
+    t.ktile_cap = (uint32_t)(N / kKeyTile + 1);
+    GE_CHECK(c, dalloc(L, &t.ktile, (size_t)t.ktile_cap * 22));
+    GE_CHECK(c, dalloc(L, &t.kmeta, kKeyMetaWords));
     if (temp) {
         GE_CHECK(c, dalloc(L, &t.ntemp, (size_t)node_cap));
         GE_CHECK(c, dalloc(L, &t.tv, N + (size_t)node_cap + 1));
@@ -636,10 +646,17 @@ int enqueue_permute(ge_ctx *c, bool with_acc) {
     return GE_OK;
 }
 
-int enqueue_build(ge_ctx *c) {
+// fresh_keys: the sort's keys (c->b.ss.keys[0]) belong to the current
+// particle order and positions (a sort and permute ran since the particles
+// last moved), so the tree can be built from them (ge_kbuild.cu)
+int enqueue_build(ge_ctx *c, bool fresh_keys = false) {
     StepParams p = step_params(c);
+    const bool keyed = fresh_keys && c->p.leaf_cap >= 1 && c->p.leaf_cap <= (uint32_t)kKeyMaxCap;
+    if (keyed)
+        GE_CHECK(c, launch_key_build(c->p.dims, cur_state(c), p, c->g, c->b.ss.keys[0], c->b.tree,
+                                     c->d_err, c->num_sms, c->stream));
     GE_CHECK(c, launch_build(c->p.dims, cur_state(c), p, c->g, c->b.tree, c->d_err, c->num_sms,
-                             c->stream));
+                             c->stream, keyed));
     if (c->p.precision == GE_PREC_MIXED) {
         Tree t = mixed_view(c);
         GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, t, c->d_err, c->num_sms,
@@ -698,7 +715,7 @@ int enqueue_frame(ge_ctx *c, cudaEvent_t *ev) {
     if (ev) GE_CHECK(c, cudaEventRecord(ev[3], c->stream));
     if ((rc = enqueue_permute(c, false))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[4], c->stream));
-    if ((rc = enqueue_build(c))) return rc;
+    if ((rc = enqueue_build(c, true))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[5], c->stream));
     if ((rc = enqueue_walk(c, true))) return rc;
     if (ev) GE_CHECK(c, cudaEventRecord(ev[6], c->stream));
@@ -1088,7 +1105,7 @@ int ge_autotune(ge_ctx *c, int32_t reps, ge_tune_result *out) {
             float tmin = 3.0e38f;
             for (int r = 0; r < reps + 1; r++) {   // the first pass is a warm-up
                 GE_CHECK(c, cudaEventRecord(c->ev[0], c->stream));
-                if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c)) ||
+                if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c, true)) ||
                     (rc = enqueue_walk(c, false))) {
                     c->p = keep;
                     return rc;
@@ -1112,7 +1129,8 @@ int ge_autotune(ge_ctx *c, int32_t reps, ge_tune_result *out) {
     out->group_size = c->p.group_size;
     out->leaf_cap = (int32_t)c->p.leaf_cap;
     // accelerations of the current positions under the chosen configuration
-    if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c)) || (rc = enqueue_walk(c, false)))
+    if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_build(c, true)) ||
+        (rc = enqueue_walk(c, false)))
         return rc;
     rc = check_device(c);
     c->tree_valid = rc == GE_OK;
@@ -1426,7 +1444,7 @@ int ge_energy_f64(ge_ctx *c, double *out) {
     if (!c->tree_valid) {
         if ((rc = enqueue_bbox(c, false)) || (rc = enqueue_keys(c)) || (rc = enqueue_sort(c)) ||
             (rc = enqueue_permute(c, true)) || (rc = enqueue_bbox(c, false)) ||
-            (rc = enqueue_build(c)))
+            (rc = enqueue_build(c, true)))
             return rc;
         if ((rc = check_device(c))) return rc;
         c->tree_valid = true;

@@ -96,6 +96,21 @@ struct Tree {
     // particle's own, both as before the walk)
     float *ntemp;
     float *tv;
+    // key-prefix build (ge_kbuild.cu), per particle: kdl = 1 + the level at
+    // which its key first differs from the previous particle's (0 at a
+    // simulation's first particle), klam = its leaf level by the key runs
+    // (levels + 1 when the keys cannot resolve it), kxr = the level of the
+    // exact-rebuild root that holds it (kEmpty: none); ksus = suspect
+    // {level, particle} pairs, kroots = exact-rebuild roots, ktile = per-tile
+    // node counts of every level, kmeta = counters and level totals
+    uint8_t *kdl, *klam;
+    uint32_t *kxr;
+    uint2 *ksus;
+    uint32_t ksus_cap;
+    uint32_t *kroots;
+    uint32_t *ktile;
+    uint32_t ktile_cap;
+    uint32_t *kmeta;
     int64_t cap;
 };
 
@@ -200,11 +215,22 @@ cudaError_t launch_perm_out(int dims, int n, const SortScratch &ss, uint32_t *pe
                             cudaStream_t st);
 cudaError_t launch_keys_out(int dims, int n, const SortScratch &ss, uint64_t *keys,
                             cudaStream_t st);
-// tree build + mass/centre of mass + walk layout (one cooperative launch)
+// tree build + mass/centre of mass + walk layout (one cooperative launch);
+// keyed: the key-prefix passes (launch_key_build) ran first, and this launch
+// completes their tree (leaf sums, upward masses, exact rebuilds, layout)
 int build_grid_blocks(int dims, int num_sms);
 int64_t build_node_slack(int dims, int num_sms);
 cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Segs &g, Tree &t,
-                         uint32_t *err, int num_sms, cudaStream_t st);
+                         uint32_t *err, int num_sms, cudaStream_t st, bool keyed = false);
+// key-prefix tree passes (ge_kbuild.cu) over the Morton-sorted particles and
+// their sorted keys (2D: key << 28 | index words; 3D: keys)
+constexpr int kKeyMaxCap = 32;   // leaf capacities the key-prefix build handles
+constexpr int kKeyTile = 256;    // particles per tile of its node-count scan (one per thread)
+constexpr int kKeyMetaWords = 64;
+int64_t key_suspect_cap(int64_t n);
+cudaError_t launch_key_build(int dims, const State &s, const StepParams &p, const Segs &g,
+                             const uint64_t *keys, Tree &t, uint32_t *err, int num_sms,
+                             cudaStream_t st);
 // GE_PREC_MIXED group walk (ge_gwalk.cu): warps walk for groups of
 // p.group_size consecutive particles of one simulation; counter = one word
 int group_walk_warps(int dims, int num_sms);

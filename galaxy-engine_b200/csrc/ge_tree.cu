@@ -35,6 +35,7 @@
 
 #include "ge_device.cuh"
 #include "ge_internal.h"
+#include "ge_tree_dev.cuh"
 
 namespace ge {
 
@@ -43,7 +44,7 @@ constexpr uint32_t kSmallNode = 32;
 
 // meta[] words used by the build
 constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 3,
-              kMetaSmall = 5, kMetaP2Alloc = 6, kMetaReal = 8, kMetaSlots = 9,
+              kMetaSmall = 5, kMetaP2Alloc = 6, kMetaTimeline = 7, kMetaReal = 8, kMetaSlots = 9,
               kMetaP2Task = 12;
 constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
 
@@ -82,127 +83,6 @@ __device__ __forceinline__ void stamp(Tree &t) {
     }
 }
 
-// std::partition_point(v + first, v + first + len, [mid](float a){ return a < mid; })
-// emulated by G consecutive lanes.  Lane j (1 <= j < G) of the group stands for
-// node j of the search's decision tree (heap order; child 2j when the probe is
-// false, 2j+1 when true); one round evaluates all of them and walks log2(G)
-// steps.  All 32 lanes call this together; groups may differ in their
-// arguments (len 0 for a group with nothing to search).
-template <int G>
-__device__ __forceinline__ uint32_t group_partition_point(const float *__restrict__ v,
-                                                          uint32_t first, uint32_t len,
-                                                          float mid) {
-    constexpr int DEPTH = (G == 32) ? 5 : (G == 16) ? 4 : (G == 8) ? 3 : (G == 4) ? 2 : 1;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned gl = lane & (G - 1u);
-    const unsigned gbase = lane & ~(G - 1u);
-    while (__any_sync(0xffffffffu, len > 0)) {
-        bool pred = false;
-        if (len > 0 && gl > 0) {
-            uint32_t f = first, l = len;
-            const int depth = 31 - __clz(gl);
-            for (int b = depth - 1; b >= 0 && l > 0; --b) {
-                uint32_t half = l >> 1;
-                if ((gl >> b) & 1u) { f += half + 1; l -= half + 1; }
-                else { l = half; }
-            }
-            if (l > 0) pred = __ldg(v + f + (l >> 1)) < mid;
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, pred) >> gbase;
-        unsigned j = 1;
-#pragma unroll
-        for (int st = 0; st < DEPTH; st++) {
-            if (len == 0) break;
-            uint32_t half = len >> 1;
-            unsigned b = (bal >> j) & 1u;
-            if (b) { first += half + 1; len -= half + 1; }
-            else { len = half; }
-            j = 2 * j + b;
-        }
-    }
-    return first;
-}
-
-// Cut points of one node per group of G lanes: Node::subGridMaker (y, then x
-// in each half) / subGridMaker3D (z, then y in each half, then x in each
-// quarter).  Every lane of the group ends with the group's b[0..Q].
-template <int D, int G>
-__device__ __forceinline__ void cut_group(const State &s, uint32_t st, uint32_t en,
-                                          const float *mid, uint32_t *b) {
-    constexpr int Q = 1 << D;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned gl = lane & (G - 1u), gbase = lane & ~(G - 1u);
-    b[0] = st; b[Q] = en;
-    if (D == 2) {
-        b[2] = group_partition_point<G>(s.y, st, en - st, mid[1]);
-        const bool lo = gl < G / 2;
-        const uint32_t f = lo ? st : b[2];
-        const uint32_t l = lo ? b[2] - st : en - b[2];
-        const uint32_t r = group_partition_point<G / 2>(s.x, f, l, mid[0]);
-        b[1] = __shfl_sync(0xffffffffu, r, gbase);
-        b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
-    } else {
-        b[4] = group_partition_point<G>(s.z, st, en - st, mid[2]);
-        const bool lo = gl < G / 2;
-        uint32_t f = lo ? st : b[4];
-        uint32_t l = lo ? b[4] - st : en - b[4];
-        uint32_t r = group_partition_point<G / 2>(s.y, f, l, mid[1]);
-        b[2] = __shfl_sync(0xffffffffu, r, gbase);
-        b[6] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
-        const unsigned g4 = gl / (G / 4);
-        const uint32_t a0 = g4 == 0 ? st : (g4 == 1 ? b[2] : (g4 == 2 ? b[4] : b[6]));
-        const uint32_t a1 = g4 == 0 ? b[2] : (g4 == 1 ? b[4] : (g4 == 2 ? b[6] : en));
-        r = group_partition_point<G / 4>(s.x, a0, a1 - a0, mid[0]);
-        b[1] = __shfl_sync(0xffffffffu, r, gbase);
-        b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 4);
-        b[5] = __shfl_sync(0xffffffffu, r, gbase + 2 * (G / 4));
-        b[7] = __shfl_sync(0xffffffffu, r, gbase + 3 * (G / 4));
-    }
-}
-
-// std::partition_point over predicate bits held in a register (bit r is the
-// predicate of element r), GNU probe sequence, positions relative to bit 0
-__device__ __forceinline__ uint32_t bits_partition_point(uint32_t bits, uint32_t first,
-                                                         uint32_t len) {
-    while (len > 0) {
-        const uint32_t half = len >> 1;
-        const uint32_t probe = first + half;
-        if ((bits >> probe) & 1u) { first = probe + 1; len -= half + 1; }
-        else { len = half; }
-    }
-    return first;
-}
-
-template <int D>
-__device__ __forceinline__ bool is_leaf(const StepParams &p, uint32_t cnt, float size) {
-    // quadtree.cpp:16 / :120 with the leaf capacity and size gate parameterised
-    return ((cnt <= p.leaf_cap && size <= p.size_gate) || cnt == 1u) || size <= p.min_size;
-}
-
-// computeLeafMass / computeLeafMass3D: sequential sums in the reference's order
-template <int D>
-__device__ __forceinline__ float4 leaf_mass(const State &s, uint32_t st, uint32_t en) {
-    float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
-    for (uint32_t i = st; i < en; i++) {
-        const float mi = s.m[i];
-        gm = fadd(gm, mi);
-        c[0] = fadd(c[0], fmul(s.x[i], mi));
-        c[1] = fadd(c[1], fmul(s.y[i], mi));
-        if (D == 3) c[2] = fadd(c[2], fmul(s.z[i], mi));
-    }
-    if (gm > 0.0f) {
-        c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
-        if (D == 3) c[2] = fdiv(c[2], gm);
-    }
-    return make_float4(c[0], c[1], c[2], gm);
-}
-
-template <int D>
-__device__ __forceinline__ void put_walk(Tree &t, uint32_t k, float4 cm, float size) {
-    const float s2 = fmul(size, size);
-    if (D == 2) t.walk[k] = make_float4(cm.x, cm.y, cm.w, s2);
-    else { t.walk[k] = make_float4(cm.x, cm.y, cm.z, cm.w); t.size2[k] = s2; }
-}
 
 // computeInternalMass / computeInternalMass3D: children read in the
 // reference's subGrids[x][y]([z]) order, x outermost
@@ -237,27 +117,36 @@ __device__ __forceinline__ float4 combine_children(const Tree &t, uint4 inf) {
 template <int D>
 __device__ __forceinline__ void finish_upward(Tree &t, uint32_t k) {
     // the decrement releases this node's mass to the parent's last child,
-    // whose decrement acquires every sibling's (one release sequence per counter)
+    // whose decrement acquires every sibling's (one release sequence per counter).
+    // An ancestor's links and cell were written before any of its children
+    // existed, so they are read ahead: the next ancestor's while this one's
+    // counter and children are on their way, which leaves two round trips
+    // (counter, children) per level.
     uint32_t par = __ldcg(&t.aux[k]).z;
-    while (par != kEmpty) {
+    if (par == kEmpty) return;
+    uint4 inf = __ldcg(&t.info[par]);
+    float size = __ldcg(&t.cell[par]).w;
+    uint32_t next = __ldcg(&t.aux[par]).z;
+    while (true) {
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> pend(t.pend[par]);
         if (pend.fetch_sub(1u, cuda::memory_order_acq_rel) != 1u) break;
-        const uint4 inf = __ldcg(&t.info[par]);
-        put_walk<D>(t, par, combine_children<D>(t, inf), __ldcg(&t.cell[par]).w);
-        par = __ldcg(&t.aux[par]).z;
+        uint4 inf2 = make_uint4(0u, 0u, 0u, 0u);
+        float size2 = 0.0f;
+        uint32_t next2 = kEmpty;
+        if (next != kEmpty) {
+            inf2 = __ldcg(&t.info[next]);
+            size2 = __ldcg(&t.cell[next]).w;
+            next2 = __ldcg(&t.aux[next]).z;
+        }
+        put_walk<D>(t, par, combine_children<D>(t, inf), size);
+        if (next == kEmpty) break;
+        par = next;
+        inf = inf2;
+        size = size2;
+        next = next2;
     }
 }
 
-// Corner of child slot q of a cell (Node::subGridMaker newPos).
-template <int D>
-__device__ __forceinline__ float4 child_cell(float4 cell, float half, unsigned q) {
-    float4 cc;
-    cc.x = fadd(cell.x, (q & 1u) ? half : 0.0f);
-    cc.y = fadd(cell.y, (q & 2u) ? half : 0.0f);
-    cc.z = D == 3 ? fadd(cell.z, (q & 4u) ? half : 0.0f) : 0.0f;
-    cc.w = half;
-    return cc;
-}
 
 // Write node k's children (slots in increasing q from `first`) and its own
 // child links; the pending count is set atomically before any child can finish.
@@ -314,6 +203,7 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
     if (leader && leaf) {
         put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), cell.w);
         finish_upward<D>(t, k);
+        atomicMax(&t.meta[kMetaLevels], ax.x + 1u);
     }
     // queue the small subtrees (one atomic per warp)
     {
@@ -692,7 +582,7 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
 
 template <int D>
 __global__ void __launch_bounds__(kBuildThreads, D == 2 ? 3 : 2)
-k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
+k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthreads = gridDim.x * blockDim.x;
@@ -700,23 +590,67 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
     const uint32_t n = (uint32_t)p.n;
     uint32_t *bar_count = t.meta + kMetaBarCount, *bar_gen = t.meta + kMetaBarGen;
 
+    // Keyed: the key passes (ge_kbuild.cu) wrote key_nodes nodes in slots
+    // [0, key_nodes), the segment roots first; pend holds each node's child
+    // bits (bit 31: an exact-rebuild root).  Phase 0 turns the bits into child
+    // masks and pending counts, sums the leaves, and passes the leaves'
+    // masses upward; phase 1 then starts from the exact-rebuild roots.
+    uint32_t lb = 0, le = (uint32_t)g.S, front = (uint32_t)g.S;
+    const uint32_t *list = nullptr;
+    // counters of this build (read only after the first grid barrier)
+    if (gtid == 0) {
+        t.meta[kMetaNodes] = 0u; t.meta[kMetaLevels] = 0u;
+        t.meta[kMetaSmall] = 0u; t.meta[kMetaP2Alloc] = 0u; t.meta[kMetaTimeline] = 0u;
+        t.meta[kMetaReal] = 0u; t.meta[kMetaSlots] = 0u; t.meta[kMetaP2Task] = 0u;
+        stamp(t);
+    }
+    for (uint32_t i = gtid; i < (uint32_t)kMaxLevels + 2u; i += nthreads) t.lvl_alloc[i] = 0u;
+    for (uint32_t i = gtid; i <= n; i += nthreads) t.endcnt[i] = 0u;
+    if (keyed) {
+        const uint32_t key_nodes = *(volatile uint32_t *)&t.kmeta[3];
+        if ((int64_t)key_nodes > t.cap) return;   // the emit pass set kErrNodeCap
+        for (uint32_t k = gtid; k < key_nodes; k += nthreads) {
+            const uint32_t pv = __ldcg(&t.pend[k]);
+            const uint32_t mask = pv & 0xFFu;
+            const bool exact = pv >> 31;
+            reinterpret_cast<uint32_t *>(t.info)[4 * (size_t)k + 1] = exact ? 0u : mask;
+            t.pend[k] = exact ? 0u : (uint32_t)__popc(mask);
+            if (!exact && !mask) {
+                const uint4 inf = __ldcg(&t.info[k]);
+                put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), __ldcg(&t.cell[k]).w);
+            }
+        }
+        if (gtid == 0) atomicMax(&t.meta[kMetaLevels], *(volatile uint32_t *)&t.kmeta[4]);
+        grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
+        for (uint32_t k = gtid; k < key_nodes; k += nthreads)
+            if (__ldcg(&t.info[k]).y == 0u && __ldcg(&t.aux[k]).w == 0u) finish_upward<D>(t, k);
+        list = t.kroots;
+        le = *(volatile uint32_t *)&t.kmeta[1];
+        front = key_nodes;
+    } else {
+        // one root per segment (seeded by the box kernel): nodes 0 .. S-1
+        for (uint32_t r = gtid; r < (uint32_t)g.S; r += nthreads)
+            t.aux[r] = make_uint4(0u, 0u, kEmpty, 0u);
+    }
+
     // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
-    // one root per segment (seeded by the box kernel): nodes 0 .. S-1
-    uint32_t lb = 0, le = (uint32_t)g.S;
+    // the first level is the segment roots (or the exact-rebuild roots, by
+    // list); children go to slots from `front` on
     int L = 0;
-    for (uint32_t r = gtid; r < (uint32_t)g.S; r += nthreads)
-        t.aux[r] = make_uint4(0u, 0u, kEmpty, 0u);
-    if (gtid == 0) t.level[0] = 0;
+    if (gtid == 0) t.level[0] = lb;
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
     while (true) {
         if (le - lb <= nwarps) {
             for (uint32_t k = lb + gwarp; k < le; k += nwarps)
-                split_level_node<D, 32>(s, p, t, k, true, le, &t.lvl_alloc[L], err);
+                split_level_node<D, 32>(s, p, t, list ? __ldcg(&list[k]) : k, true, front,
+                                        &t.lvl_alloc[L], err);
         } else {
             for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
                 const uint32_t k = kb + (lane >> 3);
-                split_level_node<D, 8>(s, p, t, k, k < le, le, &t.lvl_alloc[L], err);
+                const uint32_t node = list && k < le ? __ldcg(&list[k]) : k;
+                split_level_node<D, 8>(s, p, t, node, k < le, front, &t.lvl_alloc[L], err);
             }
         }
         grid_barrier(bar_count, bar_gen, err);
@@ -728,14 +662,17 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err) {
             if (gtid == 0) set_err(err, kErrDepth);
             break;
         }
-        lb = le;
-        le = le + cnt;
+        lb = front;
+        le = front + cnt;
+        front = le;
+        list = nullptr;
         L++;
         if (gtid == 0) t.level[L] = lb;
     }
+    le = front;   // phase-1 slots end here
     if (gtid == 0) {
         t.level[L + 1] = le;
-        atomicMax(&t.meta[kMetaLevels], (uint32_t)(L + 1));
+        if (!keyed) atomicMax(&t.meta[kMetaLevels], (uint32_t)(L + 1));
     }
     if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
 
@@ -920,19 +857,8 @@ int build_grid_blocks(int dims, int num_sms) {
 }
 
 cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Segs &g, Tree &t,
-                         uint32_t *err, int num_sms, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(t.lvl_alloc, 0, sizeof(uint32_t) * (kMaxLevels + 2), st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(t.endcnt, 0, sizeof(uint32_t) * ((size_t)p.n + 1), st);
-    if (e != cudaSuccess) return e;
-    // node count, level count, small-queue length, phase-2 allocation
-    e = cudaMemsetAsync(t.meta + kMetaNodes, 0, 2 * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
-    // small-queue length, phase-2 slots, timeline count, real phase-2 nodes, slots
-    e = cudaMemsetAsync(t.meta + kMetaSmall, 0, 5 * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(t.meta + kMetaP2Task, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
+                         uint32_t *err, int num_sms, cudaStream_t st, bool keyed) {
+    // the kernel zeroes its own counters, level allocation and end histogram
     const int blocks = build_grid_blocks(dims, num_sms);
     if (blocks < 1) return cudaErrorLaunchOutOfResources;
     State sc = s;
@@ -940,7 +866,8 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Se
     Segs gc = g;
     Tree tc = t;
     uint32_t *ec = err;
-    void *args[] = {&sc, &pc, &gc, &tc, &ec};
+    int kc = keyed ? 1 : 0;
+    void *args[] = {&sc, &pc, &gc, &tc, &ec, &kc};
     return cudaLaunchCooperativeKernel(dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
                                        dim3(blocks), dim3(kBuildThreads), args, 0, st);
 }
