@@ -304,9 +304,15 @@ template <int D>
 __global__ void __launch_bounds__(kKT)
 k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t, int tiles,
            uint32_t *err) {
-    constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32;
+    constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32, Q = 1 << D;
     __shared__ uint32_t s_w[NL][W];     // per warp: level-L starts; then their offsets
-    __shared__ uint32_t s_total;
+    __shared__ uint32_t s_total, s_maxT;
+    __shared__ uint32_t s_slot[NL][kKT];   // slot of the level-L node each particle starts
+    __shared__ float4 s_walk[2][kKT];       // mass and centre of mass by level parity
+    __shared__ uint8_t s_done[2][kKT];
+    __shared__ uint64_t s_key[kKT];
+    __shared__ uint8_t s_dl[kKT];
+    __shared__ uint32_t s_bb[W], s_bc[W];
     const uint32_t n = (uint32_t)p.n;
     const unsigned tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -355,6 +361,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         sz = box.w;
     }
     const uint32_t top = valid ? max(T, ends ? Tp : 0u) : 0u;
+    const float root_size = sz;
     uint32_t held = kEmpty;   // the level-(L-1) node holding a
     uint32_t maxl = 0;
     for (int L = 0; L < NL; L++) {
@@ -368,6 +375,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         }
         if (valid && st) {
             const uint32_t slot = excl;
+            s_slot[L][tid] = slot;
             t.cell[slot] = make_float4(cor[0], cor[1], D == 3 ? cor[2] : 0.0f, sz);
             info[4 * (size_t)slot + 2] = a;
             if ((uint32_t)L == T) info[4 * (size_t)slot + 0] = 0u;
@@ -399,6 +407,110 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     }
     for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(0xffffffffu, maxl, o));
     if (lane == 0) atomicMax(&t.kmeta[kKmLevels], maxl + 1u);
+
+    // ---- masses, bottom-up: every leaf, and every node whose particles all
+    // lie in this tile and whose children are all done (not an exact-rebuild
+    // root or above one).  A done node's walk entry is final and its aux.w is
+    // 2; the build kernel combines the rest.  Sums in the reference's order:
+    // a leaf's particles in order, a node's children x-major. ----
+    s_key[tid] = key;
+    const uint32_t dlb = valid ? dl : 0u;   // past the array's end: a boundary at every level
+    s_dl[tid] = (uint8_t)dlb;
+    if (tid == 0) s_maxT = 0u;
+    __syncthreads();
+    if (valid && dl <= T) atomicMax(&s_maxT, T);
+    const uint32_t w0 = blockIdx.x * kKeyTile;
+    const uint32_t lam = valid ? (uint32_t)t.klam[a] : 0u;
+    // a leaf's mass first (its range: up to the first level-T boundary after a)
+    float4 leaf_cm = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid && dl <= T && T == lam && T != X) {
+        uint32_t e = a + 1u;
+        while (e < w0 + kKT && e < n && s_dl[e - w0] > T) e++;
+        if (e == w0 + kKT)
+            while (e < n && t.kdl[e] > T) e++;
+        leaf_cm = leaf_mass<D>(s, a, e);
+    }
+    __syncthreads();
+    // the next tile's first particle bounds every level at or below dl_next
+    const uint32_t dl_next = w0 + kKT < n ? t.kdl[w0 + kKT] : 0u;
+    for (int L = (int)s_maxT; L >= 0; --L) {
+        const unsigned bb = __ballot_sync(0xffffffffu, dlb <= (uint32_t)L);
+        const unsigned bc = __ballot_sync(0xffffffffu, valid && dl == (uint32_t)L + 1u);
+        if (lane == 0) { s_bb[w] = bb; s_bc[w] = bc; }
+        __syncthreads();
+        if (valid && dl <= (uint32_t)L && (uint32_t)L <= T) {
+            const uint32_t slot = s_slot[L][tid];
+            bool done = false;
+            float4 cm = make_float4(0.f, 0.f, 0.f, 0.f);
+            if ((uint32_t)L != X) {
+                // the node's end: the first level-L boundary after a (tile index)
+                uint32_t ie = kKT;
+                if ((uint32_t)L != lam)
+                    for (uint32_t wi = (tid + 1u) >> 5; wi < (uint32_t)W; wi++) {
+                        uint32_t bits = s_bb[wi];
+                        if (wi == ((tid + 1u) >> 5)) bits &= ~((1u << ((tid + 1u) & 31u)) - 1u);
+                        if (bits) { ie = wi * 32u + (uint32_t)(__ffs(bits) - 1); break; }
+                    }
+                if ((uint32_t)L == lam) {   // leaf (computeLeafMass, above)
+                    cm = leaf_cm;
+                    done = true;
+                } else if (ie < (uint32_t)kKT || dl_next <= (uint32_t)L) {
+                    // inside the tile: children start at a and at the level-(L+1)
+                    // boundaries before the end
+                    const int pb = (L + 1) & 1;
+                    uint64_t lanes = 0;
+                    uint32_t cmask = 0;
+                    bool all = true;
+                    auto take = [&](uint32_t j) {
+                        const unsigned q = digit<D>(s_key[j], L);
+                        cmask |= 1u << q;
+                        lanes |= (uint64_t)j << (8 * q);
+                        all = all && s_done[pb][j];
+                    };
+                    take(tid);
+                    for (uint32_t wi = (tid + 1u) >> 5; wi < (uint32_t)W && wi * 32u < ie; wi++) {
+                        uint32_t bits = s_bc[wi];
+                        if (wi == ((tid + 1u) >> 5)) bits &= ~((1u << ((tid + 1u) & 31u)) - 1u);
+                        if (ie < wi * 32u + 32u) bits &= (1u << (ie & 31u)) - 1u;
+                        while (bits) {
+                            take(wi * 32u + (uint32_t)(__ffs(bits) - 1));
+                            bits &= bits - 1u;
+                        }
+                    }
+                    if (all) {   // computeInternalMass: children x-major
+                        float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+                        for (int kk = 0; kk < Q; kk++) {
+                            unsigned q;
+                            if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
+                            else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
+                            if (!((cmask >> q) & 1u)) continue;
+                            const float4 cw = s_walk[pb][(lanes >> (8 * q)) & 0xFFu];
+                            gm = fadd(gm, cw.w);
+                            c[0] = fadd(c[0], fmul(cw.x, cw.w));
+                            c[1] = fadd(c[1], fmul(cw.y, cw.w));
+                            if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cw.w));
+                        }
+                        if (gm > 0.0f) {
+                            c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+                            if (D == 3) c[2] = fdiv(c[2], gm);
+                        }
+                        cm = make_float4(c[0], c[1], c[2], gm);
+                        done = true;
+                    }
+                }
+            }
+            s_done[L & 1][tid] = done ? 1u : 0u;
+            if (done) {
+                s_walk[L & 1][tid] = cm;
+                float szl = root_size;
+                for (int l = 0; l < L; l++) szl = fmul(szl, 0.5f);
+                put_walk<D>(t, slot, cm, szl);
+                aux[4 * (size_t)slot + 3] = 2u;
+            }
+        }
+        __syncthreads();
+    }
 }
 
 template <int D>

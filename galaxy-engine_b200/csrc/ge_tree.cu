@@ -232,6 +232,74 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
     }
 }
 
+// Keyed build: an exact-rebuild root of up to kBlockRootMax particles is
+// rebuilt by one block, level by level with block barriers.  The block's
+// level lists hold only its nodes of more than kSmallNode particles (at most
+// count / (kSmallNode + 1) per level); a child that is a leaf is summed and
+// passed upward at once, a small one goes to the subtree queue (phase 2).
+// Children's slots come from *alloc above `base`.
+constexpr int kBlkList = 64;
+constexpr uint32_t kBlockRootMax = kSmallNode * kBlkList;
+
+template <int D, int G>
+__device__ __forceinline__ void rebuild_large_node(const State &s, const StepParams &p, Tree &t,
+                                                   uint32_t k, bool valid, uint32_t base,
+                                                   uint32_t *alloc, uint32_t *next,
+                                                   uint32_t *next_cnt, uint32_t *err) {
+    constexpr int Q = 1 << D;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gl = lane & (G - 1u);
+    uint4 inf = make_uint4(0, 0, 0, 0), ax = make_uint4(0, 0, 0, 0);
+    float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        inf = __ldcg(&t.info[k]);
+        cell = __ldcg(&t.cell[k]);
+        ax = __ldcg(&t.aux[k]);
+    }
+    const float half = fmul(cell.w, 0.5f);
+    const float mid[3] = {fadd(cell.x, half), fadd(cell.y, half), fadd(cell.z, half)};
+    uint32_t b[Q + 1];
+    cut_group<D, G>(s, valid ? inf.z : 0u, valid ? inf.w : 0u, mid, b);
+    uint32_t mask = 0;
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
+    }
+    const bool leader = valid && gl == 0;
+    const uint32_t nch = leader ? (uint32_t)__popc(mask) : 0u;
+    uint32_t incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += v;
+    }
+    const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t wbase = 0;
+    if (lane == 0 && tot) wbase = atomicAdd(alloc, tot);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    // every lane of the group learns where its node's children start
+    uint32_t first = base + wbase + incl - nch;
+    first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1u));
+    bool ok = (uint64_t)base + wbase + tot <= (uint64_t)t.cap;
+    if (!ok && lane == 0) set_err(err, kErrNodeCap);
+    if (leader && ok) emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+    __syncwarp();
+    // the group's lane q takes child q
+    if (valid && ok && gl < (unsigned)Q && ((mask >> gl) & 1u)) {
+        const uint32_t c = first + __popc(mask & ((1u << gl) - 1u));
+        const uint32_t cnt = b[gl + 1] - b[gl];
+        if (is_leaf<D>(p, cnt, half)) {
+            put_walk<D>(t, c, leaf_mass<D>(s, b[gl], b[gl + 1]), half);
+            finish_upward<D>(t, c);
+            atomicMax(&t.meta[kMetaLevels], ax.x + 2u);
+        } else if (cnt <= kSmallNode) {
+            t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = c;
+        } else {
+            next[atomicAdd(next_cnt, 1u)] = c;
+        }
+    }
+}
+
 // Phase-2 node allocation per warp: slots come from the shared counter in
 // chunks of kChunk; the unused tail of a chunk becomes holes (empty range),
 // which the layout skips.  `real` counts the slots actually used.
@@ -592,9 +660,11 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
 
     // Keyed: the key passes (ge_kbuild.cu) wrote key_nodes nodes in slots
     // [0, key_nodes), the segment roots first; pend holds each node's child
-    // bits (bit 31: an exact-rebuild root).  Phase 0 turns the bits into child
-    // masks and pending counts, sums the leaves, and passes the leaves'
-    // masses upward; phase 1 then starts from the exact-rebuild roots.
+    // bits (bit 31: an exact-rebuild root), aux.w marks exact-rebuild roots
+    // (1) and nodes whose mass is already final (2: every leaf, and the nodes
+    // inside one emit tile).  Phase 0 turns the bits into child masks and, for
+    // the other nodes, counts the children still pending; nodes with none are
+    // listed to be combined after the exact rebuilds (phases 1, 2).
     uint32_t lb = 0, le = (uint32_t)g.S, front = (uint32_t)g.S;
     const uint32_t *list = nullptr;
     // counters of this build (read only after the first grid barrier)
@@ -613,18 +683,30 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             const uint32_t pv = __ldcg(&t.pend[k]);
             const uint32_t mask = pv & 0xFFu;
             const bool exact = pv >> 31;
+            const bool done = __ldcg(&t.aux[k]).w & 2u;
             reinterpret_cast<uint32_t *>(t.info)[4 * (size_t)k + 1] = exact ? 0u : mask;
-            t.pend[k] = exact ? 0u : (uint32_t)__popc(mask);
-            if (!exact && !mask) {
-                const uint4 inf = __ldcg(&t.info[k]);
-                put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), __ldcg(&t.cell[k]).w);
+            uint32_t pending = 0;
+            if (!exact && !done) {
+                const uint32_t first = __ldcg(&t.info[k]).x;
+                const uint32_t nch = (uint32_t)__popc(mask);
+                for (uint32_t c = 0; c < nch; c++) pending += (__ldcg(&t.aux[first + c]).w & 2u) ? 0u : 1u;
+            }
+            t.pend[k] = pending;
+            const bool ready = !exact && !done && pending == 0u;
+            // combined after the exact rebuilds: list them (slot_of is free
+            // until the layout)
+            const unsigned lbits = __ballot_sync(__activemask(), ready);
+            if (ready) {
+                const int leader = __ffs(lbits) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&t.kmeta[5], (uint32_t)__popc(lbits));
+                base = __shfl_sync(lbits, base, leader);
+                t.slot_of[base + __popc(lbits & ((1u << lane) - 1u))] = k;
             }
         }
         if (gtid == 0) atomicMax(&t.meta[kMetaLevels], *(volatile uint32_t *)&t.kmeta[4]);
         grid_barrier(bar_count, bar_gen, err);
         if (gtid == 0) stamp(t);
-        for (uint32_t k = gtid; k < key_nodes; k += nthreads)
-            if (__ldcg(&t.info[k]).y == 0u && __ldcg(&t.aux[k]).w == 0u) finish_upward<D>(t, k);
         list = t.kroots;
         le = *(volatile uint32_t *)&t.kmeta[1];
         front = key_nodes;
@@ -634,23 +716,81 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             t.aux[r] = make_uint4(0u, 0u, kEmpty, 0u);
     }
 
+    if (keyed) {
+        // exact-rebuild roots of up to kBlockRootMax particles: a block each
+        __shared__ uint32_t s_list[2][kBlkList];
+        __shared__ uint32_t s_cnt[2], s_m;
+        const uint32_t nroots = le;
+        const uint32_t xbase = front;
+        uint32_t *xalloc = &t.kmeta[6];
+        const unsigned w = threadIdx.x >> 5, W = kBuildThreads / 32;
+        for (uint32_t r = blockIdx.x; r < nroots; r += gridDim.x) {
+            const uint32_t root = __ldcg(&t.kroots[r]);
+            const uint4 ri = __ldcg(&t.info[root]);
+            const uint32_t cnt = ri.w - ri.z;
+            if (cnt > kBlockRootMax) continue;   // left to the grid's level loop
+            if (cnt <= kSmallNode) {
+                if (threadIdx.x == 0) t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = root;
+                continue;
+            }
+            if (threadIdx.x == 0) { s_list[0][0] = root; s_cnt[0] = 1u; }
+            int cur = 0;
+            for (int it = 0; it < kMaxLevels; it++) {
+                if (threadIdx.x == 0) {   // one decision for the whole block
+                    s_cnt[cur ^ 1] = 0u;
+                    s_m = ((*(volatile uint32_t *)err) & kErrNodeCap) ? 0u : s_cnt[cur];
+                }
+                __syncthreads();
+                const uint32_t m = s_m;
+                if (m == 0u) break;
+                if (m <= W) {
+                    for (uint32_t j = w; j < m; j += W)
+                        rebuild_large_node<D, 32>(s, p, t, s_list[cur][j], true, xbase, xalloc,
+                                                  s_list[cur ^ 1], &s_cnt[cur ^ 1], err);
+                } else {
+                    for (uint32_t jb = w * 4; jb < m; jb += W * 4) {
+                        const uint32_t j = jb + (lane >> 3);
+                        rebuild_large_node<D, 8>(s, p, t, j < m ? s_list[cur][j] : 0u, j < m,
+                                                 xbase, xalloc, s_list[cur ^ 1], &s_cnt[cur ^ 1],
+                                                 err);
+                    }
+                }
+                __syncthreads();
+                cur ^= 1;
+            }
+            __syncthreads();
+        }
+    }
+
     // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
-    // the first level is the segment roots (or the exact-rebuild roots, by
-    // list); children go to slots from `front` on
+    // the first level is the segment roots (or, keyed, the exact-rebuild roots
+    // too large for one block, by list); children go to slots from `front` on
     int L = 0;
     if (gtid == 0) t.level[0] = lb;
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
+    if (keyed) front += *(volatile uint32_t *)&t.kmeta[6];   // after the blocks' rebuilds
     while (true) {
         if (le - lb <= nwarps) {
-            for (uint32_t k = lb + gwarp; k < le; k += nwarps)
-                split_level_node<D, 32>(s, p, t, list ? __ldcg(&list[k]) : k, true, front,
-                                        &t.lvl_alloc[L], err);
+            for (uint32_t k = lb + gwarp; k < le; k += nwarps) {
+                const uint32_t node = list ? __ldcg(&list[k]) : k;
+                bool valid = true;
+                if (list) {   // keyed first level: only the roots no block took
+                    const uint4 ri = __ldcg(&t.info[node]);
+                    valid = ri.w - ri.z > kBlockRootMax;
+                }
+                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err);
+            }
         } else {
             for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
                 const uint32_t k = kb + (lane >> 3);
                 const uint32_t node = list && k < le ? __ldcg(&list[k]) : k;
-                split_level_node<D, 8>(s, p, t, node, k < le, front, &t.lvl_alloc[L], err);
+                bool valid = k < le;
+                if (valid && list) {
+                    const uint4 ri = __ldcg(&t.info[node]);
+                    valid = ri.w - ri.z > kBlockRootMax;
+                }
+                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err);
             }
         }
         grid_barrier(bar_count, bar_gen, err);
@@ -711,6 +851,24 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         if (held != kEmpty) finish_upward<D>(t, held);
         mark_holes(t, wa.next, wa.end);
         if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
+    }
+    if (keyed) {
+        // the listed nodes (children all final) and upward from them; every
+        // lane climbs on its own and takes the next node when its chain stops
+        const uint32_t nready = *(volatile uint32_t *)&t.kmeta[5];
+        for (uint32_t idx = gtid; idx < nready; idx += nthreads) {
+            uint32_t cur = __ldcg(&t.slot_of[idx]);
+            while (true) {
+                const uint4 inf = __ldcg(&t.info[cur]);
+                const uint4 ax = __ldcg(&t.aux[cur]);
+                put_walk<D>(t, cur, combine_children<D>(t, inf), __ldcg(&t.cell[cur]).w);
+                const uint32_t par = ax.z;
+                if (par == kEmpty) break;
+                cuda::atomic_ref<uint32_t, cuda::thread_scope_device> pend(t.pend[par]);
+                if (pend.fetch_sub(1u, cuda::memory_order_acq_rel) != 1u) break;
+                cur = par;
+            }
+        }
     }
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
