@@ -294,39 +294,49 @@ k_key_scan(Tree t, int tiles) {
 }
 
 // Node slots: level L's nodes are the slots from base[L] = the node count of
-// the levels above, in the order of their first particles.  A warp walks the
-// levels together; the ballot of the lanes that start a level-L node ranks
-// them.  With excl = the level-L nodes started before particle a:
-//   a starts (L, a)            -> slot excl
-//   the level-L node holding a -> excl - 1 + (a starts it)
-//   the node holding a-1 ends at a when a is a level-L boundary -> slot excl - 1
+// the levels above, in the order of their first particles.  Per warp and
+// level, the ballot of the particles that start a level-L node ranks them, so
+// with off[L][w] = the level-L nodes started before the warp:
+//   a starts (L, a)                   -> slot off[L][w] + popc(ballot & below a)
+//   the level-L node holding a        -> off[L][w] + popc(ballot & up to a) - 1
+//   the node holding a-1 ends at a (a a level-L boundary) -> slot off[L][w] + popc(ballot & below a) - 1
+// Each particle then writes the few nodes it starts and ends.  Masses follow
+// bottom-up, one thread per node of the tile and level.
 template <int D>
 __global__ void __launch_bounds__(kKT)
 k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t, int tiles,
            uint32_t *err) {
     constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32, Q = 1 << D;
-    __shared__ uint32_t s_w[NL][W];     // per warp: level-L starts; then their offsets
+    __shared__ uint32_t s_bal[NL][W];      // per level and warp: the particles that start a node
+    __shared__ uint32_t s_bnd[NL][W];      // ... that are level-L boundaries
+    __shared__ uint32_t s_off[NL][W + 1];  // slot of each warp's first level-L node; [W] = end
     __shared__ uint32_t s_total, s_maxT;
-    __shared__ uint32_t s_slot[NL][kKT];   // slot of the level-L node each particle starts
-    __shared__ float4 s_walk[2][kKT];       // mass and centre of mass by level parity
+    __shared__ float4 s_leaf[kKT];         // leaf masses by the particle that starts the leaf
+    __shared__ float4 s_walk[2][kKT];      // masses by level parity, by node within the tile
     __shared__ uint8_t s_done[2][kKT];
-    __shared__ uint64_t s_key[kKT];
-    __shared__ uint8_t s_dl[kKT];
-    __shared__ uint32_t s_bb[W], s_bc[W];
+    __shared__ uint8_t s_lam[kKT], s_x[kKT];
+    __shared__ float s_rs[kKT];            // root size of each particle's simulation
     const uint32_t n = (uint32_t)p.n;
     const unsigned tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
-    const unsigned lt = (1u << lane) - 1u;
+    const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
     const uint32_t a = blockIdx.x * kKeyTile + tid;
+    const uint32_t w0 = blockIdx.x * kKeyTile;
     const bool valid = a < n;
     const uint32_t dl = valid ? t.kdl[a] : 1u;   // a starts the nodes of levels dl .. T
     const uint32_t T = valid ? key_depth(t, a) : 0u;
     const uint32_t Tp = valid && a > 0 ? key_depth(t, a - 1) : 0u;
-    const bool ends = valid && a > 0 && dl <= Tp;   // nodes holding a-1 end at a
+    const uint32_t X = valid ? __ldcg(&t.kxr[a]) : kEmpty;
+    const uint32_t lam = valid ? (uint32_t)t.klam[a] : 0u;
+    const uint32_t dlb = valid ? dl : 0u;   // past the array's end: a boundary at every level
 #pragma unroll
     for (int L = 0; L < NL; L++) {
         const unsigned b = __ballot_sync(0xffffffffu, dl <= (uint32_t)L && (uint32_t)L <= T);
-        if (lane == 0) s_w[L][w] = (uint32_t)__popc(b);
+        const unsigned bb = __ballot_sync(0xffffffffu, dlb <= (uint32_t)L);
+        if (lane == 0) { s_bal[L][w] = b; s_bnd[L][w] = bb; }
     }
+    s_lam[tid] = (uint8_t)lam;
+    s_x[tid] = (uint8_t)min(X, 255u);
+    if (tid == 0) s_maxT = 0u;
     __syncthreads();
     if (tid < NL) {
         uint32_t base = 0, tot = 0;
@@ -337,13 +347,14 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         }
         uint32_t run = base + t.ktile[(size_t)tid * tiles + blockIdx.x];
         for (int ww = 0; ww < W; ww++) {
-            const uint32_t c = s_w[tid][ww];
-            s_w[tid][ww] = run;
-            run += c;
+            s_off[tid][ww] = run;
+            run += (uint32_t)__popc(s_bal[tid][ww]);
         }
+        s_off[tid][W] = run;
         if (tid == 0) s_total = tot;
         if (blockIdx.x == 0 && tid == 0) t.kmeta[kKmTotal] = tot;
     }
+    if (valid && dl <= T) atomicMax(&s_maxT, T);
     __syncthreads();
     if ((int64_t)s_total > t.cap) {   // the build kernel sees the same total and stops
         if (blockIdx.x == 0 && tid == 0) set_err(err, kErrNodeCap);
@@ -351,160 +362,145 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     }
     uint32_t *info = reinterpret_cast<uint32_t *>(t.info);
     uint32_t *aux = reinterpret_cast<uint32_t *>(t.aux);
-    const uint32_t X = valid ? __ldcg(&t.kxr[a]) : kEmpty;
-    uint64_t key = 0;
-    float cor[3] = {0.f, 0.f, 0.f}, sz = 0.f;
-    if (valid && dl <= T) {
-        key = key_at<D>(keys, a);
-        const float4 box = g.box[g.seg_of ? g.seg_of[a] : 0u];
-        cor[0] = box.x; cor[1] = box.y; cor[2] = box.z;
-        sz = box.w;
-    }
-    const uint32_t top = valid ? max(T, ends ? Tp : 0u) : 0u;
-    const float root_size = sz;
-    uint32_t held = kEmpty;   // the level-(L-1) node holding a
-    uint32_t maxl = 0;
-    for (int L = 0; L < NL; L++) {
-        if (!__any_sync(0xffffffffu, valid && (uint32_t)L <= top)) break;
-        const bool st = dl <= (uint32_t)L && (uint32_t)L <= T;
-        const unsigned b = __ballot_sync(0xffffffffu, st);
-        const uint32_t excl = s_w[L][w] + (uint32_t)__popc(b & lt);
-        if (ends && dl <= (uint32_t)L && (uint32_t)L <= Tp) {
-            info[4 * (size_t)(excl - 1u) + 3] = a;
-            aux[4 * (size_t)(excl - 1u) + 1] = (uint32_t)L - dl;
-        }
-        if (valid && st) {
-            const uint32_t slot = excl;
-            s_slot[L][tid] = slot;
-            t.cell[slot] = make_float4(cor[0], cor[1], D == 3 ? cor[2] : 0.0f, sz);
-            info[4 * (size_t)slot + 2] = a;
-            if ((uint32_t)L == T) info[4 * (size_t)slot + 0] = 0u;
-            if ((uint32_t)L > dl) info[4 * (size_t)held + 0] = slot;   // a's own parent
-            aux[4 * (size_t)slot + 0] = (uint32_t)L;
-            aux[4 * (size_t)slot + 2] = L > 0 ? held : kEmpty;
-            aux[4 * (size_t)slot + 3] = (uint32_t)L == X ? 1u : 0u;
-            if (L > 0) atomicOr(&t.pend[held], 1u << digit<D>(key, L - 1));
-            if ((uint32_t)L == X) {   // exact-rebuild roots have disjoint ranges: fewer than n
-                atomicOr(&t.pend[slot], 1u << 31);
-                const uint32_t r = atomicAdd(&t.kmeta[kKmRoots], 1u);
-                if (r < n) t.kroots[r] = slot;
-            }
-            maxl = max(maxl, (uint32_t)L);
-        }
-        const uint32_t hold = excl - 1u + (st ? 1u : 0u);   // the level-L node holding a
-        if (valid && a == n - 1 && (uint32_t)L <= T) {       // nodes ending at the array's end
-            info[4 * (size_t)hold + 3] = n;
-            aux[4 * (size_t)hold + 1] = (uint32_t)L;
-        }
-        held = hold;
-        if (valid && dl <= T && (uint32_t)L < T) {
-            const float half = fmul(sz, 0.5f);
-            const unsigned q = digit<D>(key, L);
+    float rs = 0.0f;
+    if (valid) {
+        const uint32_t sg = g.seg_of ? g.seg_of[a] : 0u;
+        const float4 box = g.box[sg];
+        rs = box.w;
+        // the nodes a starts: cells along a's key path, from the root
+        if (dl <= T) {
+            const uint64_t key = key_at<D>(keys, a);
+            float cor[3] = {box.x, box.y, box.z};
+            float sz = box.w;
+            for (uint32_t L = 0; L < dl; L++) {
+                const float half = fmul(sz, 0.5f);
+                const unsigned q = digit<D>(key, (int)L);
 #pragma unroll
-            for (int ax = 0; ax < D; ax++) cor[ax] = fadd(cor[ax], ((q >> ax) & 1u) ? half : 0.0f);
-            sz = half;
+                for (int ax = 0; ax < D; ax++) cor[ax] = fadd(cor[ax], ((q >> ax) & 1u) ? half : 0.0f);
+                sz = half;
+            }
+            for (uint32_t L = dl; L <= T; L++) {
+                const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & lt);
+                t.cell[slot] = make_float4(cor[0], cor[1], D == 3 ? cor[2] : 0.0f, sz);
+                info[4 * (size_t)slot + 0] =
+                    L < T ? s_off[L + 1][w] + (uint32_t)__popc(s_bal[L + 1][w] & lt) : 0u;
+                info[4 * (size_t)slot + 2] = a;
+                const uint32_t parent =
+                    L > 0 ? s_off[L - 1][w] + (uint32_t)__popc(s_bal[L - 1][w] & le) - 1u : kEmpty;
+                aux[4 * (size_t)slot + 0] = L;
+                aux[4 * (size_t)slot + 2] = parent;
+                aux[4 * (size_t)slot + 3] = L == X ? 1u : 0u;
+                if (L > 0) atomicOr(&t.pend[parent], 1u << digit<D>(key, (int)L - 1));
+                if (L == X) {   // exact-rebuild roots have disjoint ranges: fewer than n
+                    atomicOr(&t.pend[slot], 1u << 31);
+                    const uint32_t r = atomicAdd(&t.kmeta[kKmRoots], 1u);
+                    if (r < n) t.kroots[r] = slot;
+                }
+                if (L < T) {
+                    const float half = fmul(sz, 0.5f);
+                    const unsigned q = digit<D>(key, (int)L);
+#pragma unroll
+                    for (int ax = 0; ax < D; ax++) cor[ax] = fadd(cor[ax], ((q >> ax) & 1u) ? half : 0.0f);
+                    sz = half;
+                }
+            }
+        }
+        // the nodes holding a-1 that end at a
+        if (a > 0)
+            for (uint32_t L = dl; L <= Tp; L++) {
+                const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & lt) - 1u;
+                info[4 * (size_t)slot + 3] = a;
+                aux[4 * (size_t)slot + 1] = L - dl;
+            }
+        if (a == n - 1)   // the nodes that end at the end of the particle array
+            for (uint32_t L = 0; L <= T; L++) {
+                const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & le) - 1u;
+                info[4 * (size_t)slot + 3] = n;
+                aux[4 * (size_t)slot + 1] = L;
+            }
+        // a leaf's mass (computeLeafMass): up to the first level-T boundary after a
+        if (dl <= T && T == lam && T != X) {
+            uint32_t e = a + 1u;
+            while (e < n && t.kdl[e] > T) e++;
+            s_leaf[tid] = leaf_mass<D>(s, a, e);
         }
     }
-    for (int o = 16; o > 0; o >>= 1) maxl = max(maxl, __shfl_xor_sync(0xffffffffu, maxl, o));
-    if (lane == 0) atomicMax(&t.kmeta[kKmLevels], maxl + 1u);
+    s_rs[tid] = rs;
+    {
+        const uint32_t ml = __reduce_max_sync(0xffffffffu, valid && dl <= T ? T + 1u : 0u);
+        if (lane == 0 && ml) atomicMax(&t.kmeta[kKmLevels], ml);
+    }
+    __syncthreads();
 
     // ---- masses, bottom-up: every leaf, and every node whose particles all
     // lie in this tile and whose children are all done (not an exact-rebuild
     // root or above one).  A done node's walk entry is final and its aux.w is
-    // 2; the build kernel combines the rest.  Sums in the reference's order:
-    // a leaf's particles in order, a node's children x-major. ----
-    s_key[tid] = key;
-    const uint32_t dlb = valid ? dl : 0u;   // past the array's end: a boundary at every level
-    s_dl[tid] = (uint8_t)dlb;
-    if (tid == 0) s_maxT = 0u;
-    __syncthreads();
-    if (valid && dl <= T) atomicMax(&s_maxT, T);
-    const uint32_t w0 = blockIdx.x * kKeyTile;
-    const uint32_t lam = valid ? (uint32_t)t.klam[a] : 0u;
-    // a leaf's mass first (its range: up to the first level-T boundary after a)
-    float4 leaf_cm = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid && dl <= T && T == lam && T != X) {
-        uint32_t e = a + 1u;
-        while (e < w0 + kKT && e < n && s_dl[e - w0] > T) e++;
-        if (e == w0 + kKT)
-            while (e < n && t.kdl[e] > T) e++;
-        leaf_cm = leaf_mass<D>(s, a, e);
-    }
-    __syncthreads();
-    // the next tile's first particle bounds every level at or below dl_next
+    // 2; the build kernel combines the rest.  A node's children are the
+    // contiguous level-(L+1) slots from its first child, in quadrant order. ----
     const uint32_t dl_next = w0 + kKT < n ? t.kdl[w0 + kKT] : 0u;
     for (int L = (int)s_maxT; L >= 0; --L) {
-        const unsigned bb = __ballot_sync(0xffffffffu, dlb <= (uint32_t)L);
-        const unsigned bc = __ballot_sync(0xffffffffu, valid && dl == (uint32_t)L + 1u);
-        if (lane == 0) { s_bb[w] = bb; s_bc[w] = bc; }
-        __syncthreads();
-        if (valid && dl <= (uint32_t)L && (uint32_t)L <= T) {
-            const uint32_t slot = s_slot[L][tid];
+        const uint32_t first = s_off[L][0], K = s_off[L][W] - first;
+        if (tid < K) {
+            const uint32_t slot = first + tid;
+            // the particle that starts it: the tid-th set bit of the level's ballots
+            uint32_t ww = 0;
+            while (ww + 1 < (uint32_t)W && s_off[L][ww + 1] <= slot) ww++;
+            const uint32_t r = slot - s_off[L][ww];
+            const uint32_t ol = (uint32_t)(__fns(s_bal[L][ww], 0u, (int)r + 1));
+            const uint32_t o = ww * 32u + ol;   // tile index of the starting particle
             bool done = false;
             float4 cm = make_float4(0.f, 0.f, 0.f, 0.f);
-            if ((uint32_t)L != X) {
-                // the node's end: the first level-L boundary after a (tile index)
-                uint32_t ie = kKT;
-                if ((uint32_t)L != lam)
-                    for (uint32_t wi = (tid + 1u) >> 5; wi < (uint32_t)W; wi++) {
-                        uint32_t bits = s_bb[wi];
-                        if (wi == ((tid + 1u) >> 5)) bits &= ~((1u << ((tid + 1u) & 31u)) - 1u);
-                        if (bits) { ie = wi * 32u + (uint32_t)(__ffs(bits) - 1); break; }
-                    }
-                if ((uint32_t)L == lam) {   // leaf (computeLeafMass, above)
-                    cm = leaf_cm;
+            const uint32_t ox = s_x[o];
+            if ((uint32_t)L != ox) {
+                if ((uint32_t)L == s_lam[o]) {
+                    cm = s_leaf[o];
                     done = true;
-                } else if (ie < (uint32_t)kKT || dl_next <= (uint32_t)L) {
-                    // inside the tile: children start at a and at the level-(L+1)
-                    // boundaries before the end
-                    const int pb = (L + 1) & 1;
-                    uint64_t lanes = 0;
-                    uint32_t cmask = 0;
-                    bool all = true;
-                    auto take = [&](uint32_t j) {
-                        const unsigned q = digit<D>(s_key[j], L);
-                        cmask |= 1u << q;
-                        lanes |= (uint64_t)j << (8 * q);
-                        all = all && s_done[pb][j];
-                    };
-                    take(tid);
-                    for (uint32_t wi = (tid + 1u) >> 5; wi < (uint32_t)W && wi * 32u < ie; wi++) {
-                        uint32_t bits = s_bc[wi];
-                        if (wi == ((tid + 1u) >> 5)) bits &= ~((1u << ((tid + 1u) & 31u)) - 1u);
-                        if (ie < wi * 32u + 32u) bits &= (1u << (ie & 31u)) - 1u;
-                        while (bits) {
-                            take(wi * 32u + (uint32_t)(__ffs(bits) - 1));
-                            bits &= bits - 1u;
-                        }
+                } else {
+                    // inside the tile: the first level-L boundary after o is in it,
+                    // or the next tile's first particle is one
+                    bool local = dl_next <= (uint32_t)L;
+                    for (uint32_t wi = (o + 1u) >> 5; !local && wi < (uint32_t)W; wi++) {
+                        uint32_t bits = s_bnd[L][wi];
+                        if (wi == ((o + 1u) >> 5)) bits &= ~((1u << ((o + 1u) & 31u)) - 1u);
+                        local = bits != 0u;
                     }
-                    if (all) {   // computeInternalMass: children x-major
-                        float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+                    if (local) {
+                        const uint32_t mask = __ldcg(&t.pend[slot]) & 0xFFu;
+                        const uint32_t c0 = s_off[L + 1][ww] + (uint32_t)__popc(s_bal[L + 1][ww] & ((1u << ol) - 1u))
+                                            - s_off[L + 1][0];   // first child, tile index
+                        const int pb = (L + 1) & 1;
+                        const uint32_t nch = (uint32_t)__popc(mask);
+                        bool all = true;
+                        for (uint32_t c = 0; c < nch; c++) all = all && s_done[pb][c0 + c];
+                        if (all) {   // computeInternalMass: children x-major
+                            float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-                        for (int kk = 0; kk < Q; kk++) {
-                            unsigned q;
-                            if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
-                            else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
-                            if (!((cmask >> q) & 1u)) continue;
-                            const float4 cw = s_walk[pb][(lanes >> (8 * q)) & 0xFFu];
-                            gm = fadd(gm, cw.w);
-                            c[0] = fadd(c[0], fmul(cw.x, cw.w));
-                            c[1] = fadd(c[1], fmul(cw.y, cw.w));
-                            if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cw.w));
+                            for (int kk = 0; kk < Q; kk++) {
+                                unsigned q;
+                                if (D == 2) q = ((kk >> 1) & 1) | ((kk & 1) << 1);
+                                else q = ((kk >> 2) & 1) | (((kk >> 1) & 1) << 1) | ((kk & 1) << 2);
+                                if (!((mask >> q) & 1u)) continue;
+                                const float4 cw = s_walk[pb][c0 + __popc(mask & ((1u << q) - 1u))];
+                                gm = fadd(gm, cw.w);
+                                c[0] = fadd(c[0], fmul(cw.x, cw.w));
+                                c[1] = fadd(c[1], fmul(cw.y, cw.w));
+                                if (D == 3) c[2] = fadd(c[2], fmul(cw.z, cw.w));
+                            }
+                            if (gm > 0.0f) {
+                                c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+                                if (D == 3) c[2] = fdiv(c[2], gm);
+                            }
+                            cm = make_float4(c[0], c[1], c[2], gm);
+                            done = true;
                         }
-                        if (gm > 0.0f) {
-                            c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
-                            if (D == 3) c[2] = fdiv(c[2], gm);
-                        }
-                        cm = make_float4(c[0], c[1], c[2], gm);
-                        done = true;
                     }
                 }
             }
             s_done[L & 1][tid] = done ? 1u : 0u;
             if (done) {
                 s_walk[L & 1][tid] = cm;
-                float szl = root_size;
-                for (int l = 0; l < L; l++) szl = fmul(szl, 0.5f);
+                // size at level L: the root's halved L times (exact)
+                const float szl = s_rs[o] * __int_as_float((127 - L) << 23);
                 put_walk<D>(t, slot, cm, szl);
                 aux[4 * (size_t)slot + 3] = 2u;
             }
