@@ -96,9 +96,15 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
     for (int q = threadIdx.x; q < kKT + 2 * kHalo + 1; q += kKT)
         sd[q] = (int8_t)delta_at<D>(g, keys, base - kHalo + q, n);
     // parent child bits and counts are accumulated into pend by the emit pass
-    for (int64_t k = (int64_t)blockIdx.x * kKT + threadIdx.x; k < t.cap;
-         k += (int64_t)gridDim.x * kKT)
-        t.pend[k] = 0u;
+    {
+        uint4 *p4 = reinterpret_cast<uint4 *>(t.pend);   // cudaMalloc: 16-byte aligned
+        const int64_t n4 = t.cap / 4;
+        for (int64_t k = (int64_t)blockIdx.x * kKT + threadIdx.x; k < n4;
+             k += (int64_t)gridDim.x * kKT)
+            p4[k] = make_uint4(0u, 0u, 0u, 0u);
+        if (blockIdx.x == 0 && threadIdx.x < (unsigned)(t.cap - n4 * 4))
+            t.pend[n4 * 4 + threadIdx.x] = 0u;
+    }
     __syncthreads();
     const int64_t i = base + threadIdx.x;
     if (i >= n) return;
@@ -118,15 +124,18 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
     const int l_count = best == 127 ? 127 : best + 1;
     const int l_one = max(dl(i), dl(i + 1)) + 1;
     const float4 box = g.box[sg];
-    int l_gate = 127, l_min = 127;
-    {
-        float sz = box.w;
-        for (int L = 0; L <= B; L++) {
-            if (l_gate == 127 && sz <= p.size_gate) l_gate = L;
-            if (sz <= p.min_size) { l_min = L; break; }
-            sz = fmul(sz, 0.5f);
-        }
-    }
+    // first levels whose cells are no larger than the size gate / min size
+    // (the sizes are exact halvings of the root's: box.w * 2^-L)
+    auto first_level_at_most = [&](float limit) {
+        if (box.w != box.w) return 127;
+        if (box.w <= limit) return 0;
+        if (!(limit > 0.0f)) return 127;
+        int L = max(0, ilogbf(box.w) - ilogbf(limit) - 1);
+        while (L <= B && scalbnf(box.w, -L) > limit) L++;
+        return L <= B ? L : 127;
+    };
+    const int l_gate = first_level_at_most(p.size_gate);
+    const int l_min = first_level_at_most(p.min_size);
     int lam = min(min(max(l_count, l_gate), l_one), l_min);
     if (lam > B) lam = B + 1;
     t.kdl[i] = (uint8_t)(dl(i) + 1);
@@ -158,22 +167,33 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
 }
 
 // First j in [first, last) with pred(j) false, pred monotone (true then
-// false), by a whole warp (all lanes call it with the same arguments and
-// get the same result): 32 probes per round narrow the range 33-fold.
-template <typename F>
-__device__ __forceinline__ uint32_t warp_lower_bound(uint32_t first, uint32_t last, F pred) {
+// false), by groups of G lanes, each group with its own range and predicate:
+// G probes per round narrow the range (G + 1)-fold; every lane of the warp
+// must call it, and a group's lanes get the same result.
+template <int G, typename F>
+__device__ __forceinline__ uint32_t group_lower_bound(uint32_t first, uint32_t last, F pred) {
     const unsigned lane = threadIdx.x & 31u;
-    while (last - first > 32u) {
-        const uint32_t len = last - first;
-        const uint32_t q = first + (uint32_t)(((uint64_t)len * (lane + 1u)) / 33u);
-        const unsigned t = __popc(__ballot_sync(0xffffffffu, pred(q)));   // probes still true
-        const uint32_t nf = t ? __shfl_sync(0xffffffffu, q, t - 1) + 1u : first;
-        const uint32_t nl = t < 32u ? __shfl_sync(0xffffffffu, q, t) + 1u : last;
-        first = nf;
-        last = nl;
+    const unsigned gl = lane & (G - 1u), gbase = lane & ~(G - 1u);
+    const unsigned gm = G == 32 ? 0xffffffffu : (1u << G) - 1u;
+    while (__any_sync(0xffffffffu, last - first > (uint32_t)G)) {
+        const bool act = last - first > (uint32_t)G;
+        uint32_t q = 0;
+        bool pv = false;
+        if (act) {
+            q = first + (uint32_t)(((uint64_t)(last - first) * (gl + 1u)) / (G + 1u));
+            pv = pred(q);
+        }
+        const unsigned tc = __popc((__ballot_sync(0xffffffffu, pv) >> gbase) & gm);
+        const uint32_t qa = __shfl_sync(0xffffffffu, q, gbase + (tc ? tc - 1u : 0u));
+        const uint32_t qb = __shfl_sync(0xffffffffu, q, gbase + (tc < (unsigned)G ? tc : G - 1u));
+        if (act) {
+            const uint32_t nf = tc ? qa + 1u : first;
+            last = tc < (unsigned)G ? qb + 1u : last;
+            first = nf;
+        }
     }
-    const bool v = first + lane < last && pred(first + lane);
-    return first + (uint32_t)__popc(__ballot_sync(0xffffffffu, v));
+    const bool v = first + gl < last && pred(first + gl);
+    return first + (uint32_t)__popc((__ballot_sync(0xffffffffu, v) >> gbase) & gm);
 }
 
 template <int D>
@@ -201,11 +221,15 @@ k_key_check(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tr
         const uint64_t ki = key_at<D>(keys, i);
         const int shift = D * (B - L);
         const uint64_t pre = ki >> shift;
-        // the node's range: the run of keys that agree with ki on L digits
-        const uint32_t a =
-            warp_lower_bound(lo, i, [&](uint32_t j) { return (key_at<D>(keys, j) >> shift) < pre; });
-        const uint32_t e = warp_lower_bound(
-            i + 1, hi, [&](uint32_t j) { return (key_at<D>(keys, j) >> shift) <= pre; });
+        // the node's range: the run of keys that agree with ki on L digits (its
+        // start by the low half-warp, its end by the high one, at once)
+        const bool hi_half = lane >= 16u;
+        const uint32_t r = group_lower_bound<16>(hi_half ? i + 1 : lo, hi_half ? hi : i, [&](uint32_t j) {
+            const uint64_t v = key_at<D>(keys, j) >> shift;
+            return hi_half ? v <= pre : v < pre;
+        });
+        const uint32_t a = __shfl_sync(0xffffffffu, r, 0);
+        const uint32_t e = __shfl_sync(0xffffffffu, r, 16);
         // the node's cell along the key path
         const float4 box = g.box[sg];
         float cor[3] = {box.x, box.y, box.z};
@@ -221,13 +245,17 @@ k_key_check(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tr
         const float mid[3] = {fadd(cor[0], half), fadd(cor[1], half), fadd(cor[2], half)};
         uint32_t b[Q + 1];
         cut_group<D, 32>(s, a, e, mid, b);
-        // the key boundaries: first particle of every digit value
-        bool differ = false;
-        for (unsigned q = 1; q < (unsigned)Q; q++) {
-            const uint32_t kb = warp_lower_bound(
-                a, e, [&](uint32_t j) { return digit<D>(key_at<D>(keys, j), L) < q; });
-            differ |= kb != b[q];
+        // is each cut the first particle of its digit value?  (digits are
+        // sorted within the node: one look on each side of the cut decides)
+        bool bad = false;
+        if (lane > 0u && lane < (unsigned)Q) {
+            uint32_t j = b[1];
+#pragma unroll
+            for (int q = 2; q < Q; q++) j = lane == (unsigned)q ? b[q] : j;
+            if (j > a && digit<D>(key_at<D>(keys, j - 1), L) >= lane) bad = true;
+            if (j < e && digit<D>(key_at<D>(keys, j), L) < lane) bad = true;
         }
+        const bool differ = __any_sync(0xffffffffu, bad);
         if (differ)
             for (uint32_t j = a + lane; j < e; j += 32) atomicMin(&t.kxr[j], (uint32_t)L);
     }
@@ -314,7 +342,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     __shared__ float4 s_leaf[kKT];         // leaf masses by the particle that starts the leaf
     __shared__ float4 s_walk[2][kKT];      // masses by level parity, by node within the tile
     __shared__ uint8_t s_done[2][kKT];
-    __shared__ uint8_t s_lam[kKT], s_x[kKT];
+    __shared__ uint8_t s_lam[kKT], s_x[kKT], s_dlb[kKT];
     __shared__ float s_rs[kKT];            // root size of each particle's simulation
     const uint32_t n = (uint32_t)p.n;
     const unsigned tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
@@ -336,6 +364,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     }
     s_lam[tid] = (uint8_t)lam;
     s_x[tid] = (uint8_t)min(X, 255u);
+    s_dlb[tid] = (uint8_t)dlb;
     if (tid == 0) s_maxT = 0u;
     __syncthreads();
     if (tid < NL) {
@@ -421,7 +450,9 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         // a leaf's mass (computeLeafMass): up to the first level-T boundary after a
         if (dl <= T && T == lam && T != X) {
             uint32_t e = a + 1u;
-            while (e < n && t.kdl[e] > T) e++;
+            while (e < w0 + kKT && s_dlb[e - w0] > T) e++;
+            if (e == w0 + kKT)
+                while (e < n && t.kdl[e] > T) e++;
             s_leaf[tid] = leaf_mass<D>(s, a, e);
         }
     }
@@ -440,6 +471,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     const uint32_t dl_next = w0 + kKT < n ? t.kdl[w0 + kKT] : 0u;
     for (int L = (int)s_maxT; L >= 0; --L) {
         const uint32_t first = s_off[L][0], K = s_off[L][W] - first;
+        if (K == 0u) continue;   // no node of this level starts in the tile
         if (tid < K) {
             const uint32_t slot = first + tid;
             // the particle that starts it: the tid-th set bit of the level's ballots
