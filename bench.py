@@ -208,9 +208,9 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-# 2D: box 2, keys 1, sort 5, gather 1, build 1, walk 1; the mixed mode adds the
-# moment pass (2) and the grouping of its group walk (1)
-LAUNCHES_PER_STEP = {"fast": 11, "mixed": 14}
+# 2D: box 2, keys 1, sort 5, gather 1, key-prefix tree passes 5, build 1, walk 1;
+# the mixed mode adds the moment pass (2) and the grouping of its group walk (1)
+LAUNCHES_PER_STEP = {"fast": 16, "mixed": 19}
 
 
 def _err(got, ref):
