@@ -200,17 +200,29 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
             st[(int64_t)tile * kRadix + d] = kFlagInc | sum;
         } else {
             st[(int64_t)tile * kRadix + d] = kFlagAgg | sum;
+            // look back kLookBack tiles per round trip: the words are read at
+            // once and consumed in order up to the first inclusive one (done)
+            // or the first unpublished one (read again from there)
+            constexpr int kLookBack = 8;
             int t = tile - 1;
             uint32_t spins = 0;
-            while (t >= tile0) {
-                const uint32_t word = st[(int64_t)t * kRadix + d];
-                if ((word & ~kValMask) == 0u) {
-                    if (++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
-                    continue;
+            bool done = false;
+            while (!done && t >= tile0) {
+                const int m = min(kLookBack, t - tile0 + 1);
+                uint32_t wd[kLookBack];
+#pragma unroll
+                for (int j = 0; j < kLookBack; j++)
+                    wd[j] = j < m ? st[(int64_t)(t - j) * kRadix + d] : 0u;
+                int j = 0;
+                for (; j < m; j++) {
+                    const uint32_t f = wd[j] & ~kValMask;
+                    if (f == 0u) break;
+                    excl += wd[j] & kValMask;
+                    if (f == kFlagInc) { done = true; break; }
                 }
-                excl += word & kValMask;
-                if ((word & ~kValMask) == kFlagInc) break;
-                --t;
+                if (done) break;
+                t -= j;
+                if (j < m && ++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
             }
             st[(int64_t)tile * kRadix + d] = kFlagInc | ((excl + sum) & kValMask);
         }
