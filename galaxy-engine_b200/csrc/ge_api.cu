@@ -292,6 +292,7 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     t.ktile_cap = (uint32_t)(N / kKeyTile + 1);
     GE_CHECK(c, dalloc(L, &t.ktile, (size_t)t.ktile_cap * 22));
     GE_CHECK(c, dalloc(L, &t.kmeta, kKeyMetaWords));
+    GE_CHECK(c, dalloc(L, &t.kdone, N + 1));
     if (temp) {
         GE_CHECK(c, dalloc(L, &t.ntemp, (size_t)node_cap));
         GE_CHECK(c, dalloc(L, &t.tv, N + (size_t)node_cap + 1));

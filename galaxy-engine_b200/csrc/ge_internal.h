@@ -111,6 +111,7 @@ struct Tree {
     uint32_t *ktile;
     uint32_t ktile_cap;
     uint32_t *kmeta;
+    uint32_t *kdone;      // leaves of exact rebuilds whose upward pass is deferred [n + 1]
     int64_t cap;
 };
 

@@ -174,7 +174,8 @@ __device__ __forceinline__ void emit_children(Tree &t, uint32_t k, uint32_t firs
 template <int D, int G>
 __device__ __forceinline__ void split_level_node(const State &s, const StepParams &p, Tree &t,
                                                  uint32_t k, bool valid, uint32_t level_end,
-                                                 uint32_t *lvl_alloc, uint32_t *err) {
+                                                 uint32_t *lvl_alloc, uint32_t *err,
+                                                 bool defer = false) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
@@ -202,7 +203,8 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
     const bool leader = gl == 0;
     if (leader && leaf) {
         put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), cell.w);
-        finish_upward<D>(t, k);
+        if (defer) t.kdone[atomicAdd(&t.kmeta[7], 1u)] = k;   // upward after the rebuilds
+        else finish_upward<D>(t, k);
         atomicMax(&t.meta[kMetaLevels], ax.x + 1u);
     }
     // queue the small subtrees (one atomic per warp)
@@ -289,8 +291,10 @@ __device__ __forceinline__ void rebuild_large_node(const State &s, const StepPar
         const uint32_t c = first + __popc(mask & ((1u << gl) - 1u));
         const uint32_t cnt = b[gl + 1] - b[gl];
         if (is_leaf<D>(p, cnt, half)) {
+            // its upward pass waits for the end of the rebuilds, so that no
+            // level of this loop waits for a chain up the whole tree
             put_walk<D>(t, c, leaf_mass<D>(s, b[gl], b[gl + 1]), half);
-            finish_upward<D>(t, c);
+            t.kdone[atomicAdd(&t.kmeta[7], 1u)] = c;
             atomicMax(&t.meta[kMetaLevels], ax.x + 2u);
         } else if (cnt <= kSmallNode) {
             t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = c;
@@ -779,7 +783,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                     const uint4 ri = __ldcg(&t.info[node]);
                     valid = ri.w - ri.z > kBlockRootMax;
                 }
-                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err);
+                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed);
             }
         } else {
             for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
@@ -790,7 +794,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                     const uint4 ri = __ldcg(&t.info[node]);
                     valid = ri.w - ri.z > kBlockRootMax;
                 }
-                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err);
+                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed);
             }
         }
         grid_barrier(bar_count, bar_gen, err);
@@ -853,15 +857,21 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
     }
     if (keyed) {
-        // the listed nodes (children all final) and upward from them; every
-        // lane climbs on its own and takes the next node when its chain stops
+        // the listed nodes (children all final; then the exact rebuilds'
+        // deferred leaves, already summed) and upward from them; every lane
+        // climbs on its own and takes the next node when its chain stops
         const uint32_t nready = *(volatile uint32_t *)&t.kmeta[5];
-        for (uint32_t idx = gtid; idx < nready; idx += nthreads) {
-            uint32_t cur = __ldcg(&t.slot_of[idx]);
+        const uint32_t ndone = *(volatile uint32_t *)&t.kmeta[7];
+        for (uint32_t idx = gtid; idx < nready + ndone; idx += nthreads) {
+            const bool is_ready = idx < nready;
+            uint32_t cur = is_ready ? __ldcg(&t.slot_of[idx]) : __ldcg(&t.kdone[idx - nready]);
+            bool combine = is_ready;
             while (true) {
                 const uint4 inf = __ldcg(&t.info[cur]);
                 const uint4 ax = __ldcg(&t.aux[cur]);
-                put_walk<D>(t, cur, combine_children<D>(t, inf), __ldcg(&t.cell[cur]).w);
+                if (combine)
+                    put_walk<D>(t, cur, combine_children<D>(t, inf), __ldcg(&t.cell[cur]).w);
+                combine = true;
                 const uint32_t par = ax.z;
                 if (par == kEmpty) break;
                 cuda::atomic_ref<uint32_t, cuda::thread_scope_device> pend(t.pend[par]);
