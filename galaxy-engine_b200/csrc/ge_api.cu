@@ -134,6 +134,9 @@ struct ge_ctx {
     bool tree_valid = false;
     bool keys_valid = false;
     cudaEvent_t ev[8]{};
+    // ge_frame_host: a second stream for the copies that overlap the step
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t xev[3]{};
     ge_stats stats{};
     std::string err;
 };
@@ -806,6 +809,113 @@ int get_host(ge_ctx *c, int64_t off, int64_t n, float *x, float *y, float *z, fl
     return GE_OK;
 }
 
+// ge_frame_host on a context that holds the same single simulation as its
+// last frame: the same upload, step and download, but the masses and ids go
+// up beside the kick, box, keys and sort (they are needed from the
+// permutation on), and the positions, masses and ids come back beside the
+// build and the walk (they are final once permuted); only the velocities and
+// accelerations wait for the walk.  Everything ends synchronised, as the
+// serial path does.
+int frame_overlapped(ge_ctx *c, int64_t n, const float *x, const float *y, const float *z,
+                     const float *vx, const float *vy, const float *vz, const float *ax,
+                     const float *ay, const float *az, const float *m, const uint32_t *id,
+                     float *ox, float *oy, float *oz, float *ovx, float *ovy, float *ovz,
+                     float *oax, float *oay, float *oaz, float *om, uint32_t *oid) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!c->copy_stream) {
+        GE_CHECK(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (auto &e : c->xev) GE_CHECK(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t s0 = c->stream, s1 = c->copy_stream;
+    const int D = c->p.dims;
+    const size_t B = sizeof(float) * (size_t)n;
+    // as ge_upload: pin flags cleared, the simulation restarts its count
+    c->has_pinned = false;
+    c->sims.assign(1, SimRec{c->next_handle++, n, c->total_steps});
+    c->tree_valid = false;
+    c->keys_valid = false;
+    GE_CHECK(c, cudaEventRecord(c->xev[0], s0));   // the copy stream starts after earlier work
+    GE_CHECK(c, cudaStreamWaitEvent(s1, c->xev[0], 0));
+    {
+        const State &s = c->b.st[c->cur];
+        GE_CHECK(c, cudaMemcpyAsync(s.x, x, B, cudaMemcpyHostToDevice, s0));
+        GE_CHECK(c, cudaMemcpyAsync(s.y, y, B, cudaMemcpyHostToDevice, s0));
+        GE_CHECK(c, cudaMemcpyAsync(s.vx, vx, B, cudaMemcpyHostToDevice, s0));
+        GE_CHECK(c, cudaMemcpyAsync(s.vy, vy, B, cudaMemcpyHostToDevice, s0));
+        if (D == 3) {
+            GE_CHECK(c, cudaMemcpyAsync(s.z, z, B, cudaMemcpyHostToDevice, s0));
+            GE_CHECK(c, cudaMemcpyAsync(s.vz, vz, B, cudaMemcpyHostToDevice, s0));
+        }
+        const float *acc[3] = {ax, ay, az};
+        float *dacc[3] = {s.ax, s.ay, s.az};
+        for (int a = 0; a < D; a++) {
+            if (acc[a]) GE_CHECK(c, cudaMemcpyAsync(dacc[a], acc[a], B, cudaMemcpyHostToDevice, s0));
+            else GE_CHECK(c, cudaMemsetAsync(dacc[a], 0, B, s0));
+        }
+        if (c->b.prev) {
+            GE_CHECK(c, cudaMemcpyAsync(s.pvx, s.vx, B, cudaMemcpyDeviceToDevice, s0));
+            GE_CHECK(c, cudaMemcpyAsync(s.pvy, s.vy, B, cudaMemcpyDeviceToDevice, s0));
+            if (D == 3) GE_CHECK(c, cudaMemcpyAsync(s.pvz, s.vz, B, cudaMemcpyDeviceToDevice, s0));
+        }
+        if (c->b.pinned) GE_CHECK(c, cudaMemsetAsync(s.pinned, 0, (size_t)n, s0));
+        if (s.temp) GE_CHECK(c, cudaMemsetAsync(s.temp, 0, B, s0));
+        if (s.kx) {
+            float *kp[6] = {s.kx, s.ky, s.kz, s.kvx, s.kvy, s.kvz};
+            for (float *q : kp)
+                if (q) GE_CHECK(c, cudaMemsetAsync(q, 0, B, s0));
+        }
+        GE_CHECK(c, cudaMemcpyAsync(s.m, m, B, cudaMemcpyHostToDevice, s1));
+        GE_CHECK(c, cudaMemcpyAsync(s.id, id, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s1));
+        GE_CHECK(c, cudaEventRecord(c->xev[1], s1));
+    }
+    GE_CHECK(c, cudaEventRecord(c->ev[6], s0));
+    if ((rc = enqueue_bbox(c, true)) || (rc = enqueue_keys(c)) || (rc = enqueue_sort(c))) return rc;
+    GE_CHECK(c, cudaStreamWaitEvent(s0, c->xev[1], 0));
+    if ((rc = enqueue_permute(c, false))) return rc;
+    GE_CHECK(c, cudaEventRecord(c->xev[2], s0));
+    GE_CHECK(c, cudaStreamWaitEvent(s1, c->xev[2], 0));
+    {
+        const State &s = c->b.st[c->cur];   // permuted
+        GE_CHECK(c, cudaMemcpyAsync(ox, s.x, B, cudaMemcpyDeviceToHost, s1));
+        GE_CHECK(c, cudaMemcpyAsync(oy, s.y, B, cudaMemcpyDeviceToHost, s1));
+        if (D == 3 && oz) GE_CHECK(c, cudaMemcpyAsync(oz, s.z, B, cudaMemcpyDeviceToHost, s1));
+        if (om) GE_CHECK(c, cudaMemcpyAsync(om, s.m, B, cudaMemcpyDeviceToHost, s1));
+        if (oid) GE_CHECK(c, cudaMemcpyAsync(oid, s.id, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s1));
+    }
+    if ((rc = enqueue_build(c, true)) || (rc = enqueue_walk(c, true))) return rc;
+    GE_CHECK(c, cudaEventRecord(c->ev[7], s0));
+    {
+        const State &s = c->b.st[c->cur];
+        float *h[6] = {ovx, ovy, ovz, oax, oay, oaz};
+        const float *dv[6] = {s.vx, s.vy, s.vz, s.ax, s.ay, s.az};
+        for (int q = 0; q < 6; q++)
+            if (h[q] && (D == 3 || (q % 3) != 2))
+                GE_CHECK(c, cudaMemcpyAsync(h[q], dv[q], B, cudaMemcpyDeviceToHost, s0));
+    }
+    GE_CHECK(c, cudaStreamSynchronize(s1));
+    // as ge_step_wait for one step (check_device synchronises the compute stream)
+    rc = check_device(c);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+    c->stats.ms_last_step = ms;
+    c->stats.steps += 1;
+    c->total_steps += 1;
+    c->tree_valid = rc == GE_OK;
+    if (rc == GE_OK && c->count_inter) {
+        unsigned long long v = 0;
+        GE_CHECK(c, cudaMemcpy(&v, c->b.d_inter, sizeof(v), cudaMemcpyDeviceToHost));
+        c->stats.interactions = v;
+    }
+    return rc;
+}
+
+int frame_overlapped(ge_ctx *c, int64_t n, float *x, float *y, float *z, float *vx, float *vy,
+                     float *vz, float *ax, float *ay, float *az, float *m, uint32_t *id) {
+    return frame_overlapped(c, n, x, y, z, vx, vy, vz, ax, ay, az, m, id, x, y, z, vx, vy, vz, ax,
+                            ay, az, m, id);
+}
+
 int find_sim(ge_ctx *c, int32_t handle) {
     for (size_t k = 0; k < c->sims.size(); k++)
         if (c->sims[k].handle == handle) return (int)k;
@@ -878,6 +988,11 @@ int ge_destroy(ge_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_buffers(c);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    for (auto &e : c->xev) if (e) cudaEventDestroy(e);
     if (c->h_meta) cudaFreeHost(c->h_meta);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1155,6 +1270,11 @@ int ge_profile_step(ge_ctx *c) {
 int ge_frame_host(ge_ctx *c, int64_t n, float *x, float *y, float *z, float *vx, float *vy,
                   float *vz, float *ax, float *ay, float *az, float *m, uint32_t *id) {
     if (!c) return GE_ERR_ARG;
+    const bool d3 = c->p.dims == 3;
+    // the same one simulation as the last frame: copies overlap the step
+    if (c->n == n && n > 0 && c->sims.size() == 1 && !c->pending_steps && id && x && y && vx &&
+        vy && m && (!d3 || (z && vz)))
+        return frame_overlapped(c, n, x, y, z, vx, vy, vz, ax, ay, az, m, id);
     int rc = ge_upload(c, n, x, y, z, vx, vy, vz, m, id, ax, ay, az);
     if (rc) return rc;
     if ((rc = ge_step(c, 1))) return rc;
