@@ -883,16 +883,46 @@ int frame_overlapped(ge_ctx *c, int64_t n, const float *x, const float *y, const
         if (om) GE_CHECK(c, cudaMemcpyAsync(om, s.m, B, cudaMemcpyDeviceToHost, s1));
         if (oid) GE_CHECK(c, cudaMemcpyAsync(oid, s.id, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s1));
     }
-    if ((rc = enqueue_build(c, true)) || (rc = enqueue_walk(c, true))) return rc;
-    GE_CHECK(c, cudaEventRecord(c->ev[7], s0));
+    if ((rc = enqueue_build(c, true))) return rc;
     {
         const State &s = c->b.st[c->cur];
         float *h[6] = {ovx, ovy, ovz, oax, oay, oaz};
         const float *dv[6] = {s.vx, s.vy, s.vz, s.ax, s.ay, s.az};
-        for (int q = 0; q < 6; q++)
-            if (h[q] && (D == 3 || (q % 3) != 2))
-                GE_CHECK(c, cudaMemcpyAsync(h[q], dv[q], B, cudaMemcpyDeviceToHost, s0));
+        auto back = [&](int64_t lo, int64_t hi, cudaStream_t on) -> cudaError_t {
+            for (int q = 0; q < 6; q++)
+                if (h[q] && (D == 3 || (q % 3) != 2)) {
+                    const cudaError_t e = cudaMemcpyAsync(h[q] + lo, dv[q] + lo,
+                                                          sizeof(float) * (size_t)(hi - lo),
+                                                          cudaMemcpyDeviceToHost, on);
+                    if (e != cudaSuccess) return e;
+                }
+            return cudaSuccess;
+        };
+        if (group_walk_on(c) || c->any_direct || c->count_inter) {
+            if ((rc = enqueue_walk(c, true))) return rc;
+            GE_CHECK(c, back(0, n, s0));
+        } else {
+            // the per-particle walk in particle ranges: each range's velocities and
+            // accelerations go back while the next range walks
+            constexpr int kParts = 4;
+            StepParams p = step_params(c);
+            State ws = cur_state(c);
+            if (!c->p.temp_enabled) ws.temp = nullptr;
+            for (int part = 0; part < kParts; part++) {
+                const int64_t lo = (n * part / kParts) & ~int64_t(255);
+                const int64_t hi = part + 1 == kParts ? n : (n * (part + 1) / kParts) & ~int64_t(255);
+                if (hi <= lo) continue;
+                p.i0 = (int)lo;
+                p.n = (int)hi;
+                GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, ws, p, c->g, mixed_view(c), true,
+                                        nullptr, c->d_err, s0));
+                GE_CHECK(c, cudaEventRecord(c->xev[2], s0));
+                GE_CHECK(c, cudaStreamWaitEvent(s1, c->xev[2], 0));
+                GE_CHECK(c, back(lo, hi, s1));
+            }
+        }
     }
+    GE_CHECK(c, cudaEventRecord(c->ev[7], s0));
     GE_CHECK(c, cudaStreamSynchronize(s1));
     // as ge_step_wait for one step (check_device synchronises the compute stream)
     rc = check_device(c);

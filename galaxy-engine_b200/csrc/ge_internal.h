@@ -166,6 +166,7 @@ struct StepParams {
     int group_size;   // GE_PREC_MIXED: 0 = per-particle walk, else the group walk
     float heat_cond;  // heat exchange coefficient (used when State::temp is set)
     float direct_eps2;   // value the direct sum adds to r^2
+    int i0;              // the per-particle walk: first particle (up to n), 0 by default
 };
 
 constexpr int kBBoxThreads = 256;

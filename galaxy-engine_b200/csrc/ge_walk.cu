@@ -71,7 +71,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
     const float4 *__restrict__ src = t.src;
     const int n = p.n;
     const float eps2 = p.eps2, th2 = p.theta2, G = p.G;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = p.i0 + blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_count = 0;
     // particles of simulations that take the direct sum are left to it
     const bool walks = i < n && !(g.direct && __ldg(&g.direct[g.seg_of ? __ldg(&g.seg_of[i]) : 0u]));
@@ -229,7 +229,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
 template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS, bool TEMP = false>
 static cudaError_t walk_one(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    const int blocks = (p.n + kWalkThreads - 1) / kWalkThreads;
+    const int blocks = (p.n - p.i0 + kWalkThreads - 1) / kWalkThreads;
     k_walk<D, MODE, COUNT, PER, POS_EPS, TEMP>
         <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, g, t, ie, inter, err);
     return cudaGetLastError();
