@@ -24,9 +24,9 @@
 namespace ge {
 
 constexpr int kRadix = 256;
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kItems = kSortTile / kSortThreads;  // 16
+constexpr int kItems = kSortTile / kSortThreads;  // 8
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1;
 
 __host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 5 : 8; }
@@ -144,7 +144,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     const int tile0 = g.tile_base ? (int)g.tile_base[sg] : 0;
     const uint32_t lo = seg_lo(g, sg), hi = seg_hi(g, sg, (uint32_t)n);
     // exclusive scan of this segment's digit counts (thread = digit)
-    const uint32_t gcount = hist[(size_t)sg * kRadix + tid];
+    const uint32_t gcount = tid < kRadix ? hist[(size_t)sg * kRadix + tid] : 0u;
     uint32_t incl = gcount;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -185,7 +185,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     }
     __syncthreads();
     // per digit: exclusive prefix over warps and the tile total
-    {
+    if (tid < kRadix) {
         const int d = tid;
         uint32_t sum = 0;
 #pragma unroll

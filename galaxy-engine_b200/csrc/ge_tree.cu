@@ -857,27 +857,28 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
     }
     if (keyed) {
-        // the listed nodes (children all final; then the exact rebuilds'
-        // deferred leaves, already summed) and upward from them; every lane
-        // climbs on its own and takes the next node when its chain stops
+        // the listed nodes (children all final) and the exact rebuilds'
+        // deferred leaves (already summed), upward from each: a warp takes 32
+        // at a time from a counter, so the warps that drew no small subtree
+        // above start at once and the climbs overlap the subtrees' own
         const uint32_t nready = *(volatile uint32_t *)&t.kmeta[5];
-        const uint32_t ndone = *(volatile uint32_t *)&t.kmeta[7];
-        for (uint32_t idx = gtid; idx < nready + ndone; idx += nthreads) {
-            const bool is_ready = idx < nready;
-            uint32_t cur = is_ready ? __ldcg(&t.slot_of[idx]) : __ldcg(&t.kdone[idx - nready]);
-            bool combine = is_ready;
-            while (true) {
-                const uint4 inf = __ldcg(&t.info[cur]);
-                const uint4 ax = __ldcg(&t.aux[cur]);
-                if (combine)
-                    put_walk<D>(t, cur, combine_children<D>(t, inf), __ldcg(&t.cell[cur]).w);
-                combine = true;
-                const uint32_t par = ax.z;
-                if (par == kEmpty) break;
-                cuda::atomic_ref<uint32_t, cuda::thread_scope_device> pend(t.pend[par]);
-                if (pend.fetch_sub(1u, cuda::memory_order_acq_rel) != 1u) break;
-                cur = par;
+        const uint32_t total = nready + *(volatile uint32_t *)&t.kmeta[7];
+        uint32_t *take = &t.kmeta[kKeyMetaWords - 1];   // zeroed with the key passes' words
+        while (true) {
+            uint32_t b = 0;
+            if (lane == 0) b = atomicAdd(take, 32u);
+            b = __shfl_sync(0xffffffffu, b, 0);
+            if (b >= total) break;
+            const uint32_t idx = b + lane;
+            if (idx < nready) {
+                const uint32_t cur = __ldcg(&t.slot_of[idx]);
+                put_walk<D>(t, cur, combine_children<D>(t, __ldcg(&t.info[cur])),
+                            __ldcg(&t.cell[cur]).w);
+                finish_upward<D>(t, cur);
+            } else if (idx < total) {
+                finish_upward<D>(t, __ldcg(&t.kdone[idx - nready]));
             }
+            __syncwarp();
         }
     }
     grid_barrier(bar_count, bar_gen, err);
