@@ -210,7 +210,7 @@ def run_reference(args, world, rank):
 
 # 2D: box 2, keys 1, sort 5, gather 1, key-prefix tree passes 5, build 1, walk 1;
 # the mixed mode adds the moment pass (2) and the grouping of its group walk (1)
-LAUNCHES_PER_STEP = {"fast": 16, "mixed": 19}
+LAUNCHES_PER_STEP = {"fast": 15, "mixed": 18}
 
 
 def _err(got, ref):

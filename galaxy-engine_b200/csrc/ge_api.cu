@@ -98,7 +98,6 @@ cudaError_t dalloc(AllocList &L, T **p, size_t count) {
     return cudaSuccess;
 }
 
-constexpr int kMaxPasses = 8;   // radix passes of the 3D keys (2D uses 5)
 
 }  // namespace gehost
 
@@ -482,8 +481,8 @@ int alloc_segs(ge_ctx *c, SegBuffers &nb, int64_t seg_cap, int64_t n_cap, int64_
     GE_CHECK(c, dalloc(L, &nb.boxmm, 6 * SC));
     GE_CHECK(c, dalloc(L, &nb.root_begin, SC));
     GE_CHECK(c, dalloc(L, &nb.root_end, SC));
-    GE_CHECK(c, dalloc(L, &nb.hist, (size_t)kMaxPasses * SC * 256));
-    GE_CHECK(c, dalloc(L, &nb.status, (size_t)kMaxPasses * TC * 256));
+    GE_CHECK(c, dalloc(L, &nb.hist, (size_t)kSortDigitWords * SC));
+    GE_CHECK(c, dalloc(L, &nb.status, (size_t)kSortDigitWords * TC));
     nb.dtile_cap = nb.n_cap / kDirectTile + nb.seg_cap + 1;
     GE_CHECK(c, dalloc(L, &nb.dtiles, (size_t)nb.dtile_cap));
     GE_CHECK(c, dalloc(L, &nb.dflag, SC));

@@ -149,8 +149,8 @@ __host__ __device__ __forceinline__ uint32_t seg_hi(const Segs &g, uint32_t s, u
 struct SortScratch {
     uint64_t *keys[2];     // 2D: (key << 28 | index) packed; 3D: keys
     uint32_t *vals[2];     // 3D: indices
-    uint32_t *hist;        // [passes][S][256] per-segment digit counts
-    uint32_t *status;      // [passes][tiles][256] decoupled look-back words
+    uint32_t *hist;        // [passes][S][radix] per-segment digit counts
+    uint32_t *status;      // [passes][tiles][radix] decoupled look-back words
     uint32_t *tile_ctr;    // [8]
     int box_blocks;        // grid of the kick/box kernel
 };
@@ -170,7 +170,8 @@ struct StepParams {
 };
 
 constexpr int kBBoxThreads = 256;
-constexpr int kSortTile = 4096;   // keys per look-back tile (256 threads x 16)
+constexpr int kSortTile = 4096;   // keys per look-back tile (512 threads x 8)
+constexpr int kSortDigitWords = 7 * 512;   // hist / status words per segment / tile (3D keys)
 constexpr int kTimeline = 256;    // build timeline entries
 constexpr int kDirectTile = 128;  // particles per block of the direct sum
 
@@ -196,9 +197,9 @@ cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScra
 // ss.keys[0] (and vals[0])
 cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_t *err,
                         cudaStream_t st);
-// stable radix passes over bits [shift0, shift0 + 8 * passes) of the 64-bit
-// words in words[0] (one range, no segments); digit histograms in hist
-// [passes][256]; *result = the buffer that holds the sorted words
+// stable radix passes of 8-bit digits over bits [shift0, shift0 + 8 * passes)
+// of the 64-bit words in words[0] (one range, no segments); digit histograms
+// in hist [passes][256]; *result = the buffer that holds the sorted words
 cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int passes,
                                const uint32_t *hist, uint32_t *status, uint32_t *tile_ctr,
                                uint32_t *err, int *result, cudaStream_t st);

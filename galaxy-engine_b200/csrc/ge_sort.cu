@@ -11,6 +11,8 @@
 // 2D keys use 36 bits.  They are packed with the particle's current index as
 // (key << 28) | index, so each pass moves one 8-byte word per particle
 // (N < 2^28).  3D keys use 63 bits and travel with a separate 32-bit index.
+// Digits are 9 bits wide: 4 passes in 2D, 7 in 3D.  The other callers' words
+// (the SPH grid's) sort by 8-bit digits.
 //
 // Each pass is one kernel: a tile of 4096 keys is ranked in shared memory
 // (warp-private digit counters, __match_any_sync for the ranks of equal
@@ -23,13 +25,18 @@
 
 namespace ge {
 
-constexpr int kRadix = 256;
+constexpr int kKeyBits = 9;                  // digit width of the Morton key passes
+constexpr int kKeyRadix = 1 << kKeyBits;
+constexpr int kWordBits = 8;                 // digit width of launch_radix_words
 constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kItems = kSortTile / kSortThreads;  // 8
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1;
 
-__host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 5 : 8; }
+__host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 4 : 7; }
+static_assert(4 * kKeyBits == 36 && 7 * kKeyBits == 63, "passes cover the key bits");
+static_assert(7 * kKeyRadix <= kSortDigitWords, "hist / status words per segment / tile");
+static_assert(kKeyRadix <= kSortThreads, "one thread per digit");
 __host__ __device__ constexpr int key_shift0(int dims) { return dims == 2 ? 28 : 0; }
 
 // Morton keys of every particle from its segment's root box, and the digit
@@ -41,11 +48,11 @@ template <int D>
 __global__ void __launch_bounds__(256)
 k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
        uint32_t *status, int64_t status_words, uint32_t *tile_ctr) {
-    constexpr int P = key_passes(D), S0 = key_shift0(D);
-    __shared__ uint32_t sh[P][kRadix];
+    constexpr int P = key_passes(D), S0 = key_shift0(D), R = kKeyRadix;
+    __shared__ uint32_t sh[P][R];
     const int lane = threadIdx.x & 31;
-    const size_t SH = (size_t)g.S * kRadix;   // stride of one pass in hist
-    for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+    const size_t SH = (size_t)g.S * R;   // stride of one pass in hist
+    for (int i = threadIdx.x; i < P * R; i += blockDim.x) (&sh[0][0])[i] = 0;
     // clear the look-back status words for this step's passes
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < status_words;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -67,12 +74,12 @@ k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
         if (uni && (int)s_first != cur) {
             __syncthreads();
             if (cur >= 0)
-                for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) {
+                for (int k = threadIdx.x; k < P * R; k += blockDim.x) {
                     const uint32_t c = (&sh[0][0])[k];
-                    if (c) atomicAdd(&hist[(k / kRadix) * SH + (size_t)cur * kRadix + (k % kRadix)], c);
+                    if (c) atomicAdd(&hist[(k / R) * SH + (size_t)cur * R + (k % R)], c);
                 }
             __syncthreads();
-            for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) (&sh[0][0])[k] = 0;
+            for (int k = threadIdx.x; k < P * R; k += blockDim.x) (&sh[0][0])[k] = 0;
             __syncthreads();
             cur = (int)s_first;
         }
@@ -103,48 +110,50 @@ k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
         }
 #pragma unroll
         for (int ps = 0; ps < P; ps++) {
-            const uint32_t d = ok ? (uint32_t)((word >> (S0 + 8 * ps)) & 0xFFu) : 0x100u;
+            const uint32_t d = ok ? (uint32_t)((word >> (S0 + kKeyBits * ps)) & (R - 1)) : (uint32_t)R;
             if (uni) {
                 const unsigned peers = __match_any_sync(0xffffffffu, d);
                 if (ok && lane == __ffs(peers) - 1) atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
             } else {
-                const unsigned peers = __match_any_sync(0xffffffffu, ok ? (sg << 8) | d : 0xFFFFFFFFu);
+                const unsigned peers = __match_any_sync(
+                    0xffffffffu, ok ? ((uint64_t)sg << 16) | d : ~0ull);
                 if (ok && lane == __ffs(peers) - 1)
-                    atomicAdd(&hist[ps * SH + (size_t)sg * kRadix + d], (uint32_t)__popc(peers));
+                    atomicAdd(&hist[ps * SH + (size_t)sg * R + d], (uint32_t)__popc(peers));
             }
         }
     }
     __syncthreads();
     if (cur >= 0)
-        for (int k = threadIdx.x; k < P * kRadix; k += blockDim.x) {
+        for (int k = threadIdx.x; k < P * R; k += blockDim.x) {
             const uint32_t c = (&sh[0][0])[k];
-            if (c) atomicAdd(&hist[(k / kRadix) * SH + (size_t)cur * kRadix + (k % kRadix)], c);
+            if (c) atomicAdd(&hist[(k / R) * SH + (size_t)cur * R + (k % R)], c);
         }
 }
 
-// One stable counting pass over digit (word >> shift) & 255, segment by
-// segment: a tile belongs to one segment, its digit offsets start at the
+// One stable counting pass over digit (word >> shift) & (2^BITS - 1), segment
+// by segment: a tile belongs to one segment, its digit offsets start at the
 // segment's first slot, and look-back stops at the segment's first tile.
-template <bool PAIRS>
+template <bool PAIRS, int BITS>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
              const uint32_t *__restrict__ vin, uint32_t *__restrict__ vout, int n, int shift,
              Segs g, const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
              uint32_t *err) {
-    __shared__ uint32_t s_whist[kSortWarps][kRadix];
-    __shared__ uint32_t s_off[kRadix];
+    constexpr int R = 1 << BITS;
+    __shared__ uint32_t s_whist[kSortWarps][R];
+    __shared__ uint32_t s_off[R];
     __shared__ uint32_t s_scan[kSortWarps];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
-    for (int i = tid; i < kSortWarps * kRadix; i += kSortThreads) (&s_whist[0][0])[i] = 0u;
+    for (int i = tid; i < kSortWarps * R; i += kSortThreads) (&s_whist[0][0])[i] = 0u;
     __syncthreads();
     const int tile = (int)s_tile;
     const uint32_t sg = g.tile_seg ? g.tile_seg[tile] : 0u;
     const int tile0 = g.tile_base ? (int)g.tile_base[sg] : 0;
     const uint32_t lo = seg_lo(g, sg), hi = seg_hi(g, sg, (uint32_t)n);
     // exclusive scan of this segment's digit counts (thread = digit)
-    const uint32_t gcount = tid < kRadix ? hist[(size_t)sg * kRadix + tid] : 0u;
+    const uint32_t gcount = tid < R ? hist[(size_t)sg * R + tid] : 0u;
     uint32_t incl = gcount;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -167,7 +176,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
         const bool ok = idx < (int)hi;
         k[it] = ok ? kin[idx] : 0ull;
         if (PAIRS) v[it] = ok ? vin[idx] : 0u;
-        dg[it] = ok ? (uint32_t)((k[it] >> shift) & 0xFFu) : 0x100u;
+        dg[it] = ok ? (uint32_t)((k[it] >> shift) & (R - 1)) : (uint32_t)R;
     }
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
@@ -175,7 +184,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         uint32_t prev = 0;
         const int leader = __ffs(peers) - 1;
-        if (d < 0x100u && lane == leader) {
+        if (d < (uint32_t)R && lane == leader) {
             prev = s_whist[w][d];
             s_whist[w][d] = prev + (uint32_t)__popc(peers);
         }
@@ -185,7 +194,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     }
     __syncthreads();
     // per digit: exclusive prefix over warps and the tile total
-    if (tid < kRadix) {
+    if (tid < R) {
         const int d = tid;
         uint32_t sum = 0;
 #pragma unroll
@@ -197,9 +206,9 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
         volatile uint32_t *st = status;
         uint32_t excl = 0;
         if (tile == tile0) {
-            st[(int64_t)tile * kRadix + d] = kFlagInc | sum;
+            st[(int64_t)tile * R + d] = kFlagInc | sum;
         } else {
-            st[(int64_t)tile * kRadix + d] = kFlagAgg | sum;
+            st[(int64_t)tile * R + d] = kFlagAgg | sum;
             // look back kLookBack tiles per round trip: the words are read at
             // once and consumed in order up to the first inclusive one (done)
             // or the first unpublished one (read again from there)
@@ -212,7 +221,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
                 uint32_t wd[kLookBack];
 #pragma unroll
                 for (int j = 0; j < kLookBack; j++)
-                    wd[j] = j < m ? st[(int64_t)(t - j) * kRadix + d] : 0u;
+                    wd[j] = j < m ? st[(int64_t)(t - j) * R + d] : 0u;
                 int j = 0;
                 for (; j < m; j++) {
                     const uint32_t f = wd[j] & ~kValMask;
@@ -224,7 +233,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
                 t -= j;
                 if (j < m && ++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
             }
-            st[(int64_t)tile * kRadix + d] = kFlagInc | ((excl + sum) & kValMask);
+            st[(int64_t)tile * R + d] = kFlagInc | ((excl + sum) & kValMask);
         }
         s_off[d] = gexcl + excl;
     }
@@ -232,7 +241,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
         const uint32_t d = dg[it];
-        if (d < 0x100u) {
+        if (d < (uint32_t)R) {
             const uint32_t pos = s_off[d] + s_whist[w][d] + rk[it];
             if (pos < hi) {   // always true unless a look-back wait gave up
                 kout[pos] = k[it];
@@ -289,8 +298,8 @@ static int grid_for(int n, int threads, int cap) {
 cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScratch &ss,
                         cudaStream_t st) {
     const int blocks = grid_for(n, 256, 148 * 8);
-    const int64_t words = (int64_t)key_passes(dims) * g.tiles * kRadix;
-    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kRadix, st);
+    const int64_t words = (int64_t)key_passes(dims) * g.tiles * kKeyRadix;
+    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kKeyRadix, st);
     if (e != cudaSuccess) return e;
     if (dims == 2)
         k_keys<2><<<blocks, 256, 0, st>>>(s, n, g, ss.keys[0], ss.vals[0], ss.hist, ss.status,
@@ -307,16 +316,17 @@ cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_
     const int tiles = (int)g.tiles;
     int cur = 0;
     for (int ps = 0; ps < P; ps++) {
-        uint32_t *status = ss.status + (int64_t)ps * g.tiles * kRadix;
-        const uint32_t *hist = ss.hist + (size_t)ps * g.S * kRadix;
+        uint32_t *status = ss.status + (int64_t)ps * g.tiles * kKeyRadix;
+        const uint32_t *hist = ss.hist + (size_t)ps * g.S * kKeyRadix;
+        const int shift = S0 + kKeyBits * ps;
         if (dims == 2)
-            k_radix_pass<false><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, S0 + 8 * ps, g, hist,
-                status, ss.tile_ctr + ps, err);
+            k_radix_pass<false, kKeyBits><<<tiles, kSortThreads, 0, st>>>(
+                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, shift, g, hist, status,
+                ss.tile_ctr + ps, err);
         else
-            k_radix_pass<true><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, S0 + 8 * ps, g,
-                hist, status, ss.tile_ctr + ps, err);
+            k_radix_pass<true, kKeyBits><<<tiles, kSortThreads, 0, st>>>(
+                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, shift, g, hist,
+                status, ss.tile_ctr + ps, err);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         cur ^= 1;
@@ -336,9 +346,10 @@ cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int 
     const Segs one{};   // a single range [0, n)
     int cur = 0;
     for (int ps = 0; ps < passes; ps++) {
-        k_radix_pass<false><<<(unsigned)(tiles < 1 ? 1 : tiles), kSortThreads, 0, st>>>(
-            words[cur], words[cur ^ 1], nullptr, nullptr, n, shift0 + 8 * ps, one,
-            hist + (size_t)ps * kRadix, status + ps * tiles * kRadix, tile_ctr + ps, err);
+        constexpr int R = 1 << kWordBits;
+        k_radix_pass<false, kWordBits><<<(unsigned)(tiles < 1 ? 1 : tiles), kSortThreads, 0, st>>>(
+            words[cur], words[cur ^ 1], nullptr, nullptr, n, shift0 + kWordBits * ps, one,
+            hist + (size_t)ps * R, status + ps * tiles * R, tile_ctr + ps, err);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         cur ^= 1;
