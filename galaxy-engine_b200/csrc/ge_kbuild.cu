@@ -344,6 +344,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     __shared__ uint8_t s_done[2][kKT];
     __shared__ uint8_t s_lam[kKT], s_x[kKT], s_dlb[kKT];
     __shared__ float s_rs[kKT];            // root size of each particle's simulation
+    __shared__ uint32_t s_cm[NL][kKT / 4]; // child masks of the nodes started in the tile (bytes)
     const uint32_t n = (uint32_t)p.n;
     const unsigned tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
     const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
@@ -362,6 +363,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         const unsigned bb = __ballot_sync(0xffffffffu, dlb <= (uint32_t)L);
         if (lane == 0) { s_bal[L][w] = b; s_bnd[L][w] = bb; }
     }
+    for (int k = tid; k < NL * (kKT / 4); k += kKT) (&s_cm[0][0])[k] = 0u;
     s_lam[tid] = (uint8_t)lam;
     s_x[tid] = (uint8_t)min(X, 255u);
     s_dlb[tid] = (uint8_t)dlb;
@@ -419,7 +421,14 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
                 aux[4 * (size_t)slot + 0] = L;
                 aux[4 * (size_t)slot + 2] = parent;
                 aux[4 * (size_t)slot + 3] = L == X ? 1u : 0u;
-                if (L > 0) atomicOr(&t.pend[parent], 1u << digit<D>(key, (int)L - 1));
+                if (L > 0) {
+                    const uint32_t bit = 1u << digit<D>(key, (int)L - 1);
+                    atomicOr(&t.pend[parent], bit);
+                    // and in the tile's copy when the parent started in the tile
+                    const uint32_t pl = parent - s_off[L - 1][0];
+                    if (parent >= s_off[L - 1][0] && pl < (uint32_t)kKT)
+                        atomicOr(&s_cm[L - 1][pl >> 2], bit << (8u * (pl & 3u)));
+                }
                 if (L == X) {   // exact-rebuild roots have disjoint ranges: fewer than n
                     atomicOr(&t.pend[slot], 1u << 31);
                     const uint32_t r = atomicAdd(&t.kmeta[kKmRoots], 1u);
@@ -497,7 +506,8 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
                         local = bits != 0u;
                     }
                     if (local) {
-                        const uint32_t mask = __ldcg(&t.pend[slot]) & 0xFFu;
+                        // all its children started in the tile: their bits are in s_cm
+                        const uint32_t mask = (s_cm[L][tid >> 2] >> (8u * (tid & 3u))) & 0xFFu;
                         const uint32_t c0 = s_off[L + 1][ww] + (uint32_t)__popc(s_bal[L + 1][ww] & ((1u << ol) - 1u))
                                             - s_off[L + 1][0];   // first child, tile index
                         const int pb = (L + 1) & 1;

@@ -652,6 +652,70 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
     return true;
 }
 
+// The walk-layout entries of node slot k (and of its particles when it is a
+// leaf), from its fields and the end counts C(start) = ez, C(end) = ew.
+template <int D>
+__device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tree &t, uint32_t k,
+                                              uint4 inf, uint4 ax, float4 w, float size2,
+                                              uint32_t ez, uint32_t ew, uint32_t total,
+                                              uint32_t *err) {
+    const uint32_t me = ez + ax.x + inf.z;
+    const uint32_t skip = ew + ax.x - ax.y + inf.w;
+    if (me >= total || skip > total) {   // cannot happen for a consistent tree
+        set_err(err, kErrDepth);
+        return;
+    }
+    t.aux[k].w = me;   // the node's entry (read by the moment pass)
+    if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
+        g.root_begin[k] = me;
+        g.root_end[k] = skip;
+    }
+    const float nm = D == 2 ? w.z : w.w;
+    const bool massless = nm <= 0.0f;
+    if (massless) {
+        // gridMass <= 0: the reference skips the whole subtree.  As a source
+        // it is accepted by every test (size^2 = -2; particles have -1),
+        // carries no mass (the walk makes no interaction with a massless
+        // node) and leads to its successor.
+        t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -2.0f) : make_float4(w.x, w.y, w.z, 0.0f);
+        if (D == 2) ((uint32_t *)t.link)[me] = skip;
+        else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
+    } else {
+        t.src[me] = w;
+        if (D == 2) ((uint32_t *)t.link)[me] = skip;
+        else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(size2));
+    }
+    if (inf.y) return;
+    // a leaf: its particles follow it, four at a time (loads before stores)
+    for (uint32_t j0 = inf.z; j0 < inf.w; j0 += 4u) {
+        float px[4], py[4], pz[4], pm[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t j = j0 + q;
+            const bool in = j < inf.w && !massless;
+            px[q] = in ? s.x[j] : 0.0f;
+            py[q] = in ? s.y[j] : 0.0f;
+            pz[q] = in && D == 3 ? s.z[j] : 0.0f;
+            pm[q] = in ? s.m[j] : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t j = j0 + q;
+            if (j >= inf.w) break;
+            const uint32_t e = me + 1 + (j - inf.z);
+            t.slot_of[j] = e;
+            if (massless) continue;   // never reached by the walk
+            if (D == 2) {
+                t.src[e] = make_float4(px[q], py[q], pm[q], -1.0f);
+                ((uint32_t *)t.link)[e] = e + 1;
+            } else {
+                t.src[e] = make_float4(px[q], py[q], pz[q], pm[q]);
+                ((uint2 *)t.link)[e] = make_uint2(e + 1, __float_as_uint(-1.0f));
+            }
+        }
+    }
+}
+
 template <int D>
 __global__ void __launch_bounds__(kBuildThreads, D == 2 ? 3 : 2)
 k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
@@ -952,50 +1016,30 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     //   subtree successor    = C(end) + level - same_end + end
     //   entry of particle j  = entry of its leaf + 1 + (j - start)
     const uint32_t total = nodes + n;
-    for (uint32_t k = gtid; k < slots; k += nthreads) {
-        const uint4 inf = __ldcg(&t.info[k]);
-        if (inf.w == 0u) continue;   // hole
-        const uint4 ax = __ldcg(&t.aux[k]);
-        const float4 w = __ldcg(&t.walk[k]);
-        const uint32_t me = __ldcg(&t.endcnt[inf.z]) + ax.x + inf.z;
-        const uint32_t skip = __ldcg(&t.endcnt[inf.w]) + ax.x - ax.y + inf.w;
-        if (me >= total || skip > total) {   // cannot happen for a consistent tree
-            set_err(err, kErrDepth);
-            continue;
+    // two slots per round: both slots' loads are issued before either's stores
+    for (uint32_t k0 = gtid; k0 < slots; k0 += 2u * nthreads) {
+        const uint32_t kk[2] = {k0, k0 + nthreads};
+        uint4 inf[2], ax[2];
+        float4 wv[2];
+        float s2[2];
+        uint32_t ez[2], ew[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const bool in = kk[u] < slots;
+            inf[u] = in ? __ldcg(&t.info[kk[u]]) : make_uint4(0u, 0u, 0u, 0u);
+            ax[u] = in ? __ldcg(&t.aux[kk[u]]) : make_uint4(0u, 0u, 0u, 0u);
+            wv[u] = in ? __ldcg(&t.walk[kk[u]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            s2[u] = in && D == 3 ? __ldcg(&t.size2[kk[u]]) : 0.0f;
         }
-        t.aux[k].w = me;   // the node's entry (read by the moment pass)
-        if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
-            g.root_begin[k] = me;
-            g.root_end[k] = skip;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {   // holes have an empty range ending at 0
+            ez[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].z]) : 0u;
+            ew[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].w]) : 0u;
         }
-        const float nm = D == 2 ? w.z : w.w;
-        const bool massless = nm <= 0.0f;
-        if (massless) {
-            // gridMass <= 0: the reference skips the whole subtree.  As a source
-            // it is accepted by every test (size^2 = -2; particles have -1),
-            // carries no mass (the walk makes no interaction with a massless
-            // node) and leads to its successor.
-            t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -2.0f) : make_float4(w.x, w.y, w.z, 0.0f);
-            if (D == 2) ((uint32_t *)t.link)[me] = skip;
-            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
-        } else {
-            t.src[me] = w;
-            if (D == 2) ((uint32_t *)t.link)[me] = skip;
-            else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(__ldcg(&t.size2[k])));
-        }
-        if (!inf.y) {
-            for (uint32_t j = inf.z; j < inf.w; j++) {
-                const uint32_t e = me + 1 + (j - inf.z);
-                t.slot_of[j] = e;
-                if (massless) continue;   // never reached
-                if (D == 2) {
-                    t.src[e] = make_float4(s.x[j], s.y[j], s.m[j], -1.0f);
-                    ((uint32_t *)t.link)[e] = e + 1;
-                } else {
-                    t.src[e] = make_float4(s.x[j], s.y[j], s.z[j], s.m[j]);
-                    ((uint2 *)t.link)[e] = make_uint2(e + 1, __float_as_uint(-1.0f));
-                }
-            }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            if (inf[u].w == 0u) continue;
+            scatter_entry<D>(s, g, t, kk[u], inf[u], ax[u], wv[u], s2[u], ez[u], ew[u], total, err);
         }
     }
 }
