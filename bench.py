@@ -579,7 +579,9 @@ def run_ours(args, world, rank, local):
                      "algorithmic": "18 flop-equivalents (9 FP32 issue slots) per credited interaction"},
         "build_roofline": {"bound": "hbm", "achieved": build_gbs, "peak": hbm_gbs, "unit": "GB/s",
                            "frac": build_gbs / hbm_gbs, "peak_source": peak_src,
-                           "algorithmic": "216 B/particle + 40 B/node (keys, 5 sort passes, gather, nodes)"},
+                           "algorithmic": "216 B/particle + 40 B/node (canonical count: keys, five 8-bit "
+                                          "LSD passes of 24 B, gather, nodes; the sort here runs four "
+                                          "9-bit passes of 16 B)"},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

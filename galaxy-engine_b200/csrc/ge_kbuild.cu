@@ -336,8 +336,9 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
            uint32_t *err) {
     constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32, Q = 1 << D;
     __shared__ uint32_t s_bal[NL][W];      // per level and warp: the particles that start a node
-    __shared__ uint32_t s_bnd[NL][W];      // ... that are level-L boundaries
     __shared__ uint32_t s_off[NL][W + 1];  // slot of each warp's first level-L node; [W] = end
+    __shared__ uint8_t s_start[NL][kKT];   // the particle that starts the tile's j-th level-L node
+    __shared__ uint32_t s_loc[NL][W];      // bit j: that node ends inside the tile
     __shared__ uint32_t s_total, s_maxT;
     __shared__ float4 s_leaf[kKT];         // leaf masses by the particle that starts the leaf
     __shared__ float4 s_walk[2][kKT];      // masses by level parity, by node within the tile
@@ -360,8 +361,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
 #pragma unroll
     for (int L = 0; L < NL; L++) {
         const unsigned b = __ballot_sync(0xffffffffu, dl <= (uint32_t)L && (uint32_t)L <= T);
-        const unsigned bb = __ballot_sync(0xffffffffu, dlb <= (uint32_t)L);
-        if (lane == 0) { s_bal[L][w] = b; s_bnd[L][w] = bb; }
+        if (lane == 0) { s_bal[L][w] = b; s_loc[L][w] = 0u; }
     }
     for (int k = tid; k < NL * (kKT / 4); k += kKT) (&s_cm[0][0])[k] = 0u;
     s_lam[tid] = (uint8_t)lam;
@@ -369,21 +369,25 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
     s_dlb[tid] = (uint8_t)dlb;
     if (tid == 0) s_maxT = 0u;
     __syncthreads();
-    if (tid < NL) {
-        uint32_t base = 0, tot = 0;
-        for (int L = 0; L < NL; L++) {
-            const uint32_t c = t.kmeta[kKmLevelTot + L];
-            if (L < (int)tid) base += c;
-            tot += c;
+    if (w == 0) {   // lane L: level L's slots (NL <= 32)
+        const uint32_t c = lane < (unsigned)NL ? t.kmeta[kKmLevelTot + lane] : 0u;
+        const uint32_t kt = lane < (unsigned)NL ? t.ktile[(size_t)lane * tiles + blockIdx.x] : 0u;
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += u;
         }
-        uint32_t run = base + t.ktile[(size_t)tid * tiles + blockIdx.x];
-        for (int ww = 0; ww < W; ww++) {
-            s_off[tid][ww] = run;
-            run += (uint32_t)__popc(s_bal[tid][ww]);
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane < (unsigned)NL) {
+            uint32_t run = incl - c + kt;
+            for (int ww = 0; ww < W; ww++) {
+                s_off[lane][ww] = run;
+                run += (uint32_t)__popc(s_bal[lane][ww]);
+            }
+            s_off[lane][W] = run;
         }
-        s_off[tid][W] = run;
-        if (tid == 0) s_total = tot;
-        if (blockIdx.x == 0 && tid == 0) t.kmeta[kKmTotal] = tot;
+        if (lane == 0) s_total = tot;
+        if (blockIdx.x == 0 && lane == 0) t.kmeta[kKmTotal] = tot;
     }
     if (valid && dl <= T) atomicMax(&s_maxT, T);
     __syncthreads();
@@ -412,6 +416,7 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
             }
             for (uint32_t L = dl; L <= T; L++) {
                 const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & lt);
+                s_start[L][slot - s_off[L][0]] = (uint8_t)tid;
                 t.cell[slot] = make_float4(cor[0], cor[1], D == 3 ? cor[2] : 0.0f, sz);
                 info[4 * (size_t)slot + 0] =
                     L < T ? s_off[L + 1][w] + (uint32_t)__popc(s_bal[L + 1][w] & lt) : 0u;
@@ -443,18 +448,23 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
                 }
             }
         }
-        // the nodes holding a-1 that end at a
+        // the nodes holding a-1 that end at a (and, when they started in the
+        // tile, their bits in s_loc)
         if (a > 0)
             for (uint32_t L = dl; L <= Tp; L++) {
                 const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & lt) - 1u;
                 info[4 * (size_t)slot + 3] = a;
                 aux[4 * (size_t)slot + 1] = L - dl;
+                const uint32_t j = slot - s_off[L][0];
+                if (slot >= s_off[L][0]) atomicOr(&s_loc[L][j >> 5], 1u << (j & 31u));
             }
         if (a == n - 1)   // the nodes that end at the end of the particle array
             for (uint32_t L = 0; L <= T; L++) {
                 const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & le) - 1u;
                 info[4 * (size_t)slot + 3] = n;
                 aux[4 * (size_t)slot + 1] = L;
+                const uint32_t j = slot - s_off[L][0];
+                if (slot >= s_off[L][0]) atomicOr(&s_loc[L][j >> 5], 1u << (j & 31u));
             }
         // a leaf's mass (computeLeafMass): up to the first level-T boundary after a
         if (dl <= T && T == lam && T != X) {
@@ -483,12 +493,8 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
         if (K == 0u) continue;   // no node of this level starts in the tile
         if (tid < K) {
             const uint32_t slot = first + tid;
-            // the particle that starts it: the tid-th set bit of the level's ballots
-            uint32_t ww = 0;
-            while (ww + 1 < (uint32_t)W && s_off[L][ww + 1] <= slot) ww++;
-            const uint32_t r = slot - s_off[L][ww];
-            const uint32_t ol = (uint32_t)(__fns(s_bal[L][ww], 0u, (int)r + 1));
-            const uint32_t o = ww * 32u + ol;   // tile index of the starting particle
+            const uint32_t o = s_start[L][tid];   // tile index of the starting particle
+            const uint32_t ww = o >> 5, ol = o & 31u;
             bool done = false;
             float4 cm = make_float4(0.f, 0.f, 0.f, 0.f);
             const uint32_t ox = s_x[o];
@@ -497,14 +503,9 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
                     cm = s_leaf[o];
                     done = true;
                 } else {
-                    // inside the tile: the first level-L boundary after o is in it,
-                    // or the next tile's first particle is one
-                    bool local = dl_next <= (uint32_t)L;
-                    for (uint32_t wi = (o + 1u) >> 5; !local && wi < (uint32_t)W; wi++) {
-                        uint32_t bits = s_bnd[L][wi];
-                        if (wi == ((o + 1u) >> 5)) bits &= ~((1u << ((o + 1u) & 31u)) - 1u);
-                        local = bits != 0u;
-                    }
+                    // inside the tile: a particle of the tile ended it, or the
+                    // next tile's first particle is a level-L boundary
+                    const bool local = dl_next <= (uint32_t)L || ((s_loc[L][tid >> 5] >> (tid & 31u)) & 1u);
                     if (local) {
                         // all its children started in the tile: their bits are in s_cm
                         const uint32_t mask = (s_cm[L][tid >> 2] >> (8u * (tid & 3u))) & 0xFFu;
