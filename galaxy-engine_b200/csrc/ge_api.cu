@@ -580,7 +580,7 @@ int sync_segments(ge_ctx *c) {
     }
     c->b.ss.hist = sb.hist;
     c->b.ss.status = sb.status;
-    int64_t bb = (c->n + kBBoxThreads * 16 - 1) / (kBBoxThreads * 16);
+    int64_t bb = (c->n + kBBoxThreads * kBoxItems - 1) / (kBBoxThreads * kBoxItems);
     if (bb > (int64_t)c->num_sms * 4) bb = (int64_t)c->num_sms * 4;
     if (bb < 1) bb = 1;
     c->b.ss.box_blocks = (int)bb;

@@ -16,7 +16,7 @@
 
 namespace ge {
 
-constexpr int kBoxItems = 16;   // particles per thread per block tile
+constexpr int kBoxBatch = 4;    // particles of a thread loaded together, before any store
 
 // float <-> unsigned with the same order (negative floats reversed)
 __device__ __forceinline__ uint32_t f2o(float f) {
@@ -27,13 +27,10 @@ __device__ __forceinline__ float o2f(uint32_t u) {
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
 }
 
+// pos, vel, acc: particle i's, already loaded
 template <int D>
 __device__ __forceinline__ void kick_drift(const State &s, const StepParams &p, int i,
-                                           float *pos) {
-    float vel[3], acc[3];
-    vel[0] = s.vx[i]; vel[1] = s.vy[i];
-    acc[0] = s.ax[i]; acc[1] = s.ay[i];
-    if (D == 3) { vel[2] = s.vz[i]; acc[2] = s.az[i]; }
+                                           float *pos, float *vel, const float *acc) {
     if (s.pvx) {
         s.pvx[i] = vel[0]; s.pvy[i] = vel[1];
         if (D == 3) s.pvz[i] = vel[2];
@@ -90,29 +87,51 @@ k_kick_drift_box(State s, StepParams p, int kick, Segs g) {
         const uint32_t seg0 = g.seg_of ? g.seg_of[base] : 0u;
         const bool one = !g.seg_of || g.seg_of[last] == seg0;
         float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-#pragma unroll 4
-        for (int it = 0; it < kBoxItems; it++) {
-            const uint32_t i = base + it * kBBoxThreads + threadIdx.x;
+#pragma unroll 1
+        for (int it0 = 0; it0 < kBoxItems; it0 += kBoxBatch) {
+          // the batch's loads first: stores to the state arrays would
+          // otherwise keep the next particle's loads behind them
+          float pos[kBoxBatch][3], vel[kBoxBatch][3], acc[kBoxBatch][3];
+          bool mv[kBoxBatch];
+#pragma unroll
+          for (int u = 0; u < kBoxBatch; u++) {
+            const uint32_t i = base + (it0 + u) * kBBoxThreads + threadIdx.x;
+            mv[u] = false;
+            pos[u][0] = pos[u][1] = pos[u][2] = 0.0f;
+            vel[u][0] = vel[u][1] = vel[u][2] = 0.0f;
+            acc[u][0] = acc[u][1] = acc[u][2] = 0.0f;
+            if (i < n) {
+                pos[u][0] = s.x[i]; pos[u][1] = s.y[i];
+                if (D == 3) pos[u][2] = s.z[i];
+                mv[u] = kick && !(s.pinned && s.pinned[i]);
+                if (kick) {
+                    vel[u][0] = s.vx[i]; vel[u][1] = s.vy[i];
+                    acc[u][0] = s.ax[i]; acc[u][1] = s.ay[i];
+                    if (D == 3) { vel[u][2] = s.vz[i]; acc[u][2] = s.az[i]; }
+                }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kBoxBatch; u++) {
+            const uint32_t i = base + (it0 + u) * kBBoxThreads + threadIdx.x;
             if (i >= n) break;
-            float pos[3];
-            pos[0] = s.x[i]; pos[1] = s.y[i];
-            pos[2] = D == 3 ? s.z[i] : 0.0f;
-            if (kick && !(s.pinned && s.pinned[i])) kick_drift<D>(s, p, (int)i, pos);
+            if (mv[u]) kick_drift<D>(s, p, (int)i, pos[u], vel[u], acc[u]);
             if (one) {
 #pragma unroll
                 for (int a = 0; a < D; a++) {
-                    lo[a] = ref_min(lo[a], pos[a]);
-                    hi[a] = ref_max(hi[a], pos[a]);
+                    lo[a] = ref_min(lo[a], pos[u][a]);
+                    hi[a] = ref_max(hi[a], pos[u][a]);
                 }
             } else {
                 // the tile straddles segments: update this particle's segment
                 const uint32_t sg = g.seg_of[i];
 #pragma unroll
                 for (int a = 0; a < D; a++) {
-                    atomicMin(&g.boxmm[sg * 6 + a], f2o(pos[a]));
-                    atomicMax(&g.boxmm[sg * 6 + 3 + a], f2o(pos[a]));
+                    atomicMin(&g.boxmm[sg * 6 + a], f2o(pos[u][a]));
+                    atomicMax(&g.boxmm[sg * 6 + 3 + a], f2o(pos[u][a]));
                 }
             }
+          }
         }
         if (one) {   // uniform across the block
 #pragma unroll

@@ -170,6 +170,7 @@ struct StepParams {
 };
 
 constexpr int kBBoxThreads = 256;
+constexpr int kBoxItems = 8;       // particles per thread per block tile of the kick/box pass
 constexpr int kSortTile = 4096;   // keys per look-back tile (512 threads x 8)
 constexpr int kSortDigitWords = 7 * 512;   // hist / status words per segment / tile (3D keys)
 constexpr int kTimeline = 256;    // build timeline entries

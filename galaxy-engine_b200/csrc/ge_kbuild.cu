@@ -331,7 +331,7 @@ k_key_scan(Tree t, int tiles) {
 // Each particle then writes the few nodes it starts and ends.  Masses follow
 // bottom-up, one thread per node of the tile and level.
 template <int D>
-__global__ void __launch_bounds__(kKT)
+__global__ void __launch_bounds__(kKT, 8)
 k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t, int tiles,
            uint32_t *err) {
     constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32, Q = 1 << D;

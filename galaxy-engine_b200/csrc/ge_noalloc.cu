@@ -31,8 +31,9 @@ constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr size_t kOffKeys0 = 0;
 constexpr size_t kOffKeys1 = kOffKeys0 + align256(sizeof(uint64_t) * kNoAllocMaxN);
 constexpr size_t kOffHist = kOffKeys1 + align256(sizeof(uint64_t) * kNoAllocMaxN);
-constexpr size_t kOffStatus = kOffHist + align256(sizeof(uint32_t) * 8 * 256);
-constexpr size_t kOffTileCtr = kOffStatus + align256(sizeof(uint32_t) * 8 * kNoAllocTiles * 256);
+// digit histograms and look-back words: the sort's words per segment / tile
+constexpr size_t kOffStatus = kOffHist + align256(sizeof(uint32_t) * kSortDigitWords);
+constexpr size_t kOffTileCtr = kOffStatus + align256(sizeof(uint32_t) * kSortDigitWords * kNoAllocTiles);
 constexpr size_t kOffBox = kOffTileCtr + align256(sizeof(uint32_t) * 8);
 constexpr size_t kOffBoxMM = kOffBox + align256(sizeof(float4));
 constexpr size_t kOffRootCell = kOffBoxMM + align256(sizeof(uint32_t) * 6);
@@ -40,7 +41,7 @@ constexpr size_t kOffRootInfo = kOffRootCell + align256(sizeof(float4));
 constexpr size_t kOffErr = kOffRootInfo + align256(sizeof(uint4));
 constexpr size_t kScratchBytes = kOffErr + align256(sizeof(uint32_t));
 
-// All calls on a device share this array (about 4.6 MB).
+// All calls on a device share this array (about 5.1 MB).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;

@@ -251,31 +251,69 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
     }
 }
 
+// Two particles per thread, both gathers issued before either's stores (the
+// stores could alias the next particle's loads, which would keep them apart).
+constexpr int kPermItems = 2;
+
 template <int D>
-__global__ void k_permute(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals,
-                          int n, State in, State out, int with_acc) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        uint32_t j = (D == 2) ? (uint32_t)(keys[k] & 0x0FFFFFFFull) : vals[k];
-        if (j >= (uint32_t)n) j = (uint32_t)k;   // only after a failed sort (error word set)
-        out.x[k] = in.x[j]; out.y[k] = in.y[j];
-        out.vx[k] = in.vx[j]; out.vy[k] = in.vy[j];
-        out.m[k] = in.m[j];
-        out.id[k] = in.id[j];
-        if (D == 3) { out.z[k] = in.z[j]; out.vz[k] = in.vz[j]; }
-        if (with_acc) {
-            out.ax[k] = in.ax[j]; out.ay[k] = in.ay[j];
-            if (D == 3) out.az[k] = in.az[j];
+__global__ void __launch_bounds__(256)
+k_permute(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals, int n, State in,
+          State out, int with_acc) {
+    constexpr int U = kPermItems;
+    const int stride = gridDim.x * blockDim.x * U;
+    for (int k0 = blockIdx.x * blockDim.x * U + threadIdx.x; k0 < n; k0 += stride) {
+        int kk[U];
+        uint32_t j[U];
+        float x[U], y[U], z[U], vx[U], vy[U], vz[U], m[U], ax[U], ay[U], az[U];
+        uint32_t id[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            kk[u] = k0 + u * (int)blockDim.x;
+            j[u] = 0u;
+            if (kk[u] < n) {
+                j[u] = (D == 2) ? (uint32_t)(keys[kk[u]] & 0x0FFFFFFFull) : vals[kk[u]];
+                if (j[u] >= (uint32_t)n) j[u] = (uint32_t)kk[u];   // only after a failed sort (error word set)
+            }
         }
-        if (in.pvx) {
-            out.pvx[k] = in.pvx[j]; out.pvy[k] = in.pvy[j];
-            if (D == 3) out.pvz[k] = in.pvz[j];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (kk[u] >= n) continue;
+            const uint32_t q = j[u];
+            x[u] = in.x[q]; y[u] = in.y[q];
+            vx[u] = in.vx[q]; vy[u] = in.vy[q];
+            m[u] = in.m[q];
+            id[u] = in.id[q];
+            if (D == 3) { z[u] = in.z[q]; vz[u] = in.vz[q]; }
+            if (with_acc) {
+                ax[u] = in.ax[q]; ay[u] = in.ay[q];
+                if (D == 3) az[u] = in.az[q];
+            }
         }
-        if (in.pinned) out.pinned[k] = in.pinned[j];
-        if (in.temp) out.temp[k] = in.temp[j];
-        if (in.kx) {
-            out.kx[k] = in.kx[j]; out.ky[k] = in.ky[j];
-            out.kvx[k] = in.kvx[j]; out.kvy[k] = in.kvy[j];
-            if (D == 3) { out.kz[k] = in.kz[j]; out.kvz[k] = in.kvz[j]; }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = kk[u];
+            if (k >= n) continue;
+            const uint32_t q = j[u];
+            out.x[k] = x[u]; out.y[k] = y[u];
+            out.vx[k] = vx[u]; out.vy[k] = vy[u];
+            out.m[k] = m[u];
+            out.id[k] = id[u];
+            if (D == 3) { out.z[k] = z[u]; out.vz[k] = vz[u]; }
+            if (with_acc) {
+                out.ax[k] = ax[u]; out.ay[k] = ay[u];
+                if (D == 3) out.az[k] = az[u];
+            }
+            if (in.pvx) {
+                out.pvx[k] = in.pvx[q]; out.pvy[k] = in.pvy[q];
+                if (D == 3) out.pvz[k] = in.pvz[q];
+            }
+            if (in.pinned) out.pinned[k] = in.pinned[q];
+            if (in.temp) out.temp[k] = in.temp[q];
+            if (in.kx) {
+                out.kx[k] = in.kx[q]; out.ky[k] = in.ky[q];
+                out.kvx[k] = in.kvx[q]; out.kvy[k] = in.kvy[q];
+                if (D == 3) { out.kz[k] = in.kz[q]; out.kvz[k] = in.kvz[q]; }
+            }
         }
     }
 }
@@ -295,9 +333,24 @@ static int grid_for(int n, int threads, int cap) {
     return b < 1 ? 1 : b;
 }
 
+// Blocks of `threads` that one wave holds on this device (resident blocks per
+// SM x SMs), found once per kernel; 0 if the query fails.
+static int one_wave(const void *kernel, int threads) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess)
+        return 0;
+    return per_sm * sms;
+}
+
 cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScratch &ss,
                         cudaStream_t st) {
-    const int blocks = grid_for(n, 256, 148 * 8);
+    // one wave: every block takes one contiguous chunk of the particles
+    static const int wave[2] = {one_wave((const void *)k_keys<2>, 256),
+                                one_wave((const void *)k_keys<3>, 256)};
+    const int w = wave[dims == 2 ? 0 : 1];
+    const int blocks = grid_for(n, 256, w > 0 ? w : 148 * 4);
     const int64_t words = (int64_t)key_passes(dims) * g.tiles * kKeyRadix;
     cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kKeyRadix, st);
     if (e != cudaSuccess) return e;
@@ -360,7 +413,7 @@ cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int 
 
 cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
                            const State &out, bool with_acc, cudaStream_t st) {
-    int blocks = grid_for(n, 256, 148 * 16);
+    int blocks = grid_for(n, 256 * kPermItems, 148 * 16);
     if (dims == 2)
         k_permute<2><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, in, out, with_acc);
     else

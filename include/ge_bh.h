@@ -323,7 +323,7 @@ int ge_build_timeline(ge_ctx *ctx, int32_t cap, uint64_t *ns, int32_t *count);
  * `stream` is a cudaStream_t (NULL: the legacy default stream).
  *
  * All temporaries live in one fixed-size device array inside the library
- * (about 4.6 MB on every GPU that loads it, held until the process exits), so
+ * (about 5.1 MB on every GPU that loads it, held until the process exits), so
  * n is limited to GE_NOALLOC_MAX_N; larger n returns GE_ERR_CAPACITY without
  * launching anything.  The first call on each device looks up that array's
  * device address (cudaGetSymbolAddress) for the current device; make that
