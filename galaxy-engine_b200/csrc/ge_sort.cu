@@ -15,8 +15,8 @@
 // (the SPH grid's) sort by 8-bit digits.
 //
 // Each pass is one kernel: a tile of 4096 keys is ranked in shared memory
-// (warp-private digit counters, __match_any_sync for the ranks of equal
-// digits), the tile's per-digit counts are published, and the exclusive
+// (warp-private digit counters; the lanes of equal digits found by one ballot
+// per digit bit), the tile's per-digit counts are published, and the exclusive
 // prefix over earlier tiles is found by decoupled look-back on per-tile
 // status words (bounded waits).  Digit histograms of every pass are computed
 // once, by the key kernel.
@@ -34,6 +34,21 @@ constexpr int kItems = kSortTile / kSortThreads;  // 8
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValMask = (1u << 30) - 1;
 
 __host__ __device__ constexpr int key_passes(int dims) { return dims == 2 ? 4 : 7; }
+
+// The lanes whose BITS-bit digit equals this lane's, among the lanes with
+// `valid` set: one ballot per digit bit (the same mask as __match_any_sync
+// over the digits, for valid lanes; an invalid lane's mask is not used).
+template <int BITS>
+__device__ __forceinline__ unsigned digit_peers(uint32_t d, bool valid) {
+    unsigned m = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < BITS; b++) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned bb = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? bb : ~bb;
+    }
+    return m;
+}
 static_assert(4 * kKeyBits == 36 && 7 * kKeyBits == 63, "passes cover the key bits");
 static_assert(7 * kKeyRadix <= kSortDigitWords, "hist / status words per segment / tile");
 static_assert(kKeyRadix <= kSortThreads, "one thread per digit");
@@ -112,8 +127,14 @@ k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
         for (int ps = 0; ps < P; ps++) {
             const uint32_t d = ok ? (uint32_t)((word >> (S0 + kKeyBits * ps)) & (R - 1)) : (uint32_t)R;
             if (uni) {
-                const unsigned peers = __match_any_sync(0xffffffffu, d);
-                if (ok && lane == __ffs(peers) - 1) atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
+                // a warp of one digit (the upper digits of nearly sorted keys)
+                // adds once; the others count by digit groups
+                if (__all_sync(0xffffffffu, d == __shfl_sync(0xffffffffu, d, 0) && ok)) {
+                    if (lane == 0) atomicAdd(&sh[ps][d], 32u);
+                } else {
+                    const unsigned peers = digit_peers<kKeyBits>(d, ok);
+                    if (ok && lane == __ffs(peers) - 1) atomicAdd(&sh[ps][d], (uint32_t)__popc(peers));
+                }
             } else {
                 const unsigned peers = __match_any_sync(
                     0xffffffffu, ok ? ((uint64_t)sg << 16) | d : ~0ull);
@@ -181,7 +202,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
         const uint32_t d = dg[it];
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = digit_peers<BITS>(d, d < (uint32_t)R);
         uint32_t prev = 0;
         const int leader = __ffs(peers) - 1;
         if (d < (uint32_t)R && lane == leader) {
