@@ -233,7 +233,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
             // look back kLookBack tiles per round trip: the words are read at
             // once and consumed in order up to the first inclusive one (done)
             // or the first unpublished one (read again from there)
-            constexpr int kLookBack = 8;
+            constexpr int kLookBack = 2;
             int t = tile - 1;
             uint32_t spins = 0;
             bool done = false;
