@@ -458,6 +458,9 @@ k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tre
                 const uint32_t j = slot - s_off[L][0];
                 if (slot >= s_off[L][0]) atomicOr(&s_loc[L][j >> 5], 1u << (j & 31u));
             }
+        // how many key nodes end at a (and at n): the walk layout's end counts
+        t.endcnt[a] = a > 0 && dl <= Tp ? Tp - dl + 1u : 0u;
+        if (a == n - 1) t.endcnt[n] = T + 1u;
         if (a == n - 1)   // the nodes that end at the end of the particle array
             for (uint32_t L = 0; L <= T; L++) {
                 const uint32_t slot = s_off[L][w] + (uint32_t)__popc(s_bal[L][w] & le) - 1u;

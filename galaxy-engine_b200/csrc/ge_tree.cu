@@ -40,6 +40,7 @@
 namespace ge {
 
 constexpr int kBuildThreads = 256;
+constexpr int kMaxBuildBlocks = 4 * kBuildThreads;   // blocks of the cooperative build (chunk offsets in shared memory)
 constexpr uint32_t kSmallNode = 32;
 
 // meta[] words used by the build
@@ -734,6 +735,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     // the other nodes, counts the children still pending; nodes with none are
     // listed to be combined after the exact rebuilds (phases 1, 2).
     uint32_t lb = 0, le = (uint32_t)g.S, front = (uint32_t)g.S;
+    uint32_t key_nodes = 0;   // keyed: slots [0, key_nodes) hold the key passes' nodes
     const uint32_t *list = nullptr;
     // counters of this build (read only after the first grid barrier)
     if (gtid == 0) {
@@ -743,9 +745,11 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         stamp(t);
     }
     for (uint32_t i = gtid; i < (uint32_t)kMaxLevels + 2u; i += nthreads) t.lvl_alloc[i] = 0u;
-    for (uint32_t i = gtid; i <= n; i += nthreads) t.endcnt[i] = 0u;
+    // keyed: the emit pass wrote the key nodes' end counts (every entry)
+    if (!keyed)
+        for (uint32_t i = gtid; i <= n; i += nthreads) t.endcnt[i] = 0u;
     if (keyed) {
-        const uint32_t key_nodes = *(volatile uint32_t *)&t.kmeta[3];
+        key_nodes = *(volatile uint32_t *)&t.kmeta[3];
         if ((int64_t)key_nodes > t.cap) return;   // the emit pass set kErrNodeCap
         for (uint32_t k = gtid; k < key_nodes; k += nthreads) {
             const uint32_t pv = __ldcg(&t.pend[k]);
@@ -958,20 +962,24 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
 
     // ---- phase 3: depth-first walk layout ------------------------------------
-    // histogram of range ends (endcnt was zeroed before the launch); holes have
-    // an empty range ending at 0 and are skipped
-    for (uint32_t k = gtid; k < slots; k += nthreads) {
+    // histogram of range ends (endcnt was zeroed above, or holds the key
+    // nodes' ends from the emit pass); holes have an empty range ending at 0
+    // and are skipped
+    for (uint32_t k = key_nodes + gtid; k < slots; k += nthreads) {
         const uint32_t e = __ldcg(&t.info[k]).w;
         if (e) atomicAdd(&t.endcnt[e], 1u);
     }
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
-    // inclusive scan of endcnt[0..n] in place: block chunks, then block offsets
+    // inclusive scan of endcnt[0..n] in place, by block chunks; each chunk's
+    // offset (the earlier chunks' total) is added where the scatter reads it:
+    //   C(e) = endcnt[e] + s_boff[e / chunk]
+    __shared__ uint32_t s_boff[kMaxBuildBlocks];
+    const uint32_t chunk = (n + 1 + gridDim.x - 1) / gridDim.x;
     {
         constexpr int W = kBuildThreads / 32;
         __shared__ uint32_t s_w[W];
         const uint32_t total = n + 1;
-        const uint32_t chunk = (total + gridDim.x - 1) / gridDim.x;
         const uint32_t c0 = min(blockIdx.x * chunk, total);
         const uint32_t c1 = min(c0 + chunk, total);
         uint32_t carry = 0;
@@ -997,17 +1005,31 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         if (threadIdx.x == 0) t.blocksum[blockIdx.x] = carry;
         grid_barrier(bar_count, bar_gen, err);
         if (gtid == 0) stamp(t);
-        uint32_t off = 0;
-        for (uint32_t b2 = threadIdx.x; b2 < blockIdx.x; b2 += blockDim.x)
-            off += __ldcg(&t.blocksum[b2]);
-        for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
-        if (lane == 0) s_w[threadIdx.x >> 5] = off;
+        // exclusive prefix of the chunk totals, in every block: thread j sums
+        // chunks [4j, 4j + 4), then a block scan of those sums
+        static_assert(kMaxBuildBlocks == 4 * kBuildThreads, "four chunks per thread");
+        uint32_t v4[4], s4 = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t b2 = 4u * threadIdx.x + q;
+            v4[q] = b2 < gridDim.x ? __ldcg(&t.blocksum[b2]) : 0u;
+            s4 += v4[q];
+        }
+        uint32_t incl = s4;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += u;
+        }
+        if (lane == 31) s_w[threadIdx.x >> 5] = incl;
         __syncthreads();
-        off = 0;
-        for (int w = 0; w < W; w++) off += s_w[w];
-        for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) t.endcnt[i] += off;
-        grid_barrier(bar_count, bar_gen, err);
-        if (gtid == 0) stamp(t);
+        uint32_t run = incl - s4;
+        for (int w = 0; w < (int)(threadIdx.x >> 5); w++) run += s_w[w];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            s_boff[4u * threadIdx.x + q] = run;
+            run += v4[q];
+        }
+        __syncthreads();
     }
     // scatter nodes and the particles of leaves into the walk layout, in which
     // each leaf's particles follow the leaf: with C(e) the number of nodes
@@ -1033,8 +1055,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         }
 #pragma unroll
         for (int u = 0; u < 2; u++) {   // holes have an empty range ending at 0
-            ez[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].z]) : 0u;
-            ew[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].w]) : 0u;
+            ez[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].z]) + s_boff[inf[u].z / chunk] : 0u;
+            ew[u] = inf[u].w ? __ldcg(&t.endcnt[inf[u].w]) + s_boff[inf[u].w / chunk] : 0u;
         }
 #pragma unroll
         for (int u = 0; u < 2; u++) {
@@ -1056,6 +1078,7 @@ int64_t build_node_slack(int dims, int num_sms) {
 int build_grid_blocks(int dims, int num_sms) {
     const int di = dims == 2 ? 0 : 1;
     if (g_build_blocks[di] == 0) {
+        if (num_sms < 1) return 0;
         int per_sm = 0;
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &per_sm, dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
@@ -1064,7 +1087,9 @@ int build_grid_blocks(int dims, int num_sms) {
         // at most three blocks per SM: every block joins every grid barrier, so
         // more blocks lengthen the barriers; more warps hide the latency of
         // the subtree phase
-        g_build_blocks[di] = (per_sm < 3 ? per_sm : 3) * num_sms;
+        int b = (per_sm < 3 ? per_sm : 3) * num_sms;
+        if (b > kMaxBuildBlocks) b = kMaxBuildBlocks - kMaxBuildBlocks % num_sms;
+        g_build_blocks[di] = b;
     }
     return g_build_blocks[di];
 }
