@@ -3,6 +3,11 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// First statement of a kernel launched with launch_dep: wait until the kernel
+// before it in the stream has finished and its writes are visible (a no-op
+// when the launch was an ordinary one).
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 namespace ge {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;

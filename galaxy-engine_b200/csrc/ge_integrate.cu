@@ -78,6 +78,7 @@ __device__ __forceinline__ void kick_drift(const State &s, const StepParams &p, 
 template <int D>
 __global__ void __launch_bounds__(kBBoxThreads)
 k_kick_drift_box(State s, StepParams p, int kick, Segs g) {
+    dep_wait();
     const uint32_t n = (uint32_t)p.n;
     constexpr uint32_t TILE = kBBoxThreads * kBoxItems;
     __shared__ float s_lo[kBBoxThreads / 32][3], s_hi[kBBoxThreads / 32][3];
@@ -163,6 +164,7 @@ k_kick_drift_box(State s, StepParams p, int kick, Segs g) {
 // seeding, and the min/max words reset for the next step.
 template <int D>
 __global__ void k_finalize_boxes(Segs g, Tree t, uint32_t n) {
+    dep_wait();
     const int sgi = blockIdx.x * blockDim.x + threadIdx.x;
     if (sgi >= g.S) return;
     const uint32_t sg = (uint32_t)sgi;
@@ -247,14 +249,14 @@ cudaError_t launch_reset_boxes(const Segs &g, cudaStream_t st) {
 cudaError_t launch_kick_drift_bbox(int dims, const State &s, const StepParams &p, bool kick_drift,
                                    const Segs &g, SortScratch &ss, Tree &t, cudaStream_t st) {
     const int blocks = ss.box_blocks;
-    if (dims == 2) k_kick_drift_box<2><<<blocks, kBBoxThreads, 0, st>>>(s, p, kick_drift, g);
-    else k_kick_drift_box<3><<<blocks, kBBoxThreads, 0, st>>>(s, p, kick_drift, g);
-    cudaError_t e = cudaGetLastError();
+    const int kd = kick_drift ? 1 : 0;
+    cudaError_t e = dims == 2 ? launch_dep(k_kick_drift_box<2>, blocks, kBBoxThreads, st, s, p, kd, g)
+                              : launch_dep(k_kick_drift_box<3>, blocks, kBBoxThreads, st, s, p, kd, g);
     if (e != cudaSuccess) return e;
     const int fb = (g.S + 127) / 128;
-    if (dims == 2) k_finalize_boxes<2><<<fb, 128, 0, st>>>(g, t, (uint32_t)p.n);
-    else k_finalize_boxes<3><<<fb, 128, 0, st>>>(g, t, (uint32_t)p.n);
-    return cudaGetLastError();
+    const uint32_t nn = (uint32_t)p.n;
+    return dims == 2 ? launch_dep(k_finalize_boxes<2>, fb, 128, st, g, t, nn)
+                     : launch_dep(k_finalize_boxes<3>, fb, 128, st, g, t, nn);
 }
 
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st) {

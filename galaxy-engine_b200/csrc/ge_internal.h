@@ -2,11 +2,32 @@
 // C-ABI host code (ge_api.cu) and the kernel files.
 #pragma once
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "ge_bh.h"
 
 namespace ge {
+
+// Launch that may begin while the previous kernel in the stream drains
+// (programmatic dependent launch): its blocks are scheduled early and wait in
+// dep_wait() for the previous kernel's completion, so only the launch latency
+// overlaps.  The kernel must call dep_wait() before touching memory.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dep(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                       Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Particle state, structure-of-arrays, in Morton order.  z/vz/az are unused
 // in 2D.  pvx..pvz (prevVel) and pinned are optional (nullptr).

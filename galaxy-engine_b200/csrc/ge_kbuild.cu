@@ -89,6 +89,7 @@ __device__ __forceinline__ uint32_t key_depth(const Tree &t, uint32_t i) {
 template <int D>
 __global__ void __launch_bounds__(kKT)
 k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t) {
+    dep_wait();
     constexpr int B = KeyBits<D>::B;
     __shared__ int8_t sd[kKT + 2 * kHalo + 1];
     const int n = p.n;
@@ -199,6 +200,7 @@ __device__ __forceinline__ uint32_t group_lower_bound(uint32_t first, uint32_t l
 template <int D>
 __global__ void __launch_bounds__(kKT)
 k_key_check(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t) {
+    dep_wait();
     constexpr int B = KeyBits<D>::B, Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gwarp = (blockIdx.x * kKT + threadIdx.x) >> 5;
@@ -265,6 +267,7 @@ k_key_check(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tr
 template <int D>
 __global__ void __launch_bounds__(kKT)
 k_key_count(StepParams p, Tree t, int tiles) {
+    dep_wait();
     constexpr int NL = KeyBits<D>::B + 1;
     __shared__ uint32_t sc[NL];
     if (threadIdx.x < NL) sc[threadIdx.x] = 0u;
@@ -285,6 +288,7 @@ k_key_count(StepParams p, Tree t, int tiles) {
 template <int D>
 __global__ void __launch_bounds__(1024)
 k_key_scan(Tree t, int tiles) {
+    dep_wait();
     __shared__ uint32_t sw[32];
     __shared__ uint32_t s_carry;
     const int L = blockIdx.x;
@@ -334,6 +338,7 @@ template <int D>
 __global__ void __launch_bounds__(kKT, 8)
 k_key_emit(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tree t, int tiles,
            uint32_t *err) {
+    dep_wait();
     constexpr int B = KeyBits<D>::B, NL = B + 1, W = kKT / 32, Q = 1 << D;
     __shared__ uint32_t s_bal[NL][W];      // per level and warp: the particles that start a node
     __shared__ uint32_t s_off[NL][W + 1];  // slot of each warp's first level-L node; [W] = end
@@ -563,17 +568,12 @@ cudaError_t key_build(const State &s, const StepParams &p, const Segs &g, const 
     cudaError_t e = cudaMemsetAsync(t.kmeta, 0, sizeof(uint32_t) * kKeyMetaWords, st);
     if (e != cudaSuccess) return e;
     const int blocks = (n + kKT - 1) / kKT;
-    k_key_levels<D><<<blocks, kKT, 0, st>>>(s, p, g, keys, t);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_key_check<D><<<num_sms * 4, kKT, 0, st>>>(s, p, g, keys, t);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_dep(k_key_levels<D>, blocks, kKT, st, s, p, g, keys, t)) != cudaSuccess) return e;
+    if ((e = launch_dep(k_key_check<D>, num_sms * 4, kKT, st, s, p, g, keys, t)) != cudaSuccess) return e;
     const int tiles = (n + kKeyTile - 1) / kKeyTile;
-    k_key_count<D><<<tiles, kKT, 0, st>>>(p, t, tiles);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_key_scan<D><<<NL, 1024, 0, st>>>(t, tiles);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_key_emit<D><<<tiles, kKT, 0, st>>>(s, p, g, keys, t, tiles, err);
-    return cudaGetLastError();
+    if ((e = launch_dep(k_key_count<D>, tiles, kKT, st, p, t, tiles)) != cudaSuccess) return e;
+    if ((e = launch_dep(k_key_scan<D>, NL, 1024, st, t, tiles)) != cudaSuccess) return e;
+    return launch_dep(k_key_emit<D>, tiles, kKT, st, s, p, g, keys, t, tiles, err);
 }
 
 }  // namespace

@@ -63,6 +63,7 @@ template <int D>
 __global__ void __launch_bounds__(256)
 k_keys(State s, int n, Segs g, uint64_t *keys, uint32_t *vals, uint32_t *hist,
        uint32_t *status, int64_t status_words, uint32_t *tile_ctr) {
+    dep_wait();
     constexpr int P = key_passes(D), S0 = key_shift0(D), R = kKeyRadix;
     __shared__ uint32_t sh[P][R];
     const int lane = threadIdx.x & 31;
@@ -160,6 +161,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
              const uint32_t *__restrict__ vin, uint32_t *__restrict__ vout, int n, int shift,
              Segs g, const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
              uint32_t *err) {
+    dep_wait();
     constexpr int R = 1 << BITS;
     __shared__ uint32_t s_whist[kSortWarps][R];
     __shared__ uint32_t s_off[R];
@@ -280,6 +282,7 @@ template <int D>
 __global__ void __launch_bounds__(256)
 k_permute(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ vals, int n, State in,
           State out, int with_acc) {
+    dep_wait();
     constexpr int U = kPermItems;
     const int stride = gridDim.x * blockDim.x * U;
     for (int k0 = blockIdx.x * blockDim.x * U + threadIdx.x; k0 < n; k0 += stride) {
@@ -376,12 +379,10 @@ cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScra
     cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kKeyRadix, st);
     if (e != cudaSuccess) return e;
     if (dims == 2)
-        k_keys<2><<<blocks, 256, 0, st>>>(s, n, g, ss.keys[0], ss.vals[0], ss.hist, ss.status,
-                                          words, ss.tile_ctr);
-    else
-        k_keys<3><<<blocks, 256, 0, st>>>(s, n, g, ss.keys[0], ss.vals[0], ss.hist, ss.status,
-                                          words, ss.tile_ctr);
-    return cudaGetLastError();
+        return launch_dep(k_keys<2>, blocks, 256, st, s, n, g, ss.keys[0], ss.vals[0], ss.hist,
+                          ss.status, words, ss.tile_ctr);
+    return launch_dep(k_keys<3>, blocks, 256, st, s, n, g, ss.keys[0], ss.vals[0], ss.hist,
+                      ss.status, words, ss.tile_ctr);
 }
 
 cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_t *err,
@@ -393,15 +394,15 @@ cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_
         uint32_t *status = ss.status + (int64_t)ps * g.tiles * kKeyRadix;
         const uint32_t *hist = ss.hist + (size_t)ps * g.S * kKeyRadix;
         const int shift = S0 + kKeyBits * ps;
-        if (dims == 2)
-            k_radix_pass<false, kKeyBits><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], nullptr, nullptr, n, shift, g, hist, status,
-                ss.tile_ctr + ps, err);
-        else
-            k_radix_pass<true, kKeyBits><<<tiles, kSortThreads, 0, st>>>(
-                ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1], n, shift, g, hist,
-                status, ss.tile_ctr + ps, err);
-        const cudaError_t e = cudaGetLastError();
+        const uint32_t *no_vin = nullptr;
+        uint32_t *no_vout = nullptr;
+        const cudaError_t e =
+            dims == 2 ? launch_dep(k_radix_pass<false, kKeyBits>, tiles, kSortThreads, st,
+                                   ss.keys[cur], ss.keys[cur ^ 1], no_vin, no_vout, n, shift, g,
+                                   hist, status, ss.tile_ctr + ps, err)
+                      : launch_dep(k_radix_pass<true, kKeyBits>, tiles, kSortThreads, st,
+                                   ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1],
+                                   n, shift, g, hist, status, ss.tile_ctr + ps, err);
         if (e != cudaSuccess) return e;
         cur ^= 1;
     }
@@ -435,11 +436,9 @@ cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int 
 cudaError_t launch_permute(int dims, int n, const SortScratch &ss, const State &in,
                            const State &out, bool with_acc, cudaStream_t st) {
     int blocks = grid_for(n, 256 * kPermItems, 148 * 16);
-    if (dims == 2)
-        k_permute<2><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, in, out, with_acc);
-    else
-        k_permute<3><<<blocks, 256, 0, st>>>(ss.keys[0], ss.vals[0], n, in, out, with_acc);
-    return cudaGetLastError();
+    const int wa = with_acc ? 1 : 0;
+    if (dims == 2) return launch_dep(k_permute<2>, blocks, 256, st, ss.keys[0], ss.vals[0], n, in, out, wa);
+    return launch_dep(k_permute<3>, blocks, 256, st, ss.keys[0], ss.vals[0], n, in, out, wa);
 }
 
 cudaError_t launch_perm_out(int dims, int n, const SortScratch &ss, uint32_t *perm,

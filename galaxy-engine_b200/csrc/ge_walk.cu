@@ -65,6 +65,7 @@ template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS, bool TEMP = false
 __global__ void __launch_bounds__(kWalkThreads)
 k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long long *inter,
        uint32_t *err) {
+    dep_wait();
     using LT = typename LinkOf<D>::T;
     constexpr bool kSelfTest = MODE != GE_PREC_FAST || COUNT || !POS_EPS || TEMP;
     const LT *__restrict__ link = (const LT *)t.link;
@@ -230,9 +231,8 @@ template <int D, int MODE, bool COUNT, bool PER, bool POS_EPS, bool TEMP = false
 static cudaError_t walk_one(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                             int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
     const int blocks = (p.n - p.i0 + kWalkThreads - 1) / kWalkThreads;
-    k_walk<D, MODE, COUNT, PER, POS_EPS, TEMP>
-        <<<blocks < 1 ? 1 : blocks, kWalkThreads, 0, st>>>(s, p, g, t, ie, inter, err);
-    return cudaGetLastError();
+    return launch_dep(k_walk<D, MODE, COUNT, PER, POS_EPS, TEMP>, blocks < 1 ? 1 : blocks,
+                      kWalkThreads, st, s, p, g, t, ie, inter, err);
 }
 
 template <int D, int MODE, bool PER>
