@@ -213,6 +213,8 @@ cudaError_t launch_seg_tables(const uint32_t *off, const uint32_t *tile_base, in
                               cudaStream_t st);
 // Morton keys from each segment's root box plus the per-segment digit
 // histograms of every pass
+// count 32-bit words set to zero by a kernel (launched like the step's others)
+cudaError_t launch_zero(uint32_t *w, int64_t count, cudaStream_t st);
 cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScratch &ss,
                         cudaStream_t st);
 // all radix passes (stable within each segment); leaves the sorted keys in

@@ -565,7 +565,7 @@ cudaError_t key_build(const State &s, const StepParams &p, const Segs &g, const 
                       Tree &t, uint32_t *err, int num_sms, cudaStream_t st) {
     constexpr int NL = KeyBits<D>::B + 1;
     const int n = p.n;
-    cudaError_t e = cudaMemsetAsync(t.kmeta, 0, sizeof(uint32_t) * kKeyMetaWords, st);
+    cudaError_t e = launch_zero(t.kmeta, kKeyMetaWords, st);
     if (e != cudaSuccess) return e;
     const int blocks = (n + kKT - 1) / kKT;
     if ((e = launch_dep(k_key_levels<D>, blocks, kKT, st, s, p, g, keys, t)) != cudaSuccess) return e;

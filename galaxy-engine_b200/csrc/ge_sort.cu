@@ -351,6 +351,20 @@ __global__ void k_perm_out(const uint64_t *keys, const uint32_t *vals, int n, ui
     }
 }
 
+__global__ void __launch_bounds__(256) k_zero_words(uint32_t *w, int64_t count) {
+    dep_wait();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x)
+        w[i] = 0u;
+}
+
+cudaError_t launch_zero(uint32_t *w, int64_t count, cudaStream_t st) {
+    if (count < 1) return cudaSuccess;
+    int64_t blocks = (count + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    return launch_dep(k_zero_words, (unsigned)blocks, 256, st, w, count);
+}
+
 static int grid_for(int n, int threads, int cap) {
     int b = (n + threads - 1) / threads;
     if (b > cap) b = cap;
@@ -376,7 +390,7 @@ cudaError_t launch_keys(int dims, const State &s, int n, const Segs &g, SortScra
     const int w = wave[dims == 2 ? 0 : 1];
     const int blocks = grid_for(n, 256, w > 0 ? w : 148 * 4);
     const int64_t words = (int64_t)key_passes(dims) * g.tiles * kKeyRadix;
-    cudaError_t e = cudaMemsetAsync(ss.hist, 0, sizeof(uint32_t) * key_passes(dims) * g.S * kKeyRadix, st);
+    cudaError_t e = launch_zero(ss.hist, (int64_t)key_passes(dims) * g.S * kKeyRadix, st);
     if (e != cudaSuccess) return e;
     if (dims == 2)
         return launch_dep(k_keys<2>, blocks, 256, st, s, n, g, ss.keys[0], ss.vals[0], ss.hist,

@@ -720,6 +720,7 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
 template <int D>
 __global__ void __launch_bounds__(kBuildThreads, D == 2 ? 3 : 2)
 k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
+    dep_wait();
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nthreads = gridDim.x * blockDim.x;
@@ -1106,8 +1107,28 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Se
     uint32_t *ec = err;
     int kc = keyed ? 1 : 0;
     void *args[] = {&sc, &pc, &gc, &tc, &ec, &kc};
-    return cudaLaunchCooperativeKernel(dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>,
-                                       dim3(blocks), dim3(kBuildThreads), args, 0, st);
+    const void *kern = dims == 2 ? (const void *)k_build<2> : (const void *)k_build<3>;
+    // cooperative, and launched while the previous kernel drains (dep_wait);
+    // a runtime that refuses the pair gets the plain cooperative launch
+    static bool pair_ok = true;
+    if (pair_ok) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(blocks);
+        cfg.blockDim = dim3(kBuildThreads);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[2];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 2;
+        const cudaError_t e = cudaLaunchKernelExC(&cfg, kern, args);
+        if (e == cudaSuccess) return e;
+        (void)cudaGetLastError();   // a launch-configuration error is not sticky
+        pair_ok = false;
+    }
+    return cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kBuildThreads), args, 0, st);
 }
 
 }  // namespace ge
