@@ -189,6 +189,7 @@ __device__ __forceinline__ void emit_group(const Tree &t, uint32_t a, uint32_t b
 }
 
 __global__ void k_make_groups(Tree t, uint32_t GS) {
+    dep_wait();
     const uint32_t slots = __ldcg(&t.meta[kMetaSlotsW]);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += stride) {
@@ -229,6 +230,7 @@ template <int D, int PPL, bool COUNT, bool POT = false>
 __global__ void __launch_bounds__(kGWThreads)
 k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
              unsigned long long *inter, uint32_t *err, double *epot = nullptr) {
+    dep_wait();
     __shared__ GWSmem<D> smem[kGWWarps];
     GWSmem<D> &sm = smem[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31u;
@@ -467,16 +469,16 @@ uint32_t group_walk_stack_entries() { return kGWStack; }
 template <int D, int PPL, bool COUNT>
 static cudaError_t gw_launch(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                              int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    k_make_groups<<<grid_blocks(p.n), 256, 0, st>>>(t, 32u * PPL);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_dep(k_make_groups, grid_blocks(p.n), 256, st, t, 32u * PPL);
     if (e != cudaSuccess) return e;
     // one work stack per warp bounds the grid; groups number at most n
     int blocks = (int)(t.wl_warps / kGWWarps);
     const int64_t want = ((int64_t)p.n + kGWWarps - 1) / kGWWarps;
     if (blocks > want) blocks = (int)want;
     if (blocks < 1) blocks = 1;
-    k_group_walk<D, PPL, COUNT><<<blocks, kGWThreads, 0, st>>>(s, p, g, t, ie, inter, err);
-    return cudaGetLastError();
+    double *no_pot = nullptr;
+    return launch_dep(k_group_walk<D, PPL, COUNT>, blocks, kGWThreads, st, s, p, g, t, ie, inter, err,
+                      no_pot);
 }
 
 template <int D>

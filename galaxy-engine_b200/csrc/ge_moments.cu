@@ -33,6 +33,7 @@ constexpr int kMomThreads = 256;
 constexpr int kMetaSlotsWord = 9;   // node slots of the last build (tree meta word)
 
 __global__ void k_pend_init(Tree t) {
+    dep_wait();
     const uint32_t slots = __ldcg(&t.meta[kMetaSlotsWord]);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < slots; k += stride) {
@@ -104,6 +105,7 @@ __device__ __forceinline__ int mom_index(int a, int b) {
 template <int D>
 __global__ void __launch_bounds__(kMomThreads)
 k_moments(State s, Tree t, double inv_theta, uint32_t *err) {
+    dep_wait();
     constexpr int R = MomWords<D>::value;
     const uint32_t slots = __ldcg(&t.meta[kMetaSlotsWord]);
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -192,13 +194,11 @@ k_moments(State s, Tree t, double inv_theta, uint32_t *err) {
 cudaError_t launch_moments(int dims, const State &s, const StepParams &p, Tree &t, uint32_t *err,
                            int num_sms, cudaStream_t st) {
     const int blocks = num_sms * 8;
-    k_pend_init<<<blocks, kMomThreads, 0, st>>>(t);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_dep(k_pend_init, blocks, kMomThreads, st, t);
     if (e != cudaSuccess) return e;
     const double inv_theta = 1.0 / (double)p.theta;   // theta = 0: every node is opened
-    if (dims == 2) k_moments<2><<<blocks, kMomThreads, 0, st>>>(s, t, inv_theta, err);
-    else k_moments<3><<<blocks, kMomThreads, 0, st>>>(s, t, inv_theta, err);
-    return cudaGetLastError();
+    if (dims == 2) return launch_dep(k_moments<2>, blocks, kMomThreads, st, s, t, inv_theta, err);
+    return launch_dep(k_moments<3>, blocks, kMomThreads, st, s, t, inv_theta, err);
 }
 
 }  // namespace ge
