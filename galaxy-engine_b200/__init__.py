@@ -53,7 +53,8 @@ class Params(C.Structure):
         ("size_gate", C.c_float), ("min_size", C.c_float), ("node_cap_factor", C.c_float),
         ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
         ("group_size", C.c_int32), ("temp_enabled", C.c_int32), ("heat_cond", C.c_float),
-        ("direct_below", C.c_int32), ("direct_eps2", C.c_float), ("reserved", C.c_int32 * 2),
+        ("direct_below", C.c_int32), ("direct_eps2", C.c_float), ("no_graph", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -136,6 +136,17 @@ struct ge_ctx {
     // ge_frame_host: a second stream for the copies that overlap the step
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t xev[3]{};
+    // ge_step: two consecutive steps captured as one CUDA graph (every
+    // buffer role is back where it started after two), replayed while the
+    // launches they hold would not change; two kept, by the bytes that
+    // decide those launches (frame_signature)
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uint8_t> sig;
+    } graphs[2];
+    int next_graph = 0;
+    bool graph_failed = false;    // capture or instantiation refused: plain launches
+    bool framed = false;          // a frame was enqueued (one-time launch setup done)
     ge_stats stats{};
     std::string err;
 };
@@ -159,7 +170,16 @@ int cuda_fail(ge_ctx *c, cudaError_t e, const char *where) {
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
     } while (0)
 
+void drop_graphs(ge_ctx *c) {
+    for (auto &g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.sig.clear();
+    }
+}
+
 void free_buffers(ge_ctx *c) {
+    drop_graphs(c);
     free_all(c->b.allocs);
     free_all(c->sb.allocs);
     c->b = Buffers{};
@@ -1184,6 +1204,72 @@ int ge_download_prev_vel(ge_ctx *c, float *pvx, float *pvy, float *pvz) {
     return GE_OK;
 }
 
+// The bytes that decide what enqueue_frame launches and with which
+// arguments: parameters, counts, buffer roles and every device pointer the
+// kernels take.  A graph whose bytes match launches exactly what
+// enqueue_frame would.
+std::vector<uint8_t> frame_signature(const ge_ctx *c) {
+    std::vector<uint8_t> v;
+    v.reserve(1024);
+    auto put = [&](const void *q, size_t nb) {
+        const uint8_t *b = static_cast<const uint8_t *>(q);
+        v.insert(v.end(), b, b + nb);
+    };
+    put(&c->p, sizeof c->p);
+    put(&c->n, sizeof c->n);
+    put(&c->cur, sizeof c->cur);
+    const uint8_t flags[8] = {c->has_pinned, c->any_direct, c->any_walk, c->count_inter,
+                              c->b.prev, c->b.pinned, c->b.temp, c->b.mixed};
+    put(flags, sizeof flags);
+    put(&c->b.st[0], sizeof(State));
+    put(&c->b.st[1], sizeof(State));
+    put(&c->b.ss, sizeof(SortScratch));
+    put(&c->b.tree, sizeof(Tree));
+    put(&c->b.d_inter, sizeof c->b.d_inter);
+    put(&c->g, sizeof(Segs));
+    put(&c->sb.dtiles, sizeof c->sb.dtiles);
+    const size_t nd = c->h_dtiles.size();
+    put(&nd, sizeof nd);
+    put(&c->stream, sizeof c->stream);
+    put(&c->d_err, sizeof c->d_err);
+    put(&c->num_sms, sizeof c->num_sms);
+    return v;
+}
+
+// Capture two steps into graph slot `slot` (nothing runs; the host-side
+// buffer roles, flipped twice, end where they began).  On any refusal the
+// context falls back to plain launches for good.
+void capture_two_frames(ge_ctx *c, int slot, std::vector<uint8_t> sig) {
+    ge_ctx::StepGraph &sg = c->graphs[slot];
+    if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    sg.exec = nullptr;
+    sg.sig.clear();
+    const int cur0 = c->cur;
+    const SortScratch ss0 = c->b.ss;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        c->graph_failed = true;
+        return;
+    }
+    int rc = enqueue_frame(c, nullptr);
+    if (!rc) rc = enqueue_frame(c, nullptr);
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    const bool same = c->cur == cur0 && std::memcmp(&c->b.ss, &ss0, sizeof ss0) == 0;
+    c->cur = cur0;
+    c->b.ss = ss0;
+    if (rc || e != cudaSuccess || !graph || !same ||
+        cudaGraphInstantiate(&sg.exec, graph, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        sg.exec = nullptr;
+        c->graph_failed = true;
+        c->err.clear();
+    } else {
+        sg.sig = std::move(sig);
+    }
+    if (graph) cudaGraphDestroy(graph);
+}
+
 int ge_step_async(ge_ctx *c, int32_t nsteps) {
     int rc = require_state(c);
     if (rc) return rc;
@@ -1191,7 +1277,27 @@ int ge_step_async(ge_ctx *c, int32_t nsteps) {
     if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
     if (nsteps == 0) return GE_OK;
     GE_CHECK(c, cudaEventRecord(c->ev[6], c->stream));
-    for (int k = 0; k < nsteps; k++)
+    int k = 0;
+    if (!c->framed) {   // the first frame plainly: one-time launch setup outside a capture
+        if ((rc = enqueue_frame(c, nullptr))) return rc;
+        c->framed = true;
+        k = 1;
+    }
+    if (nsteps - k >= 2 && !c->p.no_graph && !c->graph_failed) {
+        std::vector<uint8_t> sig = frame_signature(c);
+        int slot = -1;
+        for (int q = 0; q < 2; q++)
+            if (c->graphs[q].exec && c->graphs[q].sig == sig) slot = q;
+        if (slot < 0) {
+            slot = c->next_graph;
+            c->next_graph ^= 1;
+            capture_two_frames(c, slot, std::move(sig));
+        }
+        if (c->graphs[slot].exec)
+            for (; k + 2 <= nsteps; k += 2)
+                GE_CHECK(c, cudaGraphLaunch(c->graphs[slot].exec, c->stream));
+    }
+    for (; k < nsteps; k++)
         if ((rc = enqueue_frame(c, nullptr))) return rc;
     GE_CHECK(c, cudaEventRecord(c->ev[7], c->stream));
     c->pending_steps = nsteps;

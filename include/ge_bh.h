@@ -86,7 +86,9 @@ typedef struct {
                                 GE_PREC_EXACT / GE_PREC_FAST */
     float direct_eps2;       /* value the direct sum adds to r^2: softening, un-squared
                                 in 2D and 3D (physics.cpp:422, physics3D.cpp:455) */
-    int32_t reserved[2];
+    int32_t no_graph;        /* 1: ge_step launches every kernel itself; 0 (default):
+                                pairs of steps replay a captured CUDA graph */
+    int32_t reserved;
 } ge_params;
 
 typedef struct {
