@@ -208,9 +208,10 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-# 2D: box 2, keys 1, sort 5, gather 1, key-prefix tree passes 5, build 1, walk 1;
-# the mixed mode adds the moment pass (2) and the grouping of its group walk (1)
-LAUNCHES_PER_STEP = {"fast": 15, "mixed": 18}
+# 2D: box 2, histogram zeroing 1, keys 1, sort 4, gather 1, key counter zeroing 1,
+# key-prefix tree passes 5, build 1, walk 1; the mixed mode adds the moment pass
+# (2) and the grouping of its group walk (1)
+LAUNCHES_PER_STEP = {"fast": 17, "mixed": 20}
 
 
 def _err(got, ref):
