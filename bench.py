@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision, batched and serving measurements")
     ap.add_argument("--batch-sims", type=int, default=512)
+    ap.add_argument("--precision", default="fast", choices=["fast", "mixed"],
+                    help="the headline workload's mode (mixed: group walk, group 64, leaf 16; "
+                         "for profiling the mixed-mode kernels, not a bench line)")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     return ap.parse_args()
 
@@ -469,8 +472,12 @@ def run_ours(args, world, rank, local):
     ics = importlib.import_module("galaxy-engine_b200.ics")
     n = args.n
     st = workload(ics, n)
-    p = ge.default_params(2, G=1.0, theta=args.theta, softening=SOFT, dt=DT, leaf_cap=LEAF,
-                          precision=ge.PREC_FAST)
+    if args.precision == "mixed":
+        p = ge.default_params(2, G=1.0, theta=args.theta, softening=SOFT, dt=DT, leaf_cap=16,
+                              precision=ge.PREC_MIXED, group_size=64)
+    else:
+        p = ge.default_params(2, G=1.0, theta=args.theta, softening=SOFT, dt=DT, leaf_cap=LEAF,
+                              precision=ge.PREC_FAST)
     stream = torch.cuda.Stream()
     sim = ge.Simulation(p)
     sim.set_stream(stream.cuda_stream)
@@ -558,7 +565,8 @@ def run_ours(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "two-disk 2D Barnes-Hut (plain, one simulation per GPU)",
                    "n": n, "theta": args.theta, "softening": SOFT, "dt": DT,
-                   "leaf_cap": LEAF, "G": 1.0, "precision": "fast",
+                   "leaf_cap": LEAF if args.precision == "fast" else 16, "G": 1.0,
+                   "precision": args.precision,
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
         "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
