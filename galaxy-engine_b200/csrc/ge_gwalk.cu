@@ -43,6 +43,7 @@ struct GWSmem {
     float4 nB[kGWNodes];   // {lo..., Ixx...} as gq0
     float4 nC[D == 3 ? kGWNodes : 1];   // 3D {Iyy, Izz, Ixy, Ixz}
     float nD[kGWNodes];    // 2D Iyy, 3D Iyz
+    float nT[kGWNodes];    // -1.5 tr(I); the second moments in nB..nD are staged x 7.5
     float4 pA[kGWParts];   // {x, y, z, m}
     uint32_t pI[kGWParts]; // particle slot
 };
@@ -64,7 +65,9 @@ struct GroupState {
 };
 
 // accepted nodes: monopole + quadrupole of the softened kernel (with POT,
-// the potential instead: M / r + 1.5 (d.I.d) / r^5 - 0.5 tr(I) / r^3)
+// the potential instead: M / r + 1.5 (d.I.d) / r^5 - 0.5 tr(I) / r^3).  The
+// moments are staged as J = 7.5 I with t = -1.5 tr(I), so that
+//   a = (M / r^3 + (d.J.d / r^2 + t) / r^5) d - 0.4 (J d) / r^5.
 template <int D, int PPL, bool POT = false>
 __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupState<D, PPL> &g,
                                             float eps2, bool count) {
@@ -78,44 +81,44 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
     for (int j = 0; j < nl; j++) {
         const float4 A = sm.nA[j], B = sm.nB[j];
         const float4 C = D == 3 ? sm.nC[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float E = sm.nD[j];
+        const float E = sm.nD[j], tq = sm.nT[j];
         const float m = D == 2 ? A.z : A.w;
-        const float ixx = D == 2 ? B.z : B.w;
-        const float ixy = D == 2 ? B.w : C.z;
-        const float iyy = D == 2 ? E : C.x;
+        const float jxx = D == 2 ? B.z : B.w;
+        const float jxy = D == 2 ? B.w : C.z;
+        const float jyy = D == 2 ? E : C.x;
 #pragma unroll
         for (int k = 0; k < PPL; k++) {
             float d[3];
             d[0] = (A.x - g.x[k][0]) + B.x;
             d[1] = (A.y - g.x[k][1]) + B.y;
             d[2] = D == 3 ? (A.z - g.x[k][2]) + B.z : 0.0f;
-            float rr = d[0] * d[0] + d[1] * d[1] + eps2;
-            if (D == 3) rr += d[2] * d[2];
+            float rr = __fmaf_rn(d[1], d[1], eps2);
+            if (D == 3) rr = __fmaf_rn(d[2], d[2], rr);
+            rr = __fmaf_rn(d[0], d[0], rr);
             const float inv = rsqrt_fast(rr);
-            const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2, inv7 = inv5 * inv2;
-            float Id[3], tr;
+            const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
+            float Jd[3];
             if (D == 2) {
-                Id[0] = ixx * d[0] + ixy * d[1];
-                Id[1] = ixy * d[0] + iyy * d[1];
-                Id[2] = 0.0f;
-                tr = ixx + iyy;
+                Jd[0] = __fmaf_rn(jxx, d[0], jxy * d[1]);
+                Jd[1] = __fmaf_rn(jxy, d[0], jyy * d[1]);
+                Jd[2] = 0.0f;
             } else {
-                const float izz = C.y, ixz = C.w, iyz = E;
-                Id[0] = ixx * d[0] + ixy * d[1] + ixz * d[2];
-                Id[1] = ixy * d[0] + iyy * d[1] + iyz * d[2];
-                Id[2] = ixz * d[0] + iyz * d[1] + izz * d[2];
-                tr = ixx + iyy + izz;
+                const float jzz = C.y, jxz = C.w, jyz = E;
+                Jd[0] = __fmaf_rn(jxx, d[0], __fmaf_rn(jxy, d[1], jxz * d[2]));
+                Jd[1] = __fmaf_rn(jxy, d[0], __fmaf_rn(jyy, d[1], jyz * d[2]));
+                Jd[2] = __fmaf_rn(jxz, d[0], __fmaf_rn(jyz, d[1], jzz * d[2]));
             }
-            float dId = d[0] * Id[0] + d[1] * Id[1];
-            if (D == 3) dId += d[2] * Id[2];
-            if (POT) {
-                pu[k] += m * inv + 1.5f * dId * inv5 - 0.5f * tr * inv3;
+            float dJd = __fmaf_rn(d[1], Jd[1], d[0] * Jd[0]);
+            if (D == 3) dJd = __fmaf_rn(d[2], Jd[2], dJd);
+            if (POT) {   // 1.5 d.I.d = 0.2 d.J.d, -0.5 tr = t / 3
+                pu[k] += m * inv + 0.2f * dJd * inv5 + (tq * (1.0f / 3.0f)) * inv3;
                 continue;
             }
-            const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
-            const float ci = -3.0f * inv5;
+            const float q = __fmaf_rn(dJd, inv2, tq);
+            const float cm = __fmaf_rn(q, inv5, m * inv3);
+            const float ci = -0.4f * inv5;
 #pragma unroll
-            for (int a = 0; a < D; a++) acc[k][a] += cm * d[a] + ci * Id[a];
+            for (int a = 0; a < D; a++) acc[k][a] = __fmaf_rn(ci, Jd[a], __fmaf_rn(cm, d[a], acc[k][a]));
         }
     }
 #pragma unroll
@@ -316,10 +319,23 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
             }
             if (kind == 1) {
                 const int q = nl + __popc(accb & lt);
+                float4 Bq = __ldg(&t.gq0[c]);
+                float4 Cq = D == 3 ? __ldg(&t.gq1[c]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                float Eq = __ldg(&t.gq2[c]).x;
+                // staged for flush_nodes: J = 7.5 I and t = -1.5 tr(I)
+                float tr;
+                if (D == 2) {   // {lo.x, lo.y, Ixx, Ixy}, Iyy
+                    tr = Bq.z + Eq;
+                    Bq.z *= 7.5f; Bq.w *= 7.5f; Eq *= 7.5f;
+                } else {        // {lo.xyz, Ixx}, {Iyy, Izz, Ixy, Ixz}, Iyz
+                    tr = Bq.w + Cq.x + Cq.y;
+                    Bq.w *= 7.5f; Cq.x *= 7.5f; Cq.y *= 7.5f; Cq.z *= 7.5f; Cq.w *= 7.5f; Eq *= 7.5f;
+                }
                 sm.nA[q] = A;
-                sm.nB[q] = __ldg(&t.gq0[c]);
-                if (D == 3) sm.nC[q] = __ldg(&t.gq1[c]);
-                sm.nD[q] = __ldg(&t.gq2[c]).x;
+                sm.nB[q] = Bq;
+                if (D == 3) sm.nC[q] = Cq;
+                sm.nD[q] = Eq;
+                sm.nT[q] = -1.5f * tr;
             }
             nl += __popc(accb);
             // 2. children of opened internal nodes onto the work stack
