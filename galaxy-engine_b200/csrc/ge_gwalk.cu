@@ -39,12 +39,13 @@ constexpr int kMetaSlotsW = 9;         // tree meta word: node slots of the last
 
 template <int D>
 struct GWSmem {
-    float4 nA[kGWNodes];   // 2D {hi.x, hi.y, m, b^2}; 3D {hi.x, hi.y, hi.z, m}
+    float4 nA[kGWNodes];   // 2D {c.x, c.y, m, b^2}; 3D {c.x, c.y, c.z, m}; c = (hi - o) + lo,
+                           // the centre of mass from the group's centre o
     float4 nB[kGWNodes];   // {lo..., Ixx...} as gq0
     float4 nC[D == 3 ? kGWNodes : 1];   // 3D {Iyy, Izz, Ixy, Ixz}
     float nD[kGWNodes];    // 2D Iyy, 3D Iyz
     float nT[kGWNodes];    // -1.5 tr(I); the second moments in nB..nD are staged x 7.5
-    float4 pA[kGWParts];   // {x, y, z, m}
+    float4 pA[kGWParts];   // {x - o, m}
     uint32_t pI[kGWParts]; // particle slot
 };
 
@@ -89,9 +90,9 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
 #pragma unroll
         for (int k = 0; k < PPL; k++) {
             float d[3];
-            d[0] = (A.x - g.x[k][0]) + B.x;
-            d[1] = (A.y - g.x[k][1]) + B.y;
-            d[2] = D == 3 ? (A.z - g.x[k][2]) + B.z : 0.0f;
+            d[0] = A.x - g.x[k][0];
+            d[1] = A.y - g.x[k][1];
+            d[2] = D == 3 ? A.z - g.x[k][2] : 0.0f;
             float rr = __fmaf_rn(d[1], d[1], eps2);
             if (D == 3) rr = __fmaf_rn(d[2], d[2], rr);
             rr = __fmaf_rn(d[0], d[0], rr);
@@ -281,6 +282,16 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
                 hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
             }
+        // the list terms are evaluated from the group's centre o: members
+        // and staged sources are stored as offsets from it (the opening test
+        // keeps the absolute box)
+        float oc[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int a = 0; a < D; a++) oc[a] = 0.5f * (lo[a] + hi[a]);
+#pragma unroll
+        for (int k = 0; k < PPL; k++)
+#pragma unroll
+            for (int a = 0; a < D; a++) g.x[k][a] -= oc[a];
         int nl = 0, pl = 0;
         uint32_t top = 1;
         if (lane == 0) wl[0] = sg;   // the simulation's root node slot
@@ -331,7 +342,11 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                     tr = Bq.w + Cq.x + Cq.y;
                     Bq.w *= 7.5f; Cq.x *= 7.5f; Cq.y *= 7.5f; Cq.z *= 7.5f; Cq.w *= 7.5f; Eq *= 7.5f;
                 }
-                sm.nA[q] = A;
+                float4 Aq = A;
+                Aq.x = (A.x - oc[0]) + Bq.x;
+                Aq.y = (A.y - oc[1]) + Bq.y;
+                if (D == 3) Aq.z = (A.z - oc[2]) + Bq.z;
+                sm.nA[q] = Aq;
                 sm.nB[q] = Bq;
                 if (D == 3) sm.nC[q] = Cq;
                 sm.nD[q] = Eq;
@@ -368,8 +383,8 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 if (pl + ptot <= (uint32_t)kGWParts) {
                     for (uint32_t j = 0; j < pc; j++) {
                         const uint32_t q = pl + pin - pc + j, src = pbeg + j;
-                        sm.pA[q] = make_float4(s.x[src], s.y[src], D == 3 ? s.z[src] : 0.0f,
-                                               s.m[src]);
+                        sm.pA[q] = make_float4(s.x[src] - oc[0], s.y[src] - oc[1],
+                                               D == 3 ? s.z[src] - oc[2] : 0.0f, s.m[src]);
                         sm.pI[q] = src;
                     }
                     pl += (int)ptot;
@@ -385,8 +400,8 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 const uint32_t lc = __shfl_sync(0xffffffffu, pc, L);
                 const uint32_t chunk = min(lc, (uint32_t)kGWParts);
                 for (uint32_t j = lane; j < chunk; j += 32) {
-                    sm.pA[j] = make_float4(s.x[lb + j], s.y[lb + j], D == 3 ? s.z[lb + j] : 0.0f,
-                                           s.m[lb + j]);
+                    sm.pA[j] = make_float4(s.x[lb + j] - oc[0], s.y[lb + j] - oc[1],
+                                           D == 3 ? s.z[lb + j] - oc[2] : 0.0f, s.m[lb + j]);
                     sm.pI[j] = lb + j;
                 }
                 pl = (int)chunk;
