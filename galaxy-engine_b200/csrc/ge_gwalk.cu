@@ -39,12 +39,11 @@ constexpr int kMetaSlotsW = 9;         // tree meta word: node slots of the last
 
 template <int D>
 struct GWSmem {
-    float4 nA[kGWNodes];   // 2D {c.x, c.y, m, b^2}; 3D {c.x, c.y, c.z, m}; c = (hi - o) + lo,
-                           // the centre of mass from the group's centre o
-    float4 nB[kGWNodes];   // {lo..., Ixx...} as gq0
-    float4 nC[D == 3 ? kGWNodes : 1];   // 3D {Iyy, Izz, Ixy, Ixz}
-    float nD[kGWNodes];    // 2D Iyy, 3D Iyz
-    float nT[kGWNodes];    // -1.5 tr(I); the second moments in nB..nD are staged x 7.5
+    // an accepted node, staged: c = (hi - o) + lo, its centre of mass from
+    // the group's centre o; J = 7.5 I, its second moments; t = -1.5 tr(I)
+    float4 nA[kGWNodes];   // 2D {c.x, c.y, m, Jxx}; 3D {c.x, c.y, c.z, m}
+    float4 nB[kGWNodes];   // 2D {Jxy, Jyy, t, 0}; 3D {Jxx, Jyz, t, 0}
+    float4 nC[D == 3 ? kGWNodes : 1];   // 3D {Jyy, Jzz, Jxy, Jxz}
     float4 pA[kGWParts];   // {x - o, m}
     uint32_t pI[kGWParts]; // particle slot
 };
@@ -82,11 +81,11 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
     for (int j = 0; j < nl; j++) {
         const float4 A = sm.nA[j], B = sm.nB[j];
         const float4 C = D == 3 ? sm.nC[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float E = sm.nD[j], tq = sm.nT[j];
+        const float tq = B.z;
         const float m = D == 2 ? A.z : A.w;
-        const float jxx = D == 2 ? B.z : B.w;
-        const float jxy = D == 2 ? B.w : C.z;
-        const float jyy = D == 2 ? E : C.x;
+        const float jxx = D == 2 ? A.w : B.x;
+        const float jxy = D == 2 ? B.x : C.z;
+        const float jyy = D == 2 ? B.y : C.x;
 #pragma unroll
         for (int k = 0; k < PPL; k++) {
             float d[3];
@@ -104,7 +103,7 @@ __device__ __forceinline__ void flush_nodes(const GWSmem<D> &sm, int nl, GroupSt
                 Jd[1] = __fmaf_rn(jxy, d[0], jyy * d[1]);
                 Jd[2] = 0.0f;
             } else {
-                const float jzz = C.y, jxz = C.w, jyz = E;
+                const float jzz = C.y, jxz = C.w, jyz = B.y;
                 Jd[0] = __fmaf_rn(jxx, d[0], __fmaf_rn(jxy, d[1], jxz * d[2]));
                 Jd[1] = __fmaf_rn(jxy, d[0], __fmaf_rn(jyy, d[1], jyz * d[2]));
                 Jd[2] = __fmaf_rn(jxz, d[0], __fmaf_rn(jyz, d[1], jzz * d[2]));
@@ -342,15 +341,15 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                     tr = Bq.w + Cq.x + Cq.y;
                     Bq.w *= 7.5f; Cq.x *= 7.5f; Cq.y *= 7.5f; Cq.z *= 7.5f; Cq.w *= 7.5f; Eq *= 7.5f;
                 }
-                float4 Aq = A;
-                Aq.x = (A.x - oc[0]) + Bq.x;
-                Aq.y = (A.y - oc[1]) + Bq.y;
-                if (D == 3) Aq.z = (A.z - oc[2]) + Bq.z;
-                sm.nA[q] = Aq;
-                sm.nB[q] = Bq;
-                if (D == 3) sm.nC[q] = Cq;
-                sm.nD[q] = Eq;
-                sm.nT[q] = -1.5f * tr;
+                const float cx = (A.x - oc[0]) + Bq.x, cy = (A.y - oc[1]) + Bq.y;
+                if (D == 2) {
+                    sm.nA[q] = make_float4(cx, cy, A.z, Bq.z);
+                    sm.nB[q] = make_float4(Bq.w, Eq, -1.5f * tr, 0.0f);
+                } else {
+                    sm.nA[q] = make_float4(cx, cy, (A.z - oc[2]) + Bq.z, A.w);
+                    sm.nB[q] = make_float4(Bq.w, Eq, -1.5f * tr, 0.0f);
+                    sm.nC[q] = Cq;
+                }
             }
             nl += __popc(accb);
             // 2. children of opened internal nodes onto the work stack
