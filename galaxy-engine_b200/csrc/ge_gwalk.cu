@@ -144,6 +144,27 @@ __device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupSt
 #pragma unroll
         for (int a = 0; a < 3; a++) acc[k][a] = 0.0f;
     }
+    if (!POT && !count && eps2 > 0.0f) {
+        // the particle's own term is exactly zero (d = 0: its staged offset
+        // is its own offset, bit for bit), so no pair needs the test
+        for (int j = 0; j < pl; j++) {
+            const float4 P = sm.pA[j];
+#pragma unroll
+            for (int k = 0; k < PPL; k++) {
+                float d[3];
+                d[0] = P.x - g.x[k][0];
+                d[1] = P.y - g.x[k][1];
+                d[2] = D == 3 ? P.z - g.x[k][2] : 0.0f;
+                float rr = __fmaf_rn(d[1], d[1], eps2);
+                if (D == 3) rr = __fmaf_rn(d[2], d[2], rr);
+                rr = __fmaf_rn(d[0], d[0], rr);
+                const float inv = rsqrt_fast(rr);
+                const float fm = P.w * (inv * inv * inv);
+#pragma unroll
+                for (int a = 0; a < D; a++) acc[k][a] = __fmaf_rn(d[a], fm, acc[k][a]);
+            }
+        }
+    } else
     for (int j = 0; j < pl; j++) {
         const float4 P = sm.pA[j];
         const uint32_t pj = sm.pI[j];
