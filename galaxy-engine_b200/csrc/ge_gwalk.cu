@@ -33,6 +33,10 @@ constexpr int kGWThreads = kGWWarps * 32;
 constexpr int kGWNodes = 64;           // staged accepted nodes per warp
 constexpr int kGWParts = 64;           // staged leaf particles per warp
 constexpr uint32_t kGWStack = 2048;    // work stack entries per warp (global memory)
+// the work stack lives in shared memory while it fits (the deepest measured
+// stacks: ~170 entries in 2D, ~800 in 3D at theta 0.5, ~1400 at theta 0.3)
+// and moves to the warp's global stack when it would not
+template <int D> struct GWShared { static constexpr uint32_t value = D == 2 ? 256u : 1024u; };
 constexpr int kMetaGroupCtr = 10;      // tree meta word: next group to walk
 constexpr int kMetaGroupCount = 11;    // tree meta word: groups made
 constexpr int kMetaSlotsW = 9;         // tree meta word: node slots of the last build
@@ -256,7 +260,9 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
              unsigned long long *inter, uint32_t *err, double *epot = nullptr) {
     dep_wait();
     __shared__ GWSmem<D> smem[kGWWarps];
+    __shared__ uint32_t s_stack[kGWWarps][GWShared<D>::value];
     GWSmem<D> &sm = smem[threadIdx.x >> 5];
+    uint32_t *stk = s_stack[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -314,13 +320,15 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
             for (int a = 0; a < D; a++) g.x[k][a] -= oc[a];
         int nl = 0, pl = 0;
         uint32_t top = 1;
-        if (lane == 0) wl[0] = sg;   // the simulation's root node slot
+        bool spilled = false;   // warp-uniform: the stack is in wl (global)
+        if (lane == 0) stk[0] = sg;   // the simulation's root node slot
         __syncwarp();
         bool overflow = false;
         while (top > 0) {
             const uint32_t take = min(top, 32u);
             top -= take;
-            const uint32_t c = lane < take ? __ldcg(&wl[top + lane]) : kEmpty;
+            const uint32_t c = lane < take ? (spilled ? __ldcg(&wl[top + lane]) : stk[top + lane])
+                                           : kEmpty;
             __syncwarp();
             int kind = 0;   // 1 accepted node, 2 opened leaf, 3 opened internal node
             float4 A = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -382,11 +390,19 @@ k_group_walk(State s, StepParams p, Segs sg_tab, Tree t, int integrate_end,
                 if (lane >= (unsigned)o) incl += v;
             }
             const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+            if (!spilled && top + tot > GWShared<D>::value) {   // warp-uniform: move to wl
+                for (uint32_t q = lane; q < top; q += 32) wl[q] = stk[q];
+                spilled = true;
+                __syncwarp();
+            }
             if (top + tot > kGWStack) {   // warp-uniform
                 overflow = true;
                 break;
             }
-            for (uint32_t q = 0; q < nch; q++) wl[top + incl - nch + q] = inf.x + q;
+            if (spilled)
+                for (uint32_t q = 0; q < nch; q++) wl[top + incl - nch + q] = inf.x + q;
+            else
+                for (uint32_t q = 0; q < nch; q++) stk[top + incl - nch + q] = inf.x + q;
             top += tot;
             // 3. particles of opened leaves into the particle list
             uint32_t pc = kind == 2 ? inf.w - inf.z : 0u;
