@@ -9,7 +9,8 @@
 //     centre of mass to the box and b the node's opening radius (ge_moments.cu),
 //     which is at least as strict as every member's own test;
 //   * up to 32 candidate nodes are tested at once, one per lane, taken from a
-//     per-warp work stack in global memory;
+//     per-warp work stack in shared memory (moved to the warp's stack in
+//     global memory when it outgrows it);
 //   * accepted nodes (centre of mass, mass, second moments) and the
 //     particles of opened leaves are staged in shared memory and, when a list
 //     fills up or the walk ends, every lane evaluates them for its own
