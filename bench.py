@@ -397,7 +397,10 @@ def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
         reqs.append((float(t), dims, n, steps, 5000 + k))
     sts = [ics.disk2d(n, seed=sd) if d == 2 else ics.plummer3d(n, seed=sd)
            for _, d, n, _, sd in reqs]
-    p2 = ge.default_params(2, G=1.0, theta=0.7, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
+    # 2D requests at theta 0.65: at 0.7 the median error of a 2D disk after a few
+    # hundred steps sits at about 1e-3 (the mode's target), so some requests
+    # land on either side of it; 3D requests stay at 0.7 (about 4e-4)
+    p2 = ge.default_params(2, G=1.0, theta=0.65, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
                            group_size=64)
     p3 = ge.default_params(3, G=1.0, theta=0.7, softening=0.01, dt=DT, precision=ge.PREC_MIXED,
                            group_size=32)
@@ -455,6 +458,7 @@ def bench_serving(ge, ics, seconds, budget=120 << 30, rate=50.0, seed=7):
            "pool_steps": [int(s.pool_iterations[0]), int(s.pool_iterations[1])],
            "request_latency_s_p50": s.latency_s_p50, "request_latency_s_p99": s.latency_s_p99,
            "batched_steps": int(s.iterations), "precision": "mixed",
+           "theta": {"2d": 0.65, "3d": 0.7}, "group_size": {"2d": 64, "3d": 32},
            "per_request_median_err_vs_fp64": errs}
     srv.close()
     return res
