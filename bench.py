@@ -273,9 +273,10 @@ def bench_mixed(ge, torch, stream, st, n, flush, K=10):
 def bench_plummer3d(ge, ics, torch, n=1 << 22, K=20):
     """The mixed-precision 3D workload: a Plummer sphere of 4,194,304 particles,
     theta 0.5, softening 0.01 (added to r^2 as the 3D walk does), dt 5e-4,
-    group walk; throughput over K steps, the median error against the FP64
-    direct sum on 32,768 sampled particles, and the drift of the total energy
-    and of the momentum over the K steps (all in FP64)."""
+    group walk with group size and leaf capacity from the autotuner;
+    throughput over K steps, the median error against the FP64 direct sum on
+    32,768 sampled particles, and the drift of the total energy and of the
+    momentum over the K steps (all in FP64)."""
     st = ics.plummer3d(n, seed=0)
     p = ge.default_params(3, G=1.0, theta=0.5, eps2=0.01, dt=5e-4, leaf_cap=LEAF,
                           precision=ge.PREC_MIXED, group_size=32)
@@ -283,6 +284,8 @@ def bench_plummer3d(ge, ics, torch, n=1 << 22, K=20):
     with ge.Simulation(p) as sim:
         sim.set_stream(stream.cuda_stream)
         sim.upload(st)
+        sim.step(2)
+        gs, leaf, table = sim.autotune(reps=1)
         sim.step(2)
         e0 = sim.energy_f64()
         m0 = sim.sums_f64()
@@ -297,7 +300,9 @@ def bench_plummer3d(ge, ics, torch, n=1 << 22, K=20):
         stage = np.array(sim.profile_step())
     p_scale = float(np.sqrt(2.0 * m0[4] * abs(m0[0])))   # M |v|, the momentum scale
     return {"workload": f"3D Plummer sphere, N={n}, theta 0.5, softening 0.01, dt 5e-4",
-            "precision": "mixed", "group_size": 32, "value": n / (times.mean() * 1e-3),
+            "precision": "mixed", "group_size": gs, "leaf_cap": leaf,
+            "autotune_ms": {f"g{g}_l{l}": v for (g, l), v in table.items()},
+            "value": n / (times.mean() * 1e-3),
             "unit": UNIT, "ms_per_step": float(times.mean()),
             "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
             "steps": K,
