@@ -92,6 +92,7 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
     dep_wait();
     constexpr int B = KeyBits<D>::B;
     __shared__ int8_t sd[kKT + 2 * kHalo + 1];
+    __shared__ int s_lv[3];   // {segment, size-gate level, minimum-size level} of the block's first particle
     const int n = p.n;
     const int64_t base = (int64_t)blockIdx.x * kKT;
     for (int q = threadIdx.x; q < kKT + 2 * kHalo + 1; q += kKT)
@@ -105,6 +106,23 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
             p4[k] = make_uint4(0u, 0u, 0u, 0u);
         if (blockIdx.x == 0 && threadIdx.x < (unsigned)(t.cap - n4 * 4))
             t.pend[n4 * 4 + threadIdx.x] = 0u;
+    }
+    // first levels whose cells are no larger than the size gate / min size
+    // (the sizes are exact halvings of the root's: w * 2^-L)
+    auto first_level_at_most = [&](float w, float limit) {
+        if (w != w) return 127;
+        if (w <= limit) return 0;
+        if (!(limit > 0.0f)) return 127;
+        int L = max(0, ilogbf(w) - ilogbf(limit) - 1);
+        while (L <= B && scalbnf(w, -L) > limit) L++;
+        return L <= B ? L : 127;
+    };
+    if (threadIdx.x == 0 && base < n) {   // once per block, for its first particle's simulation
+        const uint32_t s0 = g.seg_of ? g.seg_of[base] : 0u;
+        const float w0 = g.box[s0].w;
+        s_lv[0] = (int)s0;
+        s_lv[1] = first_level_at_most(w0, p.size_gate);
+        s_lv[2] = first_level_at_most(w0, p.min_size);
     }
     __syncthreads();
     const int64_t i = base + threadIdx.x;
@@ -125,18 +143,9 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
     const int l_count = best == 127 ? 127 : best + 1;
     const int l_one = max(dl(i), dl(i + 1)) + 1;
     const float4 box = g.box[sg];
-    // first levels whose cells are no larger than the size gate / min size
-    // (the sizes are exact halvings of the root's: box.w * 2^-L)
-    auto first_level_at_most = [&](float limit) {
-        if (box.w != box.w) return 127;
-        if (box.w <= limit) return 0;
-        if (!(limit > 0.0f)) return 127;
-        int L = max(0, ilogbf(box.w) - ilogbf(limit) - 1);
-        while (L <= B && scalbnf(box.w, -L) > limit) L++;
-        return L <= B ? L : 127;
-    };
-    const int l_gate = first_level_at_most(p.size_gate);
-    const int l_min = first_level_at_most(p.min_size);
+    const bool same = (int)sg == s_lv[0];
+    const int l_gate = same ? s_lv[1] : first_level_at_most(box.w, p.size_gate);
+    const int l_min = same ? s_lv[2] : first_level_at_most(box.w, p.min_size);
     int lam = min(min(max(l_count, l_gate), l_one), l_min);
     if (lam > B) lam = B + 1;
     t.kdl[i] = (uint8_t)(dl(i) + 1);
