@@ -600,6 +600,16 @@ def run_ours(args, world, rank, local):
                            "algorithmic": "216 B/particle + 40 B/node (canonical count: keys, five 8-bit "
                                           "LSD passes of 24 B, gather, nodes; the sort here runs four "
                                           "9-bit passes of 16 B)"},
+        # the whole step: build and integrate bytes at the HBM peak plus the
+        # credited interactions at the FP32 interaction peak
+        "step_roofline": {
+            "value": n / ((build_bytes + 40.0 * n) / (hbm_gbs * 1e9)
+                          + inter / (fp32_peak * 1e12 / FLOPEQ_PER_INTERACTION[2])),
+            "unit": UNIT,
+            "frac": value / (n / ((build_bytes + 40.0 * n) / (hbm_gbs * 1e9)
+                                  + inter / (fp32_peak * 1e12 / FLOPEQ_PER_INTERACTION[2]))),
+            "algorithmic": "N / ((216 B/particle + 40 B/node + 40 B/particle integrate) / HBM peak "
+                           "+ credited interactions / (FP32 peak / 18 flop-eq))"},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
