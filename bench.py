@@ -166,6 +166,23 @@ def cpu_baseline(O, st, frames, params_kw):
     return dt, cores, stage / frames
 
 
+def max_over_ranks(dist, v, device):
+    """The largest of every rank's v (one all-reduce); v itself without a
+    process group.  Times are reported as the slowest rank's."""
+    if not dist:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, n, steps, total_ms):
+    """Particle-steps/s of the whole job: one replica of n particles per rank,
+    `steps` steps each, timed by the slowest rank (total_ms)."""
+    return world * n * steps / (total_ms * 1e-3)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -510,12 +527,8 @@ def run_ours(args, world, rank, local):
     if dist:
         dist.barrier()
     times = np.array([e0[k].elapsed_time(e1[k]) for k in range(K)])
-    total_ms = float(times.sum())
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n * K / (total_ms * 1e-3)
+    total_ms = max_over_ranks(dist, float(times.sum()), "cuda")
+    value = whole_job_rate(world, n, K, total_ms)
 
     # per-stage profile, interaction count, accuracy (untimed)
     stage = np.zeros(8)
@@ -546,11 +559,7 @@ def run_ours(args, world, rank, local):
     t0 = time.perf_counter()
     for _ in range(ke):
         sim.frame_host(host)
-    e2e_s = (time.perf_counter() - t0) / ke
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / ke, "cuda")
     bytes_h2d = n * 4 * 8
     bytes_d2h = n * 4 * 8
 
