@@ -363,11 +363,23 @@ def bench_batched(ge, ics, torch, count, K=5, Kp=2):
                 res["group_size"], res["leaf_cap"] = gs, leaf
             b.step(2)
             times = _timed_steps(torch, stream, b, K)
+            # the same K steps as one ge_step call: pairs of steps replay the
+            # captured CUDA graph (device time, CUDA events around the call)
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            b.step(2)   # capture
+            g0.record(stream)
+            b.step(2 * K)
+            g1.record(stream)
+            torch.cuda.synchronize()
+            graph_ms = g0.elapsed_time(g1) / (2 * K)
             res["batched"] = {"value": total / (times.mean() * 1e-3),
                               "ms_per_step": float(times.mean()),
                               "p50_ms": float(np.percentile(times, 50)),
                               "p99_ms": float(np.percentile(times, 99)), "steps": K,
-                              "launches_per_step": LAUNCHES_PER_STEP[mode]}
+                              "launches_per_step": LAUNCHES_PER_STEP[mode],
+                              "graph_ms_per_step": graph_ms,
+                              "graph_value": total / (graph_ms * 1e-3)}
             stt = b.download()
             idx = np.sort(rng.choice(total, size=8192, replace=False)).astype(np.uint32)
             ref = b.direct_sum_f64(idx)
