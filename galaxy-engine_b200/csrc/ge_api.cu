@@ -210,6 +210,7 @@ StepParams step_params(const ge_ctx *c) {
     s.group_size = c->p.group_size;
     s.heat_cond = c->p.heat_cond;
     s.direct_eps2 = c->p.direct_eps2;
+    s.mixed = c->p.precision == GE_PREC_MIXED ? 1 : 0;
     for (int a = 0; a < 3; a++) {
         s.domain[a] = c->p.domain[a];
         s.half_domain[a] = c->p.domain[a] * 0.5f;
@@ -1578,8 +1579,8 @@ int ge_predict_trajectory(ge_ctx *c, int32_t sim, int32_t nprobes, const float *
     GE_CHECK(c, cudaMemcpyAsync(dm, mass, sizeof(float) * np, cudaMemcpyHostToDevice, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     StepParams p = step_params(c);
-    GE_CHECK(c, launch_predict(D, c->b.tree, p, be[0], be[1], eps2, nprobes, dpos, dvel, dm, steps,
-                               dpath, c->stream));
+    GE_CHECK(c, launch_predict(D, c->b.tree, p, c->g.box + r, be[0], be[1], eps2, nprobes, dpos,
+                               dvel, dm, steps, dpath, c->stream));
     GE_CHECK(c, cudaMemcpyAsync(path, dpath, sizeof(float) * pn, cudaMemcpyDeviceToHost, c->stream));
     GE_CHECK(c, cudaFreeAsync(d, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));

@@ -188,7 +188,20 @@ struct StepParams {
     float heat_cond;  // heat exchange coefficient (used when State::temp is set)
     float direct_eps2;   // value the direct sum adds to r^2
     int i0;              // the per-particle walk: first particle (up to n), 0 by default
+    int mixed;           // GE_PREC_MIXED: the moment pass rewrites the node entries
 };
+
+// 2D walk entries {x, y, m, w}.  Plain layout: w = size^2 (-1 for a particle,
+// -2 for a massless node), the subtree successor in link[].  Packed layout
+// (tree meta word kMetaWalkPacked = 1): a node's w holds its level L (6 bits)
+// and its successor (26 bits); its size is the simulation's root size halved
+// L times (exact), so size^2 = fl(size_L * size_L) as the plain layout has it.
+// Particles keep w = -1.0f, whose bits no node word reaches (L <= 46).
+constexpr int kMetaWalkPacked = 13;
+constexpr uint32_t kPackSkipBits = 26, kPackMaxLevel = 46;
+__host__ __device__ constexpr uint32_t pack_entry_word(uint32_t level, uint32_t skip) {
+    return (level << kPackSkipBits) | skip;
+}
 
 constexpr int kBBoxThreads = 256;
 constexpr int kBoxItems = 8;       // particles per thread per block tile of the kick/box pass
@@ -289,7 +302,8 @@ cudaError_t launch_field(const State &s, uint32_t lo, uint32_t hi, int amount_x,
                          cudaStream_t st);
 // trajectory preview: probes stepped against the walk layout of the last
 // build, entries [begin, end) (one simulation's tree)
-cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, uint32_t begin,
+cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, const float4 *box,
+                           uint32_t begin,
                            uint32_t end, float eps2, int nprobes, const float *pos,
                            const float *vel, const float *mass, int steps, float *path,
                            cudaStream_t st);

@@ -18,8 +18,16 @@ namespace ge {
 
 constexpr int kPredThreads = 64;
 
-__device__ __forceinline__ float entry_s2(const Tree &t, int D, uint32_t k) {
-    return D == 2 ? __ldg(&t.src[k]).w : __uint_as_float(__ldg(&((const uint2 *)t.link)[k]).y);
+// size^2 of entry k (-1 for a particle); rs_bits: the simulation's root size,
+// for the packed 2D layout
+__device__ __forceinline__ float entry_s2(const Tree &t, int D, uint32_t k, bool packed,
+                                          uint32_t rs_bits) {
+    if (D == 3) return __uint_as_float(__ldg(&((const uint2 *)t.link)[k]).y);
+    const float4 A = __ldg(&t.src[k]);
+    if (!packed || A.w == -1.0f) return A.w;
+    if (!(A.z > 0.0f)) return -2.0f;
+    const float szl = __uint_as_float(rs_bits - ((__float_as_uint(A.w) >> kPackSkipBits) << 23));
+    return fmul(szl, szl);
 }
 __device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k) {
     return D == 2 ? __ldg(&((const uint32_t *)t.link)[k]) : __ldg(&((const uint2 *)t.link)[k]).x;
@@ -27,7 +35,8 @@ __device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k)
 
 template <int D>
 __device__ void old_force(const Tree &t, const StepParams &p, uint32_t begin, uint32_t end,
-                          float eps2, const float *pos, float pmass, float *F) {
+                          float eps2, const float *pos, float pmass, float *F, bool packed,
+                          uint32_t rs_bits) {
     F[0] = F[1] = F[2] = 0.0f;
     uint32_t k = begin;
     while (k < end) {
@@ -50,8 +59,8 @@ __device__ void old_force(const Tree &t, const StepParams &p, uint32_t begin, ui
         if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
         r2 = fadd(r2, eps2);
         // a leaf's particles follow it in the layout (size^2 = -1)
-        const bool leaf = k + 1 < skip && entry_s2(t, D, k + 1) == -1.0f;
-        const float s2 = D == 2 ? A.w : entry_s2(t, D, k);
+        const bool leaf = k + 1 < skip && entry_s2(t, D, k + 1, packed, rs_bits) == -1.0f;
+        const float s2 = entry_s2(t, D, k, packed, rs_bits);
         if (s2 < fmul(p.theta2, r2) || leaf) {
             if (leaf && skip - k - 1 == 1u) {   // one particle: skip it when it sits on the probe
                 const float4 o = __ldg(&t.src[k + 1]);
@@ -75,17 +84,19 @@ __device__ void old_force(const Tree &t, const StepParams &p, uint32_t begin, ui
 
 template <int D>
 __global__ void __launch_bounds__(kPredThreads)
-k_predict(Tree t, StepParams p, uint32_t begin, uint32_t end, float eps2, int nprobes,
-          const float *__restrict__ pos, const float *__restrict__ vel,
+k_predict(Tree t, StepParams p, const float4 *box, uint32_t begin, uint32_t end, float eps2,
+          int nprobes, const float *__restrict__ pos, const float *__restrict__ vel,
           const float *__restrict__ mass, int steps, float *__restrict__ path) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nprobes) return;
+    const bool packed = D == 2 && __ldg(&t.meta[kMetaWalkPacked]) != 0u;
+    const uint32_t rs_bits = packed ? __float_as_uint(__ldg(box).w) : 0u;   // the simulation's root size
     float ps[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, F[3];
 #pragma unroll
     for (int a = 0; a < D; a++) { ps[a] = pos[q * D + a]; v[a] = vel[q * D + a]; }
     const float m = mass[q], h = fmul(p.dt, 0.5f);
     for (int s = 0; s < steps; s++) {
-        old_force<D>(t, p, begin, end, eps2, ps, m, F);
+        old_force<D>(t, p, begin, end, eps2, ps, m, F, packed, rs_bits);
 #pragma unroll
         for (int a = 0; a < D; a++) v[a] = fadd(v[a], fmul(fdiv(F[a], m), h));
 #pragma unroll
@@ -100,7 +111,7 @@ k_predict(Tree t, StepParams p, uint32_t begin, uint32_t end, float eps2, int np
                 else if (ps[a] >= hi) ps[a] = fsub(ps[a], p.domain[a]);
             }
         }
-        old_force<D>(t, p, begin, end, eps2, ps, m, F);
+        old_force<D>(t, p, begin, end, eps2, ps, m, F, packed, rs_bits);
 #pragma unroll
         for (int a = 0; a < D; a++) v[a] = fadd(v[a], fmul(fdiv(F[a], m), h));
 #pragma unroll
@@ -108,18 +119,19 @@ k_predict(Tree t, StepParams p, uint32_t begin, uint32_t end, float eps2, int np
     }
 }
 
-cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, uint32_t begin,
+cudaError_t launch_predict(int dims, const Tree &t, const StepParams &p, const float4 *box,
+                           uint32_t begin,
                            uint32_t end, float eps2, int nprobes, const float *pos,
                            const float *vel, const float *mass, int steps, float *path,
                            cudaStream_t st) {
     const int blocks = (nprobes + kPredThreads - 1) / kPredThreads;
     if (blocks < 1) return cudaSuccess;
     if (dims == 2)
-        k_predict<2><<<blocks, kPredThreads, 0, st>>>(t, p, begin, end, eps2, nprobes, pos, vel,
-                                                     mass, steps, path);
+        k_predict<2><<<blocks, kPredThreads, 0, st>>>(t, p, box, begin, end, eps2, nprobes, pos,
+                                                     vel, mass, steps, path);
     else
-        k_predict<3><<<blocks, kPredThreads, 0, st>>>(t, p, begin, end, eps2, nprobes, pos, vel,
-                                                     mass, steps, path);
+        k_predict<3><<<blocks, kPredThreads, 0, st>>>(t, p, box, begin, end, eps2, nprobes, pos,
+                                                     vel, mass, steps, path);
     return cudaGetLastError();
 }
 

@@ -659,7 +659,7 @@ template <int D>
 __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tree &t, uint32_t k,
                                               uint4 inf, uint4 ax, float4 w, float size2,
                                               uint32_t ez, uint32_t ew, uint32_t total,
-                                              uint32_t *err) {
+                                              uint32_t *err, bool packed) {
     const uint32_t me = ez + ax.x + inf.z;
     const uint32_t skip = ew + ax.x - ax.y + inf.w;
     if (me >= total || skip > total) {   // cannot happen for a consistent tree
@@ -678,11 +678,14 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
         // it is accepted by every test (size^2 = -2; particles have -1),
         // carries no mass (the walk makes no interaction with a massless
         // node) and leads to its successor.
-        t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f, -2.0f) : make_float4(w.x, w.y, w.z, 0.0f);
+        t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f,
+                                         packed ? __uint_as_float(pack_entry_word(ax.x, skip)) : -2.0f)
+                           : make_float4(w.x, w.y, w.z, 0.0f);
         if (D == 2) ((uint32_t *)t.link)[me] = skip;
         else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
     } else {
-        t.src[me] = w;
+        t.src[me] = D == 2 && packed ? make_float4(w.x, w.y, w.z, __uint_as_float(pack_entry_word(ax.x, skip)))
+                                     : w;
         if (D == 2) ((uint32_t *)t.link)[me] = skip;
         else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(size2));
     }
@@ -1039,6 +1042,14 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     //   subtree successor    = C(end) + level - same_end + end
     //   entry of particle j  = entry of its leaf + 1 + (j - start)
     const uint32_t total = nodes + n;
+    // 2D, not rewritten by the moment pass: packed entries when every level
+    // and successor fits the word and every node size is a normal float (a
+    // node of size <= min_size is a leaf, so sizes stay >= min_size / 2, or
+    // the tree is one leaf), where halving L times is the exponent minus L
+    const bool packed = D == 2 && !p.mixed && p.min_size >= 1e-30f &&
+                        *(volatile uint32_t *)&t.meta[kMetaLevels] <= kPackMaxLevel + 1u &&
+                        total < (1u << kPackSkipBits);
+    if (gtid == 0) t.meta[kMetaWalkPacked] = packed ? 1u : 0u;
     // two slots per round: both slots' loads are issued before either's stores
     for (uint32_t k0 = gtid; k0 < slots; k0 += 2u * nthreads) {
         const uint32_t kk[2] = {k0, k0 + nthreads};
@@ -1062,7 +1073,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
 #pragma unroll
         for (int u = 0; u < 2; u++) {
             if (inf[u].w == 0u) continue;
-            scatter_entry<D>(s, g, t, kk[u], inf[u], ax[u], wv[u], s2[u], ez[u], ew[u], total, err);
+            scatter_entry<D>(s, g, t, kk[u], inf[u], ax[u], wv[u], s2[u], ez[u], ew[u], total, err,
+                             packed);
         }
     }
 }

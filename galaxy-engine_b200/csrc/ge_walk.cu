@@ -30,6 +30,8 @@
 //                   Kahan-compensated sums of the acceleration terms.
 // integrateEnd (physics.cpp:1114-1125) is fused into the epilogue.  A
 // simulation below params.direct_below is skipped here (ge_direct.cu).
+#include <type_traits>
+
 #include "ge_bh.h"
 #include "ge_device.cuh"
 #include "ge_internal.h"
@@ -94,11 +96,31 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         uint32_t k = __ldg(&g.root_begin[sg]);
         const uint32_t end = __ldg(&g.root_end[sg]);
         uint32_t cnt = 0;
+        // 2D packed entries: one load per step (the successor and the level
+        // in the fourth word); the root size of the particle's simulation
+        const bool packed = D == 2 && MODE != GE_PREC_MIXED && __ldg(&t.meta[kMetaWalkPacked]) != 0u;
+        const uint32_t rs_bits = packed ? __float_as_uint(__ldg(&g.box[sg]).w) : 0u;
+        // the loop once per layout, chosen here rather than at every step
+        auto walk_range = [&](auto pk) {
+        constexpr bool PK = decltype(pk)::value && D == 2 && MODE != GE_PREC_MIXED;
         while (k < end) {
             const float4 A = __ldg(&src[k]);
-            const LT L = __ldg(&link[k]);
             const float m = D == 2 ? A.z : A.w;
-            const float s2 = link_s2(L, A.w);
+            float s2;          // a node's size^2 (plain layout: -1 particle, -2 massless)
+            uint32_t nxt_skip;
+            bool part;         // a particle's entry
+            if constexpr (PK) {
+                const uint32_t wb = __float_as_uint(A.w);
+                part = A.w == -1.0f;
+                const float szl = __uint_as_float(rs_bits - ((wb >> kPackSkipBits) << 23));
+                s2 = fmul(szl, szl);   // not used for particles and massless nodes
+                nxt_skip = wb & ((1u << kPackSkipBits) - 1u);
+            } else {
+                const LT L = __ldg(&link[k]);
+                s2 = link_s2(L, A.w);
+                nxt_skip = link_skip(L);
+                part = s2 == -1.0f;
+            }
             float d[3];
             d[0] = fsub(A.x, pi[0]);
             d[1] = fsub(A.y, pi[1]);
@@ -112,12 +134,14 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
             r2 = fadd(r2, eps2);
             // MIXED entries hold the squared opening radius, which already
             // includes 1 / theta
-            const bool acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
+            bool acc;
+            if constexpr (PK) acc = part || m <= 0.0f || s2 < fmul(th2, r2);   // as -1 / -2 would
+            else acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
             if (kSelfTest) {
                 // heat exchange (physics.cpp:145-158, 183-191): an accepted node
                 // with mass, or any other particle of an opened leaf (massless
                 // ones included); the others' temperatures as before the walk
-                if (TEMP && acc && k != self && (m != 0.0f || s2 == -1.0f)) {
+                if (TEMP && acc && k != self && (m != 0.0f || part)) {
                     float inv;
                     if (MODE == GE_PREC_EXACT) inv = fdiv(1.0f, __fsqrt_rn(r2));
                     else inv = rsqrt_approx(r2);
@@ -201,8 +225,11 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
             }
             // a valid skip lies past k; max() keeps k increasing whatever the
             // layout holds, so the walk ends within end - begin entries
-            k = max(k + 1, acc ? link_skip(L) : k + 1);
+            k = max(k + 1, acc && !part ? nxt_skip : k + 1);
         }
+        };
+        if (packed) walk_range(std::true_type{});
+        else walk_range(std::false_type{});
         float a3[3];
 #pragma unroll
         for (int a = 0; a < D; a++)
