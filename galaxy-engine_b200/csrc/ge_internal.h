@@ -194,10 +194,17 @@ struct StepParams {
 // 2D walk entries {x, y, m, w}.  Plain layout: w = size^2 (-1 for a particle,
 // -2 for a massless node), the subtree successor in link[].  Packed layout
 // (tree meta word kMetaWalkPacked = 1): a node's w holds its level L (6 bits)
-// and its successor (26 bits); its size is the simulation's root size halved
-// L times (exact), so size^2 = fl(size_L * size_L) as the plain layout has it.
-// Particles keep w = -1.0f, whose bits no node word reaches (L <= 46).
+// and its successor (26 bits); its size is the simulation's root size rs
+// halved L times (exact), so the plain layout's size^2 = fl(size_L^2) =
+// fl(rs^2) * 4^-L: fl(rs^2) with 2L taken off its exponent, exact while both
+// are normal floats (every rs below 1e19 and min_size >= 1e-18, checked by
+// the build).  Particles keep w = -1.0f, whose bits no node word reaches
+// (L <= 46).
 constexpr int kMetaWalkPacked = 13;
+constexpr int kMetaBigRoot = 14;   // tree meta word: some simulation's root size >= 1e19
+__device__ __forceinline__ float packed_size2(uint32_t w_bits, uint32_t rs2_bits) {
+    return __uint_as_float(rs2_bits - ((w_bits >> 2) & 0x3F000000u));   // exponent - 2L
+}
 constexpr uint32_t kPackSkipBits = 26, kPackMaxLevel = 46;
 __host__ __device__ constexpr uint32_t pack_entry_word(uint32_t level, uint32_t skip) {
     return (level << kPackSkipBits) | skip;

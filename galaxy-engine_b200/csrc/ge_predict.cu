@@ -18,16 +18,15 @@ namespace ge {
 
 constexpr int kPredThreads = 64;
 
-// size^2 of entry k (-1 for a particle); rs_bits: the simulation's root size,
-// for the packed 2D layout
+// size^2 of entry k (-1 for a particle); rs_bits: the simulation's root
+// size^2, for the packed 2D layout
 __device__ __forceinline__ float entry_s2(const Tree &t, int D, uint32_t k, bool packed,
                                           uint32_t rs_bits) {
     if (D == 3) return __uint_as_float(__ldg(&((const uint2 *)t.link)[k]).y);
     const float4 A = __ldg(&t.src[k]);
     if (!packed || A.w == -1.0f) return A.w;
     if (!(A.z > 0.0f)) return -2.0f;
-    const float szl = __uint_as_float(rs_bits - ((__float_as_uint(A.w) >> kPackSkipBits) << 23));
-    return fmul(szl, szl);
+    return packed_size2(__float_as_uint(A.w), rs_bits);
 }
 __device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k) {
     return D == 2 ? __ldg(&((const uint32_t *)t.link)[k]) : __ldg(&((const uint2 *)t.link)[k]).x;
@@ -90,7 +89,8 @@ k_predict(Tree t, StepParams p, const float4 *box, uint32_t begin, uint32_t end,
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nprobes) return;
     const bool packed = D == 2 && __ldg(&t.meta[kMetaWalkPacked]) != 0u;
-    const uint32_t rs_bits = packed ? __float_as_uint(__ldg(box).w) : 0u;   // the simulation's root size
+    const float rs = packed ? __ldg(box).w : 0.0f;   // the simulation's root size
+    const uint32_t rs_bits = __float_as_uint(fmul(rs, rs));
     float ps[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, F[3];
 #pragma unroll
     for (int a = 0; a < D; a++) { ps[a] = pos[q * D + a]; v[a] = vel[q * D + a]; }

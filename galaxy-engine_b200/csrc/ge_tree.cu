@@ -746,6 +746,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         t.meta[kMetaNodes] = 0u; t.meta[kMetaLevels] = 0u;
         t.meta[kMetaSmall] = 0u; t.meta[kMetaP2Alloc] = 0u; t.meta[kMetaTimeline] = 0u;
         t.meta[kMetaReal] = 0u; t.meta[kMetaSlots] = 0u; t.meta[kMetaP2Task] = 0u;
+        t.meta[kMetaBigRoot] = 0u;
         stamp(t);
     }
     for (uint32_t i = gtid; i < (uint32_t)kMaxLevels + 2u; i += nthreads) t.lvl_alloc[i] = 0u;
@@ -973,6 +974,9 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         const uint32_t e = __ldcg(&t.info[k]).w;
         if (e) atomicAdd(&t.endcnt[e], 1u);
     }
+    // root sizes whose square is not a normal float rule out packed entries
+    for (uint32_t sg = gtid; sg < (uint32_t)g.S; sg += nthreads)
+        if (!(g.box[sg].w < 1e19f)) atomicOr(&t.meta[kMetaBigRoot], 1u);
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
     // inclusive scan of endcnt[0..n] in place, by block chunks; each chunk's
@@ -1043,10 +1047,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     //   entry of particle j  = entry of its leaf + 1 + (j - start)
     const uint32_t total = nodes + n;
     // 2D, not rewritten by the moment pass: packed entries when every level
-    // and successor fits the word and every node size is a normal float (a
-    // node of size <= min_size is a leaf, so sizes stay >= min_size / 2, or
-    // the tree is one leaf), where halving L times is the exponent minus L
-    const bool packed = D == 2 && !p.mixed && p.min_size >= 1e-30f &&
+    // and successor fits the word and every size^2 is a normal float (a node
+    // of size <= min_size is a leaf, so sizes stay >= min_size / 2, or the
+    // tree is one leaf; root sizes below 1e19), where quartering L times is
+    // the exponent minus 2L
+    const bool packed = D == 2 && !p.mixed && p.min_size >= 1e-18f &&
+                        *(volatile uint32_t *)&t.meta[kMetaBigRoot] == 0u &&
                         *(volatile uint32_t *)&t.meta[kMetaLevels] <= kPackMaxLevel + 1u &&
                         total < (1u << kPackSkipBits);
     if (gtid == 0) t.meta[kMetaWalkPacked] = packed ? 1u : 0u;

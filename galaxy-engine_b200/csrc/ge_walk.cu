@@ -99,7 +99,8 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         // 2D packed entries: one load per step (the successor and the level
         // in the fourth word); the root size of the particle's simulation
         const bool packed = D == 2 && MODE != GE_PREC_MIXED && __ldg(&t.meta[kMetaWalkPacked]) != 0u;
-        const uint32_t rs_bits = packed ? __float_as_uint(__ldg(&g.box[sg]).w) : 0u;
+        const float rs = packed ? __ldg(&g.box[sg]).w : 0.0f;
+        const uint32_t rs2_bits = __float_as_uint(fmul(rs, rs));   // the root's size^2
         // the loop once per layout, chosen here rather than at every step
         auto walk_range = [&](auto pk) {
         constexpr bool PK = decltype(pk)::value && D == 2 && MODE != GE_PREC_MIXED;
@@ -112,8 +113,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
             if constexpr (PK) {
                 const uint32_t wb = __float_as_uint(A.w);
                 part = A.w == -1.0f;
-                const float szl = __uint_as_float(rs_bits - ((wb >> kPackSkipBits) << 23));
-                s2 = fmul(szl, szl);   // not used for particles and massless nodes
+                s2 = packed_size2(wb, rs2_bits);   // not used for particles and massless nodes
                 nxt_skip = wb & ((1u << kPackSkipBits) - 1u);
             } else {
                 const LT L = __ldg(&link[k]);
