@@ -103,130 +103,130 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
         const uint32_t rs2_bits = __float_as_uint(fmul(rs, rs));   // the root's size^2
         // the loop once per layout, chosen here rather than at every step
         auto walk_range = [&](auto pk) {
-        constexpr bool PK = decltype(pk)::value && D == 2 && MODE != GE_PREC_MIXED;
-        while (k < end) {
-            const float4 A = __ldg(&src[k]);
-            const float m = D == 2 ? A.z : A.w;
-            float s2;          // a node's size^2 (plain layout: -1 particle, -2 massless)
-            uint32_t nxt_skip;
-            bool part;         // a particle's entry
-            if constexpr (PK) {
-                const uint32_t wb = __float_as_uint(A.w);
-                part = A.w == -1.0f;
-                s2 = packed_size2(wb, rs2_bits);   // not used for particles and massless nodes
-                nxt_skip = wb & ((1u << kPackSkipBits) - 1u);
-            } else {
-                const LT L = __ldg(&link[k]);
-                s2 = link_s2(L, A.w);
-                nxt_skip = link_skip(L);
-                part = s2 == -1.0f;
-            }
-            float d[3];
-            d[0] = fsub(A.x, pi[0]);
-            d[1] = fsub(A.y, pi[1]);
-            d[2] = D == 3 ? fsub(A.z, pi[2]) : 0.0f;
-            if (PER) {
-#pragma unroll
-                for (int a = 0; a < D; a++) d[a] = wrap_d(d[a], p.domain[a], p.half_domain[a]);
-            }
-            float r2 = fadd(fmul(d[0], d[0]), fmul(d[1], d[1]));
-            if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
-            r2 = fadd(r2, eps2);
-            // MIXED entries hold the squared opening radius, which already
-            // includes 1 / theta
-            bool acc;
-            if constexpr (PK) acc = part || m <= 0.0f || s2 < fmul(th2, r2);   // as -1 / -2 would
-            else acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
-            if (kSelfTest) {
-                // heat exchange (physics.cpp:145-158, 183-191): an accepted node
-                // with mass, or any other particle of an opened leaf (massless
-                // ones included); the others' temperatures as before the walk
-                if (TEMP && acc && k != self && (m != 0.0f || part)) {
-                    float inv;
-                    if (MODE == GE_PREC_EXACT) inv = fdiv(1.0f, __fsqrt_rn(r2));
-                    else inv = rsqrt_approx(r2);
-                    const float dist = r2 > 1e-16f ? fdiv(1.0f, inv) : 0.0f;
-                    if (dist > 1e-8f) {
-                        const float diff = fsub(__ldg(&t.tv[k]), ti);
-                        ti = fadd(ti, fmul(fdiv(fmul(p.heat_cond, diff), dist), p.dt));
-                    }
+            constexpr bool PK = decltype(pk)::value && D == 2 && MODE != GE_PREC_MIXED;
+            while (k < end) {
+                const float4 A = __ldg(&src[k]);
+                const float m = D == 2 ? A.z : A.w;
+                float s2;          // a node's size^2 (plain layout: -1 particle, -2 massless)
+                uint32_t nxt_skip;
+                bool part;         // a particle's entry
+                if constexpr (PK) {
+                    const uint32_t wb = __float_as_uint(A.w);
+                    part = A.w == -1.0f;
+                    s2 = packed_size2(wb, rs2_bits);   // not used for particles and massless nodes
+                    nxt_skip = wb & ((1u << kPackSkipBits) - 1u);
+                } else {
+                    const LT L = __ldg(&link[k]);
+                    s2 = link_s2(L, A.w);
+                    nxt_skip = link_skip(L);
+                    part = s2 == -1.0f;
                 }
-                if (acc && m != 0.0f && k != self) {
-                    if (MODE == GE_PREC_MIXED) {
-                        float term[3];
-                        if (s2 >= 0.0f) {
-                            // node: centre of mass = hi + lo, then monopole +
-                            // quadrupole of the softened kernel:
-                            //   m d / r^3 - 3 I d / r^5 - 1.5 tr(I) d / r^5
-                            //   + 7.5 (d.I.d) d / r^7,   r^2 = |d|^2 + eps2
-                            const float4 B = __ldg(&t.mq0[k]);
-                            d[0] += B.x; d[1] += B.y;
-                            if (D == 3) d[2] += B.z;
-                            float rr = d[0] * d[0] + d[1] * d[1] + eps2;
-                            if (D == 3) rr += d[2] * d[2];
-                            const float inv = rsqrt_approx(rr);
-                            const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
-                            const float inv7 = inv5 * inv2;
-                            float Id[3], tr;
-                            if (D == 2) {
-                                const float ixx = B.z, ixy = B.w, iyy = __ldg(&t.mq2[k]);
-                                Id[0] = ixx * d[0] + ixy * d[1];
-                                Id[1] = ixy * d[0] + iyy * d[1];
-                                Id[2] = 0.0f;
-                                tr = ixx + iyy;
+                float d[3];
+                d[0] = fsub(A.x, pi[0]);
+                d[1] = fsub(A.y, pi[1]);
+                d[2] = D == 3 ? fsub(A.z, pi[2]) : 0.0f;
+                if (PER) {
+    #pragma unroll
+                    for (int a = 0; a < D; a++) d[a] = wrap_d(d[a], p.domain[a], p.half_domain[a]);
+                }
+                float r2 = fadd(fmul(d[0], d[0]), fmul(d[1], d[1]));
+                if (D == 3) r2 = fadd(r2, fmul(d[2], d[2]));
+                r2 = fadd(r2, eps2);
+                // MIXED entries hold the squared opening radius, which already
+                // includes 1 / theta
+                bool acc;
+                if constexpr (PK) acc = part || m <= 0.0f || s2 < fmul(th2, r2);   // as -1 / -2 would
+                else acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
+                if (kSelfTest) {
+                    // heat exchange (physics.cpp:145-158, 183-191): an accepted node
+                    // with mass, or any other particle of an opened leaf (massless
+                    // ones included); the others' temperatures as before the walk
+                    if (TEMP && acc && k != self && (m != 0.0f || part)) {
+                        float inv;
+                        if (MODE == GE_PREC_EXACT) inv = fdiv(1.0f, __fsqrt_rn(r2));
+                        else inv = rsqrt_approx(r2);
+                        const float dist = r2 > 1e-16f ? fdiv(1.0f, inv) : 0.0f;
+                        if (dist > 1e-8f) {
+                            const float diff = fsub(__ldg(&t.tv[k]), ti);
+                            ti = fadd(ti, fmul(fdiv(fmul(p.heat_cond, diff), dist), p.dt));
+                        }
+                    }
+                    if (acc && m != 0.0f && k != self) {
+                        if (MODE == GE_PREC_MIXED) {
+                            float term[3];
+                            if (s2 >= 0.0f) {
+                                // node: centre of mass = hi + lo, then monopole +
+                                // quadrupole of the softened kernel:
+                                //   m d / r^3 - 3 I d / r^5 - 1.5 tr(I) d / r^5
+                                //   + 7.5 (d.I.d) d / r^7,   r^2 = |d|^2 + eps2
+                                const float4 B = __ldg(&t.mq0[k]);
+                                d[0] += B.x; d[1] += B.y;
+                                if (D == 3) d[2] += B.z;
+                                float rr = d[0] * d[0] + d[1] * d[1] + eps2;
+                                if (D == 3) rr += d[2] * d[2];
+                                const float inv = rsqrt_approx(rr);
+                                const float inv2 = inv * inv, inv3 = inv2 * inv, inv5 = inv3 * inv2;
+                                const float inv7 = inv5 * inv2;
+                                float Id[3], tr;
+                                if (D == 2) {
+                                    const float ixx = B.z, ixy = B.w, iyy = __ldg(&t.mq2[k]);
+                                    Id[0] = ixx * d[0] + ixy * d[1];
+                                    Id[1] = ixy * d[0] + iyy * d[1];
+                                    Id[2] = 0.0f;
+                                    tr = ixx + iyy;
+                                } else {
+                                    const float4 C = __ldg(&t.mq1[k]);   // {Iyy, Izz, Ixy, Ixz}
+                                    const float ixx = B.w, iyz = __ldg(&t.mq2[k]);
+                                    Id[0] = ixx * d[0] + C.z * d[1] + C.w * d[2];
+                                    Id[1] = C.z * d[0] + C.x * d[1] + iyz * d[2];
+                                    Id[2] = C.w * d[0] + iyz * d[1] + C.y * d[2];
+                                    tr = ixx + C.x + C.y;
+                                }
+                                float dId = d[0] * Id[0] + d[1] * Id[1];
+                                if (D == 3) dId += d[2] * Id[2];
+                                const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
+                                const float ci = -3.0f * inv5;
+    #pragma unroll
+                                for (int a = 0; a < D; a++) term[a] = cm * d[a] + ci * Id[a];
                             } else {
-                                const float4 C = __ldg(&t.mq1[k]);   // {Iyy, Izz, Ixy, Ixz}
-                                const float ixx = B.w, iyz = __ldg(&t.mq2[k]);
-                                Id[0] = ixx * d[0] + C.z * d[1] + C.w * d[2];
-                                Id[1] = C.z * d[0] + C.x * d[1] + iyz * d[2];
-                                Id[2] = C.w * d[0] + iyz * d[1] + C.y * d[2];
-                                tr = ixx + C.x + C.y;
+                                const float inv = rsqrt_approx(r2);
+                                const float fm = m * (inv * inv * inv);
+    #pragma unroll
+                                for (int a = 0; a < D; a++) term[a] = d[a] * fm;
                             }
-                            float dId = d[0] * Id[0] + d[1] * Id[1];
-                            if (D == 3) dId += d[2] * Id[2];
-                            const float cm = m * inv3 - 1.5f * tr * inv5 + 7.5f * dId * inv7;
-                            const float ci = -3.0f * inv5;
-#pragma unroll
-                            for (int a = 0; a < D; a++) term[a] = cm * d[a] + ci * Id[a];
+    #pragma unroll
+                            for (int a = 0; a < D; a++) {   // Kahan summation
+                                const float y = fsub(term[a], fc[a]);
+                                const float tt = fadd(f[a], y);
+                                fc[a] = fsub(fsub(tt, f[a]), y);
+                                f[a] = tt;
+                            }
+                        } else if (MODE == GE_PREC_EXACT) {
+                            const float inv = fdiv(1.0f, __fsqrt_rn(r2));
+                            const float inv3 = fmul(fmul(inv, inv), inv);
+                            const float fm = fmul(fmul(gm_i, m), inv3);
+    #pragma unroll
+                            for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(d[a], fm));
                         } else {
                             const float inv = rsqrt_approx(r2);
                             const float fm = m * (inv * inv * inv);
-#pragma unroll
-                            for (int a = 0; a < D; a++) term[a] = d[a] * fm;
+    #pragma unroll
+                            for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
                         }
-#pragma unroll
-                        for (int a = 0; a < D; a++) {   // Kahan summation
-                            const float y = fsub(term[a], fc[a]);
-                            const float tt = fadd(f[a], y);
-                            fc[a] = fsub(fsub(tt, f[a]), y);
-                            f[a] = tt;
-                        }
-                    } else if (MODE == GE_PREC_EXACT) {
-                        const float inv = fdiv(1.0f, __fsqrt_rn(r2));
-                        const float inv3 = fmul(fmul(inv, inv), inv);
-                        const float fm = fmul(fmul(gm_i, m), inv3);
-#pragma unroll
-                        for (int a = 0; a < D; a++) f[a] = fadd(f[a], fmul(d[a], fm));
-                    } else {
-                        const float inv = rsqrt_approx(r2);
-                        const float fm = m * (inv * inv * inv);
-#pragma unroll
-                        for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
+                        if (COUNT) cnt++;
                     }
-                    if (COUNT) cnt++;
+                } else {
+                    // eps2 > 0: the self term (d = 0) and massless sources add exactly
+                    // zero, so no test is needed for them
+                    const float inv = rsqrt_approx(r2);
+                    const float fm = acc ? m * (inv * inv * inv) : 0.0f;
+    #pragma unroll
+                    for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
                 }
-            } else {
-                // eps2 > 0: the self term (d = 0) and massless sources add exactly
-                // zero, so no test is needed for them
-                const float inv = rsqrt_approx(r2);
-                const float fm = acc ? m * (inv * inv * inv) : 0.0f;
-#pragma unroll
-                for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
+                // a valid skip lies past k; max() keeps k increasing whatever the
+                // layout holds, so the walk ends within end - begin entries
+                k = max(k + 1, acc && !part ? nxt_skip : k + 1);
             }
-            // a valid skip lies past k; max() keeps k increasing whatever the
-            // layout holds, so the walk ends within end - begin entries
-            k = max(k + 1, acc && !part ? nxt_skip : k + 1);
-        }
         };
         if (packed) walk_range(std::true_type{});
         else walk_range(std::false_type{});
