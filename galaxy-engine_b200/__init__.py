@@ -54,7 +54,7 @@ class Params(C.Structure):
         ("periodic", C.c_int32), ("domain", C.c_float * 3), ("track_prev_vel", C.c_int32),
         ("group_size", C.c_int32), ("temp_enabled", C.c_int32), ("heat_cond", C.c_float),
         ("direct_below", C.c_int32), ("direct_eps2", C.c_float), ("no_graph", C.c_int32),
-        ("reserved", C.c_int32),
+        ("walk_kind", C.c_int32),
     ]
 
 
@@ -140,6 +140,7 @@ SIGNATURES = {
                                _vp], C.c_int),
     "ge_download_temp": ([_vp, _vp], C.c_int),
     "ge_step": ([_vp, C.c_int32], C.c_int),
+    "ge_set_sort_wait_test": ([_vp, C.c_uint32, C.c_int32], C.c_int),
     "ge_profile_step": ([_vp], C.c_int),
     "ge_frame_host": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
     "ge_integrate_start": ([_vp], C.c_int),
@@ -508,6 +509,12 @@ class Simulation:
 
     def count_interactions(self, enable=True):
         self._check(lib().ge_set_count_interactions(self._h, 1 if enable else 0))
+
+    def set_sort_wait_test(self, spin_limit=0, withhold=False):
+        """Test hook of the bounded waits (ge_set_sort_wait_test): cap the
+        sort's look-back polls, and make the first tile withhold its counts
+        so that the waits run out (the next sort returns GE_ERR_TIMEOUT)."""
+        self._check(lib().ge_set_sort_wait_test(self._h, int(spin_limit), 1 if withhold else 0))
 
     def direct_sum_f64(self, idx):
         """FP64 direct-sum accelerations of the particles at indices idx of the

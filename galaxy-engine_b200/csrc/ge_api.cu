@@ -147,6 +147,9 @@ struct ge_ctx {
     int next_graph = 0;
     bool graph_failed = false;    // capture or instantiation refused: plain launches
     bool framed = false;          // a frame was enqueued (one-time launch setup done)
+    // ge_set_sort_wait_test: the sort's look-back poll cap and withheld tile,
+    // kept here so that a reallocation of the buffers keeps them
+    uint32_t sort_spin_limit = 0, sort_withhold = 0;
     ge_stats stats{};
     std::string err;
 };
@@ -211,6 +214,7 @@ StepParams step_params(const ge_ctx *c) {
     s.heat_cond = c->p.heat_cond;
     s.direct_eps2 = c->p.direct_eps2;
     s.mixed = c->p.precision == GE_PREC_MIXED ? 1 : 0;
+    s.walk_kind = c->p.walk_kind;
     for (int a = 0; a < 3; a++) {
         s.domain[a] = c->p.domain[a];
         s.half_domain[a] = c->p.domain[a] * 0.5f;
@@ -235,6 +239,7 @@ int validate(ge_ctx *c, const ge_params *p) {
         return fail(c, GE_ERR_UNSUPPORTED, "the direct sum runs in GE_PREC_EXACT and GE_PREC_FAST");
     if (p->direct_below > 0 && !(p->direct_eps2 > 0.0f && p->direct_eps2 < INFINITY))
         return fail(c, GE_ERR_ARG, "direct_eps2 must be positive and finite (the self term divides by it)");
+    if (p->walk_kind != 0 && p->walk_kind != 1) return fail(c, GE_ERR_ARG, "walk_kind must be 0 or 1");
     if (p->group_size != 0 && p->group_size != 32 && p->group_size != 64 && p->group_size != 128)
         return fail(c, GE_ERR_ARG, "group_size must be 0, 32, 64 or 128");
     if (p->periodic && (!(p->domain[0] > 0) || !(p->domain[1] > 0) ||
@@ -301,9 +306,11 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
         t.link = l;
     }
     GE_CHECK(c, dalloc(L, &t.slot_of, N));
+    GE_CHECK(c, dalloc(L, &t.nrange, (size_t)node_cap));
+    GE_CHECK(c, dalloc(L, &t.wctr, kWWCtrWords));
     GE_CHECK(c, dalloc(L, &t.level, kMaxLevels + 2));
     GE_CHECK(c, dalloc(L, &t.lvl_alloc, kMaxLevels + 2));
-    GE_CHECK(c, dalloc(L, &t.meta, 16));
+    GE_CHECK(c, dalloc(L, &t.meta, kMetaWords));
     GE_CHECK(c, dalloc(L, &t.tl, kTimeline));
     // key-prefix build
     GE_CHECK(c, dalloc(L, &t.kdl, N));
@@ -321,7 +328,7 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
         GE_CHECK(c, dalloc(L, &t.tv, N + (size_t)node_cap + 1));
     }
     nb.temp = temp;
-    if (!L.dry) GE_CHECK(c, cudaMemsetAsync(t.meta, 0, 16 * sizeof(uint32_t), c->stream));
+    if (!L.dry) GE_CHECK(c, cudaMemsetAsync(t.meta, 0, kMetaWords * sizeof(uint32_t), c->stream));
     GE_CHECK(c, dalloc(L, &nb.d_inter, 1));
     return GE_OK;
 }
@@ -480,6 +487,7 @@ int ensure_capacity(ge_ctx *c, int64_t n, int64_t S, bool keep, bool exact = fal
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
     free_all(ob.allocs);
     c->b = std::move(nb);
+    c->b.ss.spin_limit = c->sort_spin_limit;
     c->cur = 0;
     c->d_err = c->b.tree.meta + 4;
     c->tree_valid = false;
@@ -724,7 +732,7 @@ int enqueue_walk(ge_ctx *c, bool integrate_end) {
     if (!c->any_walk) return GE_OK;
     if (!c->p.temp_enabled) s.temp = nullptr;
     GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, s, p, c->g, mixed_view(c), integrate_end,
-                            cnt, c->d_err, c->stream));
+                            cnt, c->d_err, c->num_sms, c->stream));
     return GE_OK;
 }
 
@@ -935,7 +943,7 @@ int frame_overlapped(ge_ctx *c, int64_t n, const float *x, const float *y, const
                 p.i0 = (int)lo;
                 p.n = (int)hi;
                 GE_CHECK(c, launch_walk(c->p.dims, c->p.precision, ws, p, c->g, mixed_view(c), true,
-                                        nullptr, c->d_err, s0));
+                                        nullptr, c->d_err, c->num_sms, s0));
                 GE_CHECK(c, cudaEventRecord(c->xev[2], s0));
                 GE_CHECK(c, cudaStreamWaitEvent(s1, c->xev[2], 0));
                 GE_CHECK(c, back(lo, hi, s1));
@@ -1106,6 +1114,16 @@ int ge_get_stats(ge_ctx *c, ge_stats *out) {
     if (!c || !out) return GE_ERR_ARG;
     c->stats.n = c->n;
     *out = c->stats;
+    return GE_OK;
+}
+
+int ge_set_sort_wait_test(ge_ctx *c, uint32_t spin_limit, int32_t withhold) {
+    if (!c) return GE_ERR_ARG;
+    if (withhold != 0 && withhold != 1) return fail(c, GE_ERR_ARG, "withhold must be 0 or 1");
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    c->sort_spin_limit = spin_limit;
+    c->sort_withhold = (uint32_t)withhold;
+    c->b.ss.spin_limit = spin_limit;
     return GE_OK;
 }
 
@@ -1464,7 +1482,12 @@ int ge_sort_by_morton_key(ge_ctx *c, uint32_t *perm_out) {
     int rc = require_state(c);
     if (rc) return rc;
     if (!c->keys_valid) return fail(c, GE_ERR_STATE, "compute the Morton keys first");
-    if ((rc = enqueue_sort(c))) return rc;
+    // the wait test's withheld tile applies to this stage call only (a whole
+    // frame would go on to build on an unsorted order)
+    c->b.ss.withhold_first = c->sort_withhold;
+    rc = enqueue_sort(c);
+    c->b.ss.withhold_first = 0u;
+    if (rc) return rc;
     if ((rc = enqueue_permute(c, true))) return rc;
     c->keys_valid = false;
     c->tree_valid = false;

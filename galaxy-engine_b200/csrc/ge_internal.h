@@ -86,6 +86,8 @@ struct Tree {
     float4 *src;          // [n + cap + 1]
     void *link;           // [n + cap + 1] uint32 (2D) / uint2 (3D)
     uint32_t *slot_of;    // [n]
+    uint2 *nrange;        // [cap] each node slot's {layout entry, subtree successor}
+    uint32_t *wctr;       // [kWWCtrWords] warp walk: chunk counter, fallback count
     uint32_t *level;      // [kMaxLevels + 2]
     uint32_t *lvl_alloc;  // [kMaxLevels + 2] per-level child allocation counters
     uint32_t *meta;       // [8] {node_count, levels, bar_count, bar_gen, err, small,
@@ -174,6 +176,12 @@ struct SortScratch {
     uint32_t *status;      // [passes][tiles][radix] decoupled look-back words
     uint32_t *tile_ctr;    // [8]
     int box_blocks;        // grid of the kick/box kernel
+    // look-back polls of a radix pass before it gives up (0: kSpinLimit)
+    uint32_t spin_limit;
+    // test hook (ge_set_sort_wait_test): 1 = the first tile of every pass
+    // keeps its digit counts to itself, so the look-back waits of the tiles
+    // after it run out and the sort reports GE_ERR_TIMEOUT
+    uint32_t withhold_first;
 };
 
 struct StepParams {
@@ -189,6 +197,7 @@ struct StepParams {
     float direct_eps2;   // value the direct sum adds to r^2
     int i0;              // the per-particle walk: first particle (up to n), 0 by default
     int mixed;           // GE_PREC_MIXED: the moment pass rewrites the node entries
+    int walk_kind;       // GE_PREC_FAST: 0 per-particle walk, 1 warp-cooperative walk
 };
 
 // 2D walk entries {x, y, m, w}.  Plain layout: w = size^2 (-1 for a particle,
@@ -202,6 +211,10 @@ struct StepParams {
 // (L <= 46).
 constexpr int kMetaWalkPacked = 13;
 constexpr int kMetaBigRoot = 14;   // tree meta word: some simulation's root size >= 1e19
+constexpr int kMetaWords = 32;     // tree meta words allocated
+// warp-cooperative walk counters (Tree::wctr, zeroed before each launch): the
+// chunk counter and the count of chunks that fell back to the per-particle walk
+constexpr int kWWCtrWords = 2;
 __device__ __forceinline__ float packed_size2(uint32_t w_bits, uint32_t rs2_bits) {
     return __uint_as_float(rs2_bits - ((w_bits >> 2) & 0x3F000000u));   // exponent - 2L
 }
@@ -297,10 +310,18 @@ cudaError_t launch_group_walk(int dims, const State &s, const StepParams &p, con
 cudaError_t launch_direct(int dims, int precision, const State &s, const StepParams &p,
                           const Segs &g, const uint2 *tiles, int64_t ntiles, bool integrate_end,
                           cudaStream_t st);
-// tree walk; integrate_end fuses integrateEnd (v += a*dt/2)
+// tree walk; integrate_end fuses integrateEnd (v += a*dt/2).  With
+// p.walk_kind == 1, GE_PREC_FAST with eps2 > 0 and without periodic wrap or
+// heat exchange runs the warp-cooperative walk (ge_wwalk.cu); everything else
+// the per-particle walk (ge_walk.cu)
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
                         const Segs &g, const Tree &t, bool integrate_end,
-                        unsigned long long *inter_count, uint32_t *err, cudaStream_t st);
+                        unsigned long long *inter_count, uint32_t *err, int num_sms,
+                        cudaStream_t st);
+// the warp-cooperative FAST walk of particles [p.i0, p.n) (ge_wwalk.cu)
+cudaError_t launch_warp_walk(int dims, const State &s, const StepParams &p, const Segs &g,
+                             const Tree &t, bool integrate_end, unsigned long long *inter_count,
+                             uint32_t *err, int num_sms, cudaStream_t st);
 cudaError_t launch_integrate_end(int dims, const State &s, const StepParams &p, cudaStream_t st);
 // gravity field display: strength (and RGBA8 colour) of every cell
 cudaError_t launch_field(const State &s, uint32_t lo, uint32_t hi, int amount_x, int amount_y,

@@ -24,7 +24,6 @@ namespace {
 
 constexpr int64_t kNoAllocMaxN = GE_NOALLOC_MAX_N;
 constexpr int64_t kNoAllocTiles = (kNoAllocMaxN + kSortTile - 1) / kSortTile;
-constexpr int kNoAllocBoxBlocks = 148 * 4;
 
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // byte offsets inside the scratch array
@@ -46,24 +45,31 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 static unsigned char *g_scratch_dev[kMaxDevices];
+static int g_sms_dev[kMaxDevices];   // SM count of each device (sizes the box grid)
 static std::mutex g_scratch_mu;
 
-// Device address of the scratch array on the current device.  In host code
-// the array's name is only a host-side stand-in, so the address must come from
-// cudaGetSymbolAddress, made once per device with that device current.
-cudaError_t scratch_for_current_device(unsigned char **out) {
+// Device address of the scratch array on the current device, and that
+// device's SM count.  In host code the array's name is only a host-side
+// stand-in, so the address must come from cudaGetSymbolAddress, made once per
+// device with that device current.
+cudaError_t scratch_for_current_device(unsigned char **out, int *sms) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (!g_scratch_dev[dev]) {
+        int count = 0;
+        e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
+        g_sms_dev[dev] = count > 0 ? count : 1;
         g_scratch_dev[dev] = (unsigned char *)p;
     }
     *out = g_scratch_dev[dev];
+    *sms = g_sms_dev[dev];
     return cudaSuccess;
 }
 
@@ -77,7 +83,8 @@ extern "C" int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const floa
     if (n < 1 || !d_x || !d_y || !d_perm) return GE_ERR_ARG;
     if (n > kNoAllocMaxN) return GE_ERR_CAPACITY;
     unsigned char *base = nullptr;
-    if (scratch_for_current_device(&base) != cudaSuccess) return GE_ERR_CUDA;
+    int sms = 0;
+    if (scratch_for_current_device(&base, &sms) != cudaSuccess) return GE_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
 
     SortScratch ss{};
@@ -88,8 +95,11 @@ extern "C" int ge_morton_sort_2d_noalloc(int64_t n, const float *d_x, const floa
     ss.status = (uint32_t *)(base + kOffStatus);
     ss.tile_ctr = (uint32_t *)(base + kOffTileCtr);
     const int64_t tiles = (n + kSortTile - 1) / kSortTile;
-    const int64_t blocks = tiles < kNoAllocBoxBlocks ? tiles : kNoAllocBoxBlocks;
-    ss.box_blocks = (int)blocks;
+    // the box grid as a context sizes it: one block per kBBoxThreads *
+    // kBoxItems particles, at most four per SM
+    int64_t blocks = (n + kBBoxThreads * kBoxItems - 1) / (kBBoxThreads * kBoxItems);
+    if (blocks > (int64_t)sms * 4) blocks = (int64_t)sms * 4;
+    ss.box_blocks = (int)(blocks < 1 ? 1 : blocks);
     uint32_t *err = (uint32_t *)(base + kOffErr);
 
     // one segment: every particle belongs to it, so no segment tables

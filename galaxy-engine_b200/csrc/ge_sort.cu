@@ -160,9 +160,10 @@ __global__ void __launch_bounds__(kSortThreads)
 k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
              const uint32_t *__restrict__ vin, uint32_t *__restrict__ vout, int n, int shift,
              Segs g, const uint32_t *__restrict__ hist, uint32_t *status, uint32_t *tile_ctr,
-             uint32_t *err) {
+             uint32_t *err, uint32_t spin_limit, uint32_t withhold_first) {
     dep_wait();
     constexpr int R = 1 << BITS;
+    const uint32_t max_spins = spin_limit ? spin_limit : kSpinLimit;
     __shared__ uint32_t s_whist[kSortWarps][R];
     __shared__ uint32_t s_off[R];
     __shared__ uint32_t s_scan[kSortWarps];
@@ -229,7 +230,9 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
         volatile uint32_t *st = status;
         uint32_t excl = 0;
         if (tile == tile0) {
-            st[(int64_t)tile * R + d] = kFlagInc | sum;
+            // (withheld only under the test hook: the first tile of the whole
+            // sort then never publishes, and every later wait on it is bounded)
+            if (!(withhold_first && tile == 0)) st[(int64_t)tile * R + d] = kFlagInc | sum;
         } else {
             st[(int64_t)tile * R + d] = kFlagAgg | sum;
             // look back kLookBack tiles per round trip: the words are read at
@@ -254,7 +257,7 @@ k_radix_pass(const uint64_t *__restrict__ kin, uint64_t *__restrict__ kout,
                 }
                 if (done) break;
                 t -= j;
-                if (j < m && ++spins > kSpinLimit) { set_err(err, kErrSpin); break; }
+                if (j < m && ++spins > max_spins) { set_err(err, kErrSpin); break; }
             }
             st[(int64_t)tile * R + d] = kFlagInc | ((excl + sum) & kValMask);
         }
@@ -413,10 +416,12 @@ cudaError_t launch_sort(int dims, int n, const Segs &g, SortScratch &ss, uint32_
         const cudaError_t e =
             dims == 2 ? launch_dep(k_radix_pass<false, kKeyBits>, tiles, kSortThreads, st,
                                    ss.keys[cur], ss.keys[cur ^ 1], no_vin, no_vout, n, shift, g,
-                                   hist, status, ss.tile_ctr + ps, err)
+                                   hist, status, ss.tile_ctr + ps, err, ss.spin_limit,
+                                   ss.withhold_first)
                       : launch_dep(k_radix_pass<true, kKeyBits>, tiles, kSortThreads, st,
                                    ss.keys[cur], ss.keys[cur ^ 1], ss.vals[cur], ss.vals[cur ^ 1],
-                                   n, shift, g, hist, status, ss.tile_ctr + ps, err);
+                                   n, shift, g, hist, status, ss.tile_ctr + ps, err,
+                                   ss.spin_limit, ss.withhold_first);
         if (e != cudaSuccess) return e;
         cur ^= 1;
     }
@@ -438,7 +443,7 @@ cudaError_t launch_radix_words(uint64_t *const words[2], int n, int shift0, int 
         constexpr int R = 1 << kWordBits;
         k_radix_pass<false, kWordBits><<<(unsigned)(tiles < 1 ? 1 : tiles), kSortThreads, 0, st>>>(
             words[cur], words[cur ^ 1], nullptr, nullptr, n, shift0 + kWordBits * ps, one,
-            hist + (size_t)ps * R, status + ps * tiles * R, tile_ctr + ps, err);
+            hist + (size_t)ps * R, status + ps * tiles * R, tile_ctr + ps, err, 0u, 0u);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         cur ^= 1;

@@ -667,6 +667,7 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
         return;
     }
     t.aux[k].w = me;   // the node's entry (read by the moment pass)
+    t.nrange[k] = make_uint2(me, skip);   // its layout range (read by the warp walk)
     if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
         g.root_begin[k] = me;
         g.root_end[k] = skip;

@@ -290,9 +290,15 @@ static cudaError_t walk_mode(const State &s, const StepParams &p, const Segs &g,
 
 cudaError_t launch_walk(int dims, int precision, const State &s, const StepParams &p,
                         const Segs &g, const Tree &t, bool integrate_end,
-                        unsigned long long *inter_count, uint32_t *err, cudaStream_t st) {
+                        unsigned long long *inter_count, uint32_t *err, int num_sms,
+                        cudaStream_t st) {
     const int ie = integrate_end ? 1 : 0;
     const bool exact = precision == GE_PREC_EXACT;
+    // (the warp walk stages a particle's own term with its leaf, which adds
+    // zero only with eps2 > 0)
+    if (p.walk_kind == 1 && precision == GE_PREC_FAST && !p.periodic && !(s.temp && t.tv) &&
+        p.eps2 > 0.0f)
+        return launch_warp_walk(dims, s, p, g, t, integrate_end, inter_count, err, num_sms, st);
     if (precision == GE_PREC_MIXED)
         return dims == 2 ? walk_mode<2, GE_PREC_MIXED>(s, p, g, t, ie, inter_count, err, st)
                          : walk_mode<3, GE_PREC_MIXED>(s, p, g, t, ie, inter_count, err, st);

@@ -88,7 +88,14 @@ typedef struct {
                                 in 2D and 3D (physics.cpp:422, physics3D.cpp:455) */
     int32_t no_graph;        /* 1: ge_step launches every kernel itself; 0 (default):
                                 pairs of steps replay a captured CUDA graph */
-    int32_t reserved;
+    int32_t walk_kind;       /* GE_PREC_FAST tree walk (same interaction set either way):
+                                0 (default) every particle walks the depth-first layout
+                                on its own; 1 the 32 particles of a warp walk together
+                                (a shared node stack, nodes decided for the whole warp
+                                against its bounding box, a staged source list, per-
+                                particle walks only for the undecided subtrees); 1
+                                needs eps2 > 0 and no periodic wrap or heat exchange,
+                                otherwise the per-particle walk runs */
 } ge_params;
 
 typedef struct {
@@ -205,6 +212,18 @@ int ge_compute_forces(ge_ctx *ctx);
 int ge_integrate_end(ge_ctx *ctx);
 /* enable per-particle interaction counting in ge_compute_forces (stats) */
 int ge_set_count_interactions(ge_ctx *ctx, int32_t enable);
+/* Test hook for the failure path of the bounded device-side waits (no
+   counterpart in the reference, whose GL path only prints shader errors,
+   globalLogic.cpp:601-615).  spin_limit caps every look-back wait of the key
+   sort at that many polls (0 restores the default, 2^22).  withhold = 1
+   makes the first tile of every pass of ge_sort_by_morton_key keep its digit
+   counts to itself, so the waits of the tiles after it run out: that call
+   returns GE_ERR_TIMEOUT and the particle state is unspecified until the
+   next ge_upload (the frame calls, ge_step and ge_frame_host, never
+   withhold).  Nothing faults or hangs: every wait is bounded, and the sort's
+   scatter and gather stay inside their arrays whatever the waits found.
+   withhold = 0 restores normal operation.  Kept across reallocations. */
+int ge_set_sort_wait_test(ge_ctx *ctx, uint32_t spin_limit, int32_t withhold);
 
 /* --- trajectory preview ------------------------------------------------
  * ParticlesSpawning::predictTrajectory (particlesSpawning.cpp:443-500, 3D

@@ -25,6 +25,16 @@ def _context_result(ge, st):
     return perm, keys[perm]
 
 
+def _oracle_result(st):
+    """The oracle's statement of the reference's box, keys and sort
+    (globalLogic.cpp:1083-1099, morton.cpp:27-63), stable on equal keys."""
+    import oracle as O
+    bb = O.bbox(st["x"], st["y"])
+    keys = O.morton_keys(st["x"], st["y"], bb)
+    perm = O.sort_perm(keys)
+    return perm, keys[perm]
+
+
 def test_noalloc_sort_matches_context_path_twice_in_a_row(ge):
     import torch
     ics = importlib.import_module("galaxy-engine_b200.ics")
@@ -34,6 +44,8 @@ def test_noalloc_sort_matches_context_path_twice_in_a_row(ge):
     for n, seed in ((ge.NOALLOC_MAX_N, 3), (100003, 4)):
         st = ics.two_disks2d(n, seed=seed)
         perm_ref, keys_ref = _context_result(ge, st)
+        perm_or, keys_or = _oracle_result(st)
+        assert np.array_equal(perm_ref, perm_or) and np.array_equal(keys_ref, keys_or), n
         x = torch.from_numpy(st["x"]).cuda()
         y = torch.from_numpy(st["y"]).cuda()
         perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
@@ -49,6 +61,24 @@ def test_noalloc_sort_matches_context_path_twice_in_a_row(ge):
             torch.cuda.synchronize()
             assert np.array_equal(perm.cpu().numpy().view(np.uint32), perm_ref), (n, call)
             assert np.array_equal(keys.cpu().numpy().view(np.uint64), keys_ref), (n, call)
+
+
+def test_noalloc_sort_without_keys_output(ge):
+    """d_keys is optional: a NULL keys pointer gives the same permutation."""
+    import torch
+    ics = importlib.import_module("galaxy-engine_b200.ics")
+    n = 5000
+    st = ics.disk2d(n, seed=9)
+    perm_ref, _ = _context_result(ge, st)
+    x = torch.from_numpy(st["x"]).cuda()
+    y = torch.from_numpy(st["y"]).cuda()
+    perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = ge.lib().ge_morton_sort_2d_noalloc(n, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                            C.c_void_p(perm.data_ptr()), None, C.c_void_p(stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(perm.cpu().numpy().view(np.uint32), perm_ref)
 
 
 def test_noalloc_sort_rejects_sizes_beyond_the_limit(ge):
