@@ -45,6 +45,10 @@ class GeError(RuntimeError):
         self.code = code
 
 
+STATE_KEYS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m", "id", "kx", "ky", "kz",
+              "kvx", "kvy", "kvz", "pvx", "pvy", "pvz", "temp", "pinned")
+
+
 class Params(C.Structure):
     """ge_params (include/ge_bh.h)."""
     _fields_ = [
@@ -65,6 +69,18 @@ class Stats(C.Structure):
         ("interactions", C.c_uint64), ("bbox", C.c_float * 4), ("ms_last_step", C.c_float),
         ("stage_ms", C.c_float * 8),
     ]
+
+
+class StateArrays(C.Structure):
+    """ge_state_arrays (include/ge_bh.h): host arrays of a checkpoint."""
+    _fields_ = [(k, C.c_void_p) for k in STATE_KEYS]
+
+
+class AosLayout(C.Structure):
+    """ge_aos_layout (include/ge_bh.h): byte offsets of the record members."""
+    _fields_ = [(k, C.c_int32) for k in ("stride", "off_pos", "off_vel", "off_acc",
+                                          "off_prev_vel", "off_mass", "off_id", "off_temp",
+                                          "r_stride", "r_off_pinned")]
 
 
 class ServerConfig(C.Structure):
@@ -140,6 +156,10 @@ SIGNATURES = {
                                _vp], C.c_int),
     "ge_download_temp": ([_vp, _vp], C.c_int),
     "ge_step": ([_vp, C.c_int32], C.c_int),
+    "ge_download_state": ([_vp, C.POINTER(StateArrays)], C.c_int),
+    "ge_aos_layout_default": ([C.POINTER(AosLayout), C.c_int], None),
+    "ge_frame_aos": ([_vp, C.c_int64, _vp, _vp, C.POINTER(AosLayout), _vp], C.c_int),
+    "ge_upload_state": ([_vp, C.c_int64, C.POINTER(StateArrays)], C.c_int),
     "ge_set_sort_wait_test": ([_vp, C.c_uint32, C.c_int32], C.c_int),
     "ge_profile_step": ([_vp], C.c_int),
     "ge_frame_host": ([_vp, C.c_int64] + [_vp] * 11, C.c_int),
@@ -297,6 +317,48 @@ class Simulation:
                                     _ptr(arrs["vx"]), _ptr(arrs["vy"]), _ptr(arrs["vz"]),
                                     _ptr(arrs["m"]), _ptr(ids), _ptr(arrs["ax"]),
                                     _ptr(arrs["ay"]), _ptr(arrs["az"])))
+        self.n = n
+
+    def frame_aos(self, phys, rend=None, layout=None, order=True):
+        """One frame on the reference's particle records (ge_frame_aos):
+        phys / rend are numpy byte-record arrays (updated in place, in their
+        own order); returns the Morton order (slot -> record) when asked."""
+        if layout is None:
+            layout = aos_layout(self.dims)
+        phys = np.ascontiguousarray(phys)
+        n = len(phys)
+        out = np.zeros(n, np.uint32) if order else None
+        self._check(lib().ge_frame_aos(self._h, n, _ptr(phys), _ptr(rend), C.byref(layout),
+                                       _ptr(out)))
+        self.n = n
+        return out
+
+    def download_state(self):
+        """Checkpoint: every term the next step reads (ge_download_state), as
+        a dict of host arrays in the current particle order."""
+        n = self.n
+        out = {}
+        for k in STATE_KEYS:
+            if k in ("z", "vz", "az", "kz", "kvz", "pvz") and self.dims == 2:
+                continue
+            out[k] = np.zeros(n, np.uint32 if k == "id" else np.uint8 if k == "pinned" else np.float32)
+        arr = StateArrays(*[_ptr(out.get(k)) for k in STATE_KEYS])
+        self._check(lib().ge_download_state(self._h, C.byref(arr)))
+        return out
+
+    def upload_state(self, state):
+        """Resume from download_state()'s dict (ge_upload_state); keys that
+        are missing are left out."""
+        conv = {k: (np.ascontiguousarray(v, np.uint32) if k == "id" else
+                    np.ascontiguousarray(v, np.uint8) if k == "pinned" else _f32(v))
+                for k, v in state.items() if k in STATE_KEYS and v is not None}
+        n = len(conv["x"])
+        if self.params.precision != PREC_MIXED:
+            for k in ("kx", "ky", "kz", "kvx", "kvy", "kvz"):
+                conv.pop(k, None)
+        self._keep = conv
+        arr = StateArrays(*[_ptr(conv.get(k)) for k in STATE_KEYS])
+        self._check(lib().ge_upload_state(self._h, n, C.byref(arr)))
         self.n = n
 
     def upload_pinned(self, pinned):
@@ -560,6 +622,13 @@ class Simulation:
                                          _ptr(out["child"])))
         k = cnt.value
         return {a: v[:k] for a, v in out.items()}
+
+
+def aos_layout(dims):
+    """The reference's record layout (ge_aos_layout_default)."""
+    L = AosLayout()
+    lib().ge_aos_layout_default(C.byref(L), dims)
+    return L
 
 
 def estimate_bytes(params, n, sims=1):

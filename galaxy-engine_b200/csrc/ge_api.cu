@@ -150,6 +150,11 @@ struct ge_ctx {
     // ge_set_sort_wait_test: the sort's look-back poll cap and withheld tile,
     // kept here so that a reallocation of the buffers keeps them
     uint32_t sort_spin_limit = 0, sort_withhold = 0;
+    // ge_frame_aos: device copies of the caller's records and the order output
+    unsigned char *d_aos = nullptr, *d_aos_r = nullptr;
+    size_t aos_bytes = 0, aos_r_bytes = 0;
+    uint32_t *d_order = nullptr;
+    int64_t order_cap = 0;
     ge_stats stats{};
     std::string err;
 };
@@ -974,6 +979,44 @@ int frame_overlapped(ge_ctx *c, int64_t n, float *x, float *y, float *z, float *
                             ay, az, m, id);
 }
 
+// Temperature arrays (both state buffers, zeroed) and the node temperature
+// arrays, when the context has none yet.
+int ensure_temp(ge_ctx *c) {
+    if (c->b.temp) return GE_OK;
+    auto &L = c->b.allocs;
+    const size_t N = (size_t)c->b.cap_n;
+    for (int k = 0; k < 2; k++) {
+        GE_CHECK(c, dalloc(L, &c->b.st[k].temp, N));
+        GE_CHECK(c, cudaMemsetAsync(c->b.st[k].temp, 0, sizeof(float) * N, c->stream));
+    }
+    GE_CHECK(c, dalloc(L, &c->b.tree.ntemp, (size_t)c->b.tree.cap));
+    GE_CHECK(c, dalloc(L, &c->b.tree.tv, N + (size_t)c->b.tree.cap + 1));
+    c->b.temp = true;
+    return GE_OK;
+}
+
+// Pin flag arrays (both state buffers), when the context has none yet.
+int ensure_pinned(ge_ctx *c) {
+    if (c->b.pinned) return GE_OK;
+    for (int k = 0; k < 2; k++)
+        GE_CHECK(c, dalloc(c->b.allocs, &c->b.st[k].pinned, (size_t)c->b.cap_n));
+    c->b.pinned = true;
+    return GE_OK;
+}
+
+// A device buffer of at least `bytes`, grown (and its contents dropped) when
+// too small.
+int ensure_bytes(ge_ctx *c, unsigned char **buf, size_t *have, size_t bytes) {
+    if (*have >= bytes && *buf) return GE_OK;
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+    GE_CHECK(c, cudaMalloc((void **)buf, bytes));
+    *have = bytes;
+    return GE_OK;
+}
+
 int find_sim(ge_ctx *c, int32_t handle) {
     for (size_t k = 0; k < c->sims.size(); k++)
         if (c->sims[k].handle == handle) return (int)k;
@@ -1052,6 +1095,9 @@ int ge_destroy(ge_ctx *c) {
     }
     for (auto &e : c->xev) if (e) cudaEventDestroy(e);
     if (c->h_meta) cudaFreeHost(c->h_meta);
+    if (c->d_aos) cudaFree(c->d_aos);
+    if (c->d_aos_r) cudaFree(c->d_aos_r);
+    if (c->d_order) cudaFree(c->d_order);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return GE_OK;
@@ -1156,11 +1202,7 @@ int ge_upload_pinned(ge_ctx *c, const uint8_t *pinned) {
         c->has_pinned = false;
         return GE_OK;
     }
-    if (!c->b.pinned) {
-        for (int k = 0; k < 2; k++)
-            GE_CHECK(c, dalloc(c->b.allocs, &c->b.st[k].pinned, (size_t)c->b.cap_n));
-        c->b.pinned = true;
-    }
+    if ((rc = ensure_pinned(c))) return rc;
     GE_CHECK(c, cudaMemcpyAsync(c->b.st[c->cur].pinned, pinned, (size_t)c->n,
                                 cudaMemcpyHostToDevice, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
@@ -1173,17 +1215,7 @@ int ge_upload_temp(ge_ctx *c, const float *temp) {
     if (rc) return rc;
     if (!temp) return fail(c, GE_ERR_ARG, "temp is NULL");
     if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
-    if (!c->b.temp) {
-        auto &L = c->b.allocs;
-        const size_t N = (size_t)c->b.cap_n;
-        for (int k = 0; k < 2; k++) {
-            GE_CHECK(c, dalloc(L, &c->b.st[k].temp, N));
-            GE_CHECK(c, cudaMemsetAsync(c->b.st[k].temp, 0, sizeof(float) * N, c->stream));
-        }
-        GE_CHECK(c, dalloc(L, &c->b.tree.ntemp, (size_t)c->b.tree.cap));
-        GE_CHECK(c, dalloc(L, &c->b.tree.tv, N + (size_t)c->b.tree.cap + 1));
-        c->b.temp = true;
-    }
+    if ((rc = ensure_temp(c))) return rc;
     GE_CHECK(c, cudaMemcpyAsync(c->b.st[c->cur].temp, temp, sizeof(float) * (size_t)c->n,
                                 cudaMemcpyHostToDevice, c->stream));
     GE_CHECK(c, cudaStreamSynchronize(c->stream));
@@ -1207,6 +1239,163 @@ int ge_download(ge_ctx *c, float *x, float *y, float *z, float *vx, float *vy, f
     int rc = require_state(c);
     if (rc) return rc;
     return get_host(c, 0, c->n, x, y, z, vx, vy, vz, ax, ay, az, m, id);
+}
+
+void ge_aos_layout_default(ge_aos_layout *l, int dims) {
+    if (!l) return;
+    // member offsets of the reference's records (include/Particles/particle.h):
+    // ParticlePhysics 128 B, ParticlePhysics3D 160 B, ParticleRendering[3D] 60 B
+    if (dims == 3) *l = ge_aos_layout{160, 0, 12, 24, 48, 96, 148, 136, 60, 56};
+    else *l = ge_aos_layout{128, 0, 8, 16, 32, 64, 116, 104, 60, 56};
+}
+
+int ge_frame_aos(ge_ctx *c, int64_t n, void *phys, const void *rend, const ge_aos_layout *L,
+                 uint32_t *order) {
+    if (!c) return GE_ERR_ARG;
+    if (c->pending_steps) return fail(c, GE_ERR_STATE, "ge_step_wait first");
+    if (n < 1 || !phys || !L) return fail(c, GE_ERR_ARG, "records and layout are required");
+    const int D = c->p.dims;
+    const int vec = 4 * D;
+    auto member_ok = [&](int32_t off, int bytes) {
+        return off >= 0 && off % 4 == 0 && (int64_t)off + bytes <= L->stride;
+    };
+    if (L->stride < 4 || L->stride % 4 != 0 || !member_ok(L->off_pos, vec) ||
+        !member_ok(L->off_vel, vec) || !member_ok(L->off_acc, vec) || !member_ok(L->off_mass, 4) ||
+        !member_ok(L->off_id, 4) || (L->off_prev_vel != -1 && !member_ok(L->off_prev_vel, vec)) ||
+        (L->off_temp != -1 && !member_ok(L->off_temp, 4)))
+        return fail(c, GE_ERR_ARG, "record layout: offsets must be 4-byte aligned members inside the stride");
+    const bool pins = rend && L->r_off_pinned >= 0;
+    if (pins && !(L->r_stride >= 1 && L->r_off_pinned < L->r_stride))
+        return fail(c, GE_ERR_ARG, "record layout: isPinned outside the rendering record");
+    const bool temps = c->p.temp_enabled && L->off_temp >= 0;
+    const bool prevs = c->p.track_prev_vel && L->off_prev_vel >= 0;
+    int rc;
+    if ((rc = ensure_capacity(c, n, 1, false))) return rc;
+    if ((rc = ensure_bytes(c, &c->d_aos, &c->aos_bytes, (size_t)n * L->stride))) return rc;
+    if (pins && (rc = ensure_bytes(c, &c->d_aos_r, &c->aos_r_bytes, (size_t)n * L->r_stride)))
+        return rc;
+    if (order && c->order_cap < n) {
+        GE_CHECK(c, cudaStreamSynchronize(c->stream));
+        if (c->d_order) cudaFree(c->d_order);
+        c->d_order = nullptr;
+        c->order_cap = 0;
+        GE_CHECK(c, cudaMalloc((void **)&c->d_order, sizeof(uint32_t) * (size_t)n));
+        c->order_cap = n;
+    }
+    if (pins && (rc = ensure_pinned(c))) return rc;
+    if (temps && (rc = ensure_temp(c))) return rc;
+    if ((rc = ensure_mode(c))) return rc;
+    // as ge_upload: one simulation, restarting its step count
+    c->cur = 0;
+    c->has_pinned = pins;
+    c->n = n;
+    c->sims.assign(1, SimRec{c->next_handle++, n, c->total_steps});
+    c->tree_valid = false;
+    c->keys_valid = false;
+    if ((rc = sync_segments(c))) return rc;
+    cudaStream_t st = c->stream;
+    GE_CHECK(c, cudaMemcpyAsync(c->d_aos, phys, (size_t)n * L->stride, cudaMemcpyHostToDevice, st));
+    if (pins)
+        GE_CHECK(c, cudaMemcpyAsync(c->d_aos_r, rend, (size_t)n * L->r_stride,
+                                    cudaMemcpyHostToDevice, st));
+    State s = c->b.st[c->cur];
+    if (!pins) s.pinned = nullptr;
+    if (!temps) s.temp = nullptr;
+    if (!c->b.prev) s.pvx = s.pvy = s.pvz = nullptr;
+    GE_CHECK(c, launch_aos_in(D, c->d_aos, pins ? c->d_aos_r : nullptr, *L, (int)n, s, st));
+    {   // the mixed mode's compensation terms start at zero, as after ge_upload
+        const State &sb = c->b.st[c->cur];
+        float *kp[6] = {sb.kx, sb.ky, sb.kz, sb.kvx, sb.kvy, sb.kvz};
+        for (float *q : kp)
+            if (q) GE_CHECK(c, cudaMemsetAsync(q, 0, sizeof(float) * (size_t)n, st));
+    }
+    GE_CHECK(c, cudaEventRecord(c->ev[6], st));
+    if ((rc = enqueue_frame(c, nullptr))) return rc;
+    GE_CHECK(c, cudaEventRecord(c->ev[7], st));
+    State o = c->b.st[c->cur];
+    if (!temps) o.temp = nullptr;
+    if (!prevs) o.pvx = o.pvy = o.pvz = nullptr;
+    GE_CHECK(c, launch_aos_out(D, c->d_aos, *L, (int)n, o, c->b.ss, st));
+    // the byte span of each record that the frame changed, one pitched copy
+    int32_t lo = std::min(L->off_pos, std::min(L->off_vel, L->off_acc));
+    int32_t hi = std::max(L->off_pos, std::max(L->off_vel, L->off_acc)) + vec;
+    if (prevs) { lo = std::min(lo, L->off_prev_vel); hi = std::max(hi, L->off_prev_vel + vec); }
+    if (temps) { lo = std::min(lo, L->off_temp); hi = std::max(hi, L->off_temp + 4); }
+    GE_CHECK(c, cudaMemcpy2DAsync((unsigned char *)phys + lo, (size_t)L->stride, c->d_aos + lo,
+                                  (size_t)L->stride, (size_t)(hi - lo), (size_t)n,
+                                  cudaMemcpyDeviceToHost, st));
+    if (order) {
+        GE_CHECK(c, launch_perm_out(D, (int)n, c->b.ss, c->d_order, st));
+        GE_CHECK(c, cudaMemcpyAsync(order, c->d_order, sizeof(uint32_t) * (size_t)n,
+                                    cudaMemcpyDeviceToHost, st));
+    }
+    rc = check_device(c);   // synchronises the stream
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+    c->stats.ms_last_step = ms;
+    c->stats.steps += 1;
+    c->total_steps += 1;
+    c->tree_valid = rc == GE_OK;
+    return rc;
+}
+
+int ge_download_state(ge_ctx *c, const ge_state_arrays *h) {
+    int rc = require_state(c);
+    if (rc) return rc;
+    if (!h) return fail(c, GE_ERR_ARG, "state arrays are NULL");
+    if ((rc = get_host(c, 0, c->n, h->x, h->y, h->z, h->vx, h->vy, h->vz, h->ax, h->ay, h->az,
+                       h->m, h->id)))
+        return rc;
+    const State &s = c->b.st[c->cur];
+    const bool d3 = c->p.dims == 3;
+    const size_t B = sizeof(float) * (size_t)c->n;
+    struct { float *h; const float *d; } cp[] = {
+        {h->kx, c->b.mixed ? s.kx : nullptr}, {h->ky, c->b.mixed ? s.ky : nullptr},
+        {d3 ? h->kz : nullptr, c->b.mixed ? s.kz : nullptr},
+        {h->kvx, c->b.mixed ? s.kvx : nullptr}, {h->kvy, c->b.mixed ? s.kvy : nullptr},
+        {d3 ? h->kvz : nullptr, c->b.mixed ? s.kvz : nullptr},
+        {h->pvx, c->b.prev ? s.pvx : nullptr}, {h->pvy, c->b.prev ? s.pvy : nullptr},
+        {d3 ? h->pvz : nullptr, c->b.prev ? s.pvz : nullptr},
+        {h->temp, c->b.temp ? s.temp : nullptr}};
+    for (auto &q : cp) {
+        if (!q.h) continue;
+        if (q.d) GE_CHECK(c, cudaMemcpyAsync(q.h, q.d, B, cudaMemcpyDeviceToHost, c->stream));
+        else std::memset(q.h, 0, B);
+    }
+    if (h->pinned) {
+        if (c->has_pinned)
+            GE_CHECK(c, cudaMemcpyAsync(h->pinned, s.pinned, (size_t)c->n, cudaMemcpyDeviceToHost,
+                                        c->stream));
+        else std::memset(h->pinned, 0, (size_t)c->n);
+    }
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    return GE_OK;
+}
+
+int ge_upload_state(ge_ctx *c, int64_t n, const ge_state_arrays *h) {
+    if (!c) return GE_ERR_ARG;
+    if (!h) return fail(c, GE_ERR_ARG, "state arrays are NULL");
+    const bool d3 = c->p.dims == 3;
+    const bool comp = h->kx || h->ky || h->kvx || h->kvy || (d3 && (h->kz || h->kvz));
+    if (comp && c->p.precision != GE_PREC_MIXED)
+        return fail(c, GE_ERR_STATE, "compensation terms exist in GE_PREC_MIXED only");
+    int rc = ge_upload(c, n, h->x, h->y, h->z, h->vx, h->vy, h->vz, h->m, h->id, h->ax, h->ay,
+                       h->az);
+    if (rc) return rc;
+    if ((rc = require_state(c))) return rc;   // the mixed mode's arrays
+    const State &s = c->b.st[c->cur];
+    const size_t B = sizeof(float) * (size_t)n;
+    struct { const float *h; float *d; } cp[] = {
+        {h->kx, s.kx}, {h->ky, s.ky}, {d3 ? h->kz : nullptr, s.kz},
+        {h->kvx, s.kvx}, {h->kvy, s.kvy}, {d3 ? h->kvz : nullptr, s.kvz},
+        {h->pvx, c->b.prev ? s.pvx : nullptr}, {h->pvy, c->b.prev ? s.pvy : nullptr},
+        {d3 ? h->pvz : nullptr, c->b.prev ? s.pvz : nullptr}};
+    for (auto &q : cp)
+        if (q.h && q.d) GE_CHECK(c, cudaMemcpyAsync(q.d, q.h, B, cudaMemcpyHostToDevice, c->stream));
+    GE_CHECK(c, cudaStreamSynchronize(c->stream));
+    if (h->pinned && (rc = ge_upload_pinned(c, h->pinned))) return rc;
+    if (h->temp && (rc = ge_upload_temp(c, h->temp))) return rc;
+    return GE_OK;
 }
 
 int ge_download_prev_vel(ge_ctx *c, float *pvx, float *pvy, float *pvz) {

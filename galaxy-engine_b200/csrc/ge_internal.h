@@ -230,6 +230,15 @@ constexpr int kSortDigitWords = 7 * 512;   // hist / status words per segment / 
 constexpr int kTimeline = 256;    // build timeline entries
 constexpr int kDirectTile = 128;  // particles per block of the direct sum
 
+// the reference's particle records (ge_aos.cu): members of n records into
+// the state (k_aos_in), and the updated members back into each particle's
+// record before the frame's sort (k_aos_out, after sort and permute)
+using AosLayout = ge_aos_layout;
+cudaError_t launch_aos_in(int dims, const unsigned char *phys, const unsigned char *rend,
+                          const AosLayout &L, int n, const State &s, cudaStream_t st);
+cudaError_t launch_aos_out(int dims, unsigned char *phys, const AosLayout &L, int n,
+                           const State &s, const SortScratch &ss, cudaStream_t st);
+
 // --- launchers (each runs on `st`) ----------------------------------------
 // integrateStart (kick + drift) fused with the per-segment bounding-box
 // reduction; a second small kernel applies the reference's box formula per

@@ -153,6 +153,69 @@ int ge_download_prev_vel(ge_ctx *ctx, float *pvx, float *pvy, float *pvz);
 int ge_upload_temp(ge_ctx *ctx, const float *temp);
 int ge_download_temp(ge_ctx *ctx, float *temp);
 
+/* --- the reference's particle records (array of structures) --------------
+ * The reference keeps its particles as two record arrays,
+ * std::vector<ParticlePhysics> and std::vector<ParticleRendering>
+ * (include/Particles/particle.h:5-140; ParticlePhysics3D /
+ * ParticleRendering3D :142-277), copies the gravity members into SoA
+ * vectors before the walk (Physics::flattenParticles, src/Physics/
+ * physics.cpp:354-390) and back after it (readFlattenBack, :542-565), and
+ * reorders both arrays by Morton key every frame (morton.cpp:40-63).
+ * ge_frame_aos is one frame (as ge_frame_host) on those records as they
+ * are: the n physics records (and, for the pin flags, the rendering
+ * records; rend may be NULL) go to the device in one copy each; after the
+ * frame the updated members -- pos, vel, acc, and prevVel with
+ * track_prev_vel, temp with temp_enabled -- are written back into each
+ * particle's own record, so the caller's arrays keep their order and their
+ * other members.  order (optional, n entries) receives the Morton order the
+ * reference would have moved its arrays to: order[k] = the record in slot k.
+ * The layout gives the byte offsets of the members read and written (-1:
+ * not present); ge_aos_layout_default fills the reference's (the offsets of
+ * the structs in particle.h, pinned by a test that compiles that header).
+ * Positions, velocities and accelerations are float vectors of dims
+ * components; mass and temp floats; id uint32; isPinned one byte. */
+typedef struct {
+    int32_t stride;        /* bytes per physics record (sizeof ParticlePhysics[3D]) */
+    int32_t off_pos, off_vel, off_acc;
+    int32_t off_prev_vel;  /* written back with track_prev_vel; -1: none */
+    int32_t off_mass, off_id;
+    int32_t off_temp;      /* read and written back with temp_enabled; -1: none */
+    int32_t r_stride;      /* bytes per rendering record (sizeof ParticleRendering[3D]) */
+    int32_t r_off_pinned;  /* isPinned; -1: no pin flags */
+} ge_aos_layout;
+void ge_aos_layout_default(ge_aos_layout *layout, int dims);
+int ge_frame_aos(ge_ctx *ctx, int64_t n, void *phys, const void *rend,
+                 const ge_aos_layout *layout, uint32_t *order);
+
+/* --- checkpoint / resume --------------------------------------------------
+ * No counterpart in the reference, whose scene files (SaveSystem,
+ * src/UX/saveSystem.cpp:285-410) keep no compensation terms.  The particle
+ * state with every term the next step reads, as caller-owned host arrays in
+ * the current particle order (all simulations, slot order); any pointer may
+ * be NULL (z members ignored in 2D):
+ *   x y z vx vy vz ax ay az m id   as ge_download / ge_upload
+ *   kx ky kz kvx kvy kvz           GE_PREC_MIXED: the Kahan compensation terms
+ *                                  of positions and velocities
+ *   pvx pvy pvz                    prevVel (track_prev_vel)
+ *   temp, pinned                   temperatures and pin flags
+ * ge_download_state fills zeros for what the context does not hold (the
+ * compensation terms outside GE_PREC_MIXED, prevVel without track_prev_vel,
+ * temperatures or pin flags never uploaded).  ge_upload_state replaces the
+ * context's particles by one simulation of n particles, as ge_upload does,
+ * then sets every array given (compensation terms: GE_PREC_MIXED only, else
+ * GE_ERR_STATE).  A context restored from a snapshot, with the same
+ * parameters, steps on bit for bit as the context that wrote it. */
+typedef struct {
+    float *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az, *m;
+    uint32_t *id;
+    float *kx, *ky, *kz, *kvx, *kvy, *kvz;
+    float *pvx, *pvy, *pvz;
+    float *temp;
+    uint8_t *pinned;
+} ge_state_arrays;
+int ge_download_state(ge_ctx *ctx, const ge_state_arrays *s);
+int ge_upload_state(ge_ctx *ctx, int64_t n, const ge_state_arrays *s);
+
 /* --- the fused step ---------------------------------------------------- */
 /* nsteps full frames on the resident state (globalLogic.cpp:1155-1370 /
    :1584-1719 with dt != 0), all on the device. */

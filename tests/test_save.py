@@ -136,3 +136,61 @@ def test_loaded_scene_steps_like_the_oracle(ge, ics, O, tmp_path):
     assert np.any(sc["pinned"])
     for k in ("x", "y", "vx", "vy", "ax", "ay", "id", "temp"):
         assert np.array_equal(out[k], fr[k]), k
+
+
+# --- fixtures written through the reference's own particle types ----------
+# tests/golden/save{2d,3d}_ref.bin come from oracle/ref_save_fixture.cpp,
+# compiled against the reference's include/Particles/particle.h (make -C
+# oracle save-fixture REF=<checkout>/GalaxyEngine), 300 particles each, with
+# the member values below.
+
+def _ref_fixture_values(dims, n=300):
+    i = np.arange(n)
+    f = np.float32
+    pos = [(i % 37) * f(0.25) - f(4), (i // 37) * f(0.5) - f(2), (i % 11) * f(0.125) - f(0.5)]
+    vel = [(i % 5) * f(0.125) - f(0.25), (i % 7) * f(0.0625) - f(0.1875), (i % 3) * f(0.25) - f(0.25)]
+    acc = [((i % 3) - f(1)) * f(0.5), ((i % 4) - f(2)) * f(0.5), ((i % 5) - f(2)) * f(0.5)]
+    out = {}
+    for a, c in enumerate("xyz"[:dims]):
+        out[c] = pos[a].astype(np.float32)
+        out["v" + c] = vel[a].astype(np.float32)
+        out["a" + c] = acc[a].astype(np.float32)
+    out["m"] = (1 + i % 9).astype(np.float32)
+    out["temp"] = (100 + i).astype(np.float32)
+    out["id"] = (1000 + i).astype(np.uint32)
+    out["pinned"] = (i % 13 == 0).astype(np.uint8)
+    return out
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_reader_on_files_written_with_the_reference_types(ge, dims):
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, f"save{dims}d_ref.bin")
+    got = ge.load_save(path)
+    assert got["dims"] == dims
+    want = _ref_fixture_values(dims)
+    for k, v in want.items():
+        assert np.array_equal(got[k], v), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [2, 3])
+def test_reference_typed_scene_steps_like_the_oracle(ge, O, dims):
+    """The reference-typed fixture, loaded and stepped three frames in
+    GE_PREC_EXACT, equals the oracle frame loop on the same arrays."""
+    from conftest import GOLDEN
+    sc = ge.load_save(os.path.join(GOLDEN, f"save{dims}d_ref.bin"))
+    keys = ["x", "y", "vx", "vy", "ax", "ay", "m", "id"] + (["z", "vz", "az"] if dims == 3 else [])
+    eps2 = 0.01
+    p = ge.default_params(dims, G=1e-3, theta=0.7, eps2=eps2, dt=1e-2, precision=ge.PREC_EXACT)
+    with ge.Simulation(p) as s:
+        s.upload({k: sc[k] for k in keys})
+        s.upload_pinned(sc["pinned"])
+        s.step(3)
+        out = s.download()
+    fr = {k: np.array(sc[k], copy=True) for k in keys + ["pinned"]}
+    op = O.make_params(dims, G=1e-3, theta=0.7, eps2=eps2, dt=1e-2, leaf_cap=4)
+    for _ in range(3):
+        O.frame(op, fr, walk_kind=0)
+    for k in keys:
+        assert np.array_equal(out[k], fr[k]), k
