@@ -101,6 +101,9 @@ class ServerStats(C.Structure):
         ("latency_s_p99", C.c_double), ("pool_bytes", C.c_int64 * 2),
         ("pool_capacity", C.c_int64 * 2), ("pool_iterations", C.c_int64 * 2),
         ("pool_step_ms_p50", C.c_double * 2), ("pool_step_ms_p99", C.c_double * 2),
+        ("pool_busy_s", C.c_double * 2), ("pool_admit_s", C.c_double * 2),
+        ("pool_retire_s", C.c_double * 2), ("pool_particle_steps", C.c_int64 * 2),
+        ("queue_wait_s_p50", C.c_double), ("queue_wait_s_p99", C.c_double),
     ]
 
 

@@ -72,7 +72,8 @@ struct Pool {
     bool stepping = false;
     Clock::time_point t_step;
     int64_t iterations = 0;
-    double busy_s = 0.0;
+    double busy_s = 0.0, admit_s = 0.0, retire_s = 0.0;
+    int64_t particle_steps = 0;
     std::vector<double> step_ms;
 };
 
@@ -101,6 +102,7 @@ struct ge_server {
     // statistics
     int64_t submitted = 0, completed = 0, failed = 0, particle_steps = 0;
     std::vector<double> latency_s;
+    std::vector<double> queue_wait_s;
     std::string err;
     int loop_error = GE_OK;
 };
@@ -138,6 +140,16 @@ int size_pool(const ge_params *p, int64_t share, int32_t max_sims, int64_t *cap)
 int admit(ge_server *s, int k) {
     Pool &P = s->pool[k];
     if (!P.ctx) return GE_OK;
+    const Clock::time_point ta = Clock::now();
+    struct AddTime {   // time spent adding simulations, on every way out
+        ge_server *s;
+        Pool &P;
+        Clock::time_point t;
+        ~AddTime() {
+            std::lock_guard<std::mutex> lk(s->mu);
+            P.admit_s += seconds_since(t);
+        }
+    } add_time{s, P, ta};
     while (true) {
         Request *r = nullptr;
         {
@@ -167,6 +179,7 @@ int admit(ge_server *s, int k) {
         r->sim = h;
         r->state = GE_REQ_RUNNING;
         r->t_admit = seconds_since(s->t0);
+        s->queue_wait_s.push_back(r->t_admit - r->t_submit);
         r->in.clear();
         r->in.shrink_to_fit();
         P.used_n += n;
@@ -199,6 +212,7 @@ int finish_step(ge_server *s, int k, int32_t *stepped) {
     if (rc) return sfail(s, rc, ge_last_error(P.ctx));
     const double dt = seconds_since(P.t_step);
     const int64_t ps = P.used_n;
+    const Clock::time_point tr = Clock::now();
     *stepped = 1;
     std::vector<int32_t> gone;
     std::vector<int64_t> keep, done;
@@ -243,7 +257,9 @@ int finish_step(ge_server *s, int k, int32_t *stepped) {
     P.running.swap(keep);
     P.iterations++;
     s->particle_steps += ps;
+    P.particle_steps += ps;
     P.busy_s += dt;
+    P.retire_s += seconds_since(tr);
     if (P.step_ms.size() < (1u << 22)) P.step_ms.push_back(dt * 1e3);
     s->cv.notify_all();
     return GE_OK;
@@ -487,8 +503,14 @@ int ge_server_get_stats(ge_server *s, ge_server_stats *out) {
         out->pool_iterations[k] = P.iterations;
         out->pool_step_ms_p50[k] = percentile(P.step_ms, 0.50);
         out->pool_step_ms_p99[k] = percentile(P.step_ms, 0.99);
+        out->pool_busy_s[k] = P.busy_s;
+        out->pool_admit_s[k] = P.admit_s;
+        out->pool_retire_s[k] = P.retire_s;
+        out->pool_particle_steps[k] = P.particle_steps;
         all.insert(all.end(), P.step_ms.begin(), P.step_ms.end());
     }
+    out->queue_wait_s_p50 = percentile(s->queue_wait_s, 0.50);
+    out->queue_wait_s_p99 = percentile(s->queue_wait_s, 0.99);
     out->step_ms_p50 = percentile(all, 0.50);
     out->step_ms_p99 = percentile(all, 0.99);
     out->latency_s_p50 = percentile(s->latency_s, 0.50);

@@ -509,6 +509,11 @@ typedef struct {
     int64_t pool_capacity[2];    /* particles each pool runs at once */
     int64_t pool_iterations[2];
     double pool_step_ms_p50[2], pool_step_ms_p99[2];
+    double pool_busy_s[2];       /* wall time of each pool's batched steps */
+    double pool_admit_s[2];      /* ... adding admitted simulations to the pool */
+    double pool_retire_s[2];     /* ... copying finished ones out and compacting */
+    int64_t pool_particle_steps[2];
+    double queue_wait_s_p50, queue_wait_s_p99;   /* submit -> admit, admitted requests */
 } ge_server_stats;
 
 int ge_server_create(const ge_server_config *cfg, ge_server **out);
