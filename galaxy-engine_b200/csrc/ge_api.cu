@@ -1269,10 +1269,17 @@ int ge_frame_aos(ge_ctx *c, int64_t n, void *phys, const void *rend, const ge_ao
         return fail(c, GE_ERR_ARG, "record layout: isPinned outside the rendering record");
     const bool temps = c->p.temp_enabled && L->off_temp >= 0;
     const bool prevs = c->p.track_prev_vel && L->off_prev_vel >= 0;
+    // (the members could also be read and written in place when the records
+    // are page-locked, over PCIe from the kernels: measured 2.5x slower than
+    // these copies at 1M particles -- scattered 32-byte reads of 128-byte
+    // records -- so every record array goes through one device copy)
+    unsigned char *phys_map = nullptr, *rend_map = nullptr;
     int rc;
     if ((rc = ensure_capacity(c, n, 1, false))) return rc;
-    if ((rc = ensure_bytes(c, &c->d_aos, &c->aos_bytes, (size_t)n * L->stride))) return rc;
-    if (pins && (rc = ensure_bytes(c, &c->d_aos_r, &c->aos_r_bytes, (size_t)n * L->r_stride)))
+    if (!phys_map && (rc = ensure_bytes(c, &c->d_aos, &c->aos_bytes, (size_t)n * L->stride)))
+        return rc;
+    if (pins && !rend_map &&
+        (rc = ensure_bytes(c, &c->d_aos_r, &c->aos_r_bytes, (size_t)n * L->r_stride)))
         return rc;
     if (order && c->order_cap < n) {
         GE_CHECK(c, cudaStreamSynchronize(c->stream));
@@ -1294,15 +1301,19 @@ int ge_frame_aos(ge_ctx *c, int64_t n, void *phys, const void *rend, const ge_ao
     c->keys_valid = false;
     if ((rc = sync_segments(c))) return rc;
     cudaStream_t st = c->stream;
-    GE_CHECK(c, cudaMemcpyAsync(c->d_aos, phys, (size_t)n * L->stride, cudaMemcpyHostToDevice, st));
-    if (pins)
+    unsigned char *dphys = phys_map ? phys_map : c->d_aos;
+    const unsigned char *drend = pins ? (rend_map ? rend_map : c->d_aos_r) : nullptr;
+    if (!phys_map)
+        GE_CHECK(c, cudaMemcpyAsync(c->d_aos, phys, (size_t)n * L->stride, cudaMemcpyHostToDevice,
+                                    st));
+    if (pins && !rend_map)
         GE_CHECK(c, cudaMemcpyAsync(c->d_aos_r, rend, (size_t)n * L->r_stride,
                                     cudaMemcpyHostToDevice, st));
     State s = c->b.st[c->cur];
     if (!pins) s.pinned = nullptr;
     if (!temps) s.temp = nullptr;
     if (!c->b.prev) s.pvx = s.pvy = s.pvz = nullptr;
-    GE_CHECK(c, launch_aos_in(D, c->d_aos, pins ? c->d_aos_r : nullptr, *L, (int)n, s, st));
+    GE_CHECK(c, launch_aos_in(D, dphys, drend, *L, (int)n, s, st));
     {   // the mixed mode's compensation terms start at zero, as after ge_upload
         const State &sb = c->b.st[c->cur];
         float *kp[6] = {sb.kx, sb.ky, sb.kz, sb.kvx, sb.kvy, sb.kvz};
@@ -1315,15 +1326,17 @@ int ge_frame_aos(ge_ctx *c, int64_t n, void *phys, const void *rend, const ge_ao
     State o = c->b.st[c->cur];
     if (!temps) o.temp = nullptr;
     if (!prevs) o.pvx = o.pvy = o.pvz = nullptr;
-    GE_CHECK(c, launch_aos_out(D, c->d_aos, *L, (int)n, o, c->b.ss, st));
-    // the byte span of each record that the frame changed, one pitched copy
-    int32_t lo = std::min(L->off_pos, std::min(L->off_vel, L->off_acc));
-    int32_t hi = std::max(L->off_pos, std::max(L->off_vel, L->off_acc)) + vec;
-    if (prevs) { lo = std::min(lo, L->off_prev_vel); hi = std::max(hi, L->off_prev_vel + vec); }
-    if (temps) { lo = std::min(lo, L->off_temp); hi = std::max(hi, L->off_temp + 4); }
-    GE_CHECK(c, cudaMemcpy2DAsync((unsigned char *)phys + lo, (size_t)L->stride, c->d_aos + lo,
-                                  (size_t)L->stride, (size_t)(hi - lo), (size_t)n,
-                                  cudaMemcpyDeviceToHost, st));
+    GE_CHECK(c, launch_aos_out(D, dphys, *L, (int)n, o, c->b.ss, st));
+    if (!phys_map) {
+        // the byte span of each record that the frame changed, one pitched copy
+        int32_t lo = std::min(L->off_pos, std::min(L->off_vel, L->off_acc));
+        int32_t hi = std::max(L->off_pos, std::max(L->off_vel, L->off_acc)) + vec;
+        if (prevs) { lo = std::min(lo, L->off_prev_vel); hi = std::max(hi, L->off_prev_vel + vec); }
+        if (temps) { lo = std::min(lo, L->off_temp); hi = std::max(hi, L->off_temp + 4); }
+        GE_CHECK(c, cudaMemcpy2DAsync((unsigned char *)phys + lo, (size_t)L->stride, c->d_aos + lo,
+                                      (size_t)L->stride, (size_t)(hi - lo), (size_t)n,
+                                      cudaMemcpyDeviceToHost, st));
+    }
     if (order) {
         GE_CHECK(c, launch_perm_out(D, (int)n, c->b.ss, c->d_order, st));
         GE_CHECK(c, cudaMemcpyAsync(order, c->d_order, sizeof(uint32_t) * (size_t)n,

@@ -162,12 +162,14 @@ int ge_download_temp(ge_ctx *ctx, float *temp);
  * physics.cpp:354-390) and back after it (readFlattenBack, :542-565), and
  * reorders both arrays by Morton key every frame (morton.cpp:40-63).
  * ge_frame_aos is one frame (as ge_frame_host) on those records as they
- * are: the n physics records (and, for the pin flags, the rendering
- * records; rend may be NULL) go to the device in one copy each; after the
- * frame the updated members -- pos, vel, acc, and prevVel with
- * track_prev_vel, temp with temp_enabled -- are written back into each
- * particle's own record, so the caller's arrays keep their order and their
- * other members.  order (optional, n entries) receives the Morton order the
+ * are: the members are read from the n physics records (and the pin flags
+ * from the rendering records; rend may be NULL), and after the frame the
+ * updated members -- pos, vel, acc, and prevVel with track_prev_vel, temp
+ * with temp_enabled -- are written back into each particle's own record, so
+ * the caller's arrays keep their order and their other members.  The
+ * records go to the device in one copy per array and the changed bytes of
+ * each record come back in one pitched copy (page-locked arrays copy
+ * fastest).  order (optional, n entries) receives the Morton order the
  * reference would have moved its arrays to: order[k] = the record in slot k.
  * The layout gives the byte offsets of the members read and written (-1:
  * not present); ge_aos_layout_default fills the reference's (the offsets of

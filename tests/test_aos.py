@@ -131,3 +131,27 @@ def test_frame_aos_rejects_bad_layouts(ge, ics):
         with pytest.raises(ge.GeError) as ei:
             s.frame_aos(phys, rend, layout=bad)
         assert ei.value.code == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [2, 3])
+def test_page_locked_records_give_the_same_frames(ge, ics, dims):
+    """Records in page-locked memory (the copies are asynchronous DMA) give
+    the same frames as pageable records, bit for bit."""
+    import torch
+    st = ics.disk2d(5000, seed=11) if dims == 2 else ics.plummer3d(5000, seed=11)
+    p = ge.default_params(dims, G=1.0, theta=0.7, eps2=1e-4 if dims == 2 else 0.01, dt=1e-3,
+                          precision=ge.PREC_EXACT)
+    phys, rend = make_records(ge, st, dims, seed=7)
+    pdt, rdt = phys.dtype, rend.dtype
+    lphys = torch.zeros(phys.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+    lrend = torch.zeros(rend.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+    lphys[:] = phys.view(np.uint8).ravel()
+    lrend[:] = rend.view(np.uint8).ravel()
+    lphys, lrend = lphys.view(pdt), lrend.view(rdt)
+    with ge.Simulation(p) as a, ge.Simulation(p) as b:
+        for _ in range(2):
+            oa = a.frame_aos(phys, rend)
+            ob = b.frame_aos(lphys, lrend)
+            assert np.array_equal(oa, ob)
+            assert np.array_equal(phys.view(np.uint8), lphys.view(np.uint8))
