@@ -207,8 +207,8 @@ struct StepParams {
 // halved L times (exact), so the plain layout's size^2 = fl(size_L^2) =
 // fl(rs^2) * 4^-L: fl(rs^2) with 2L taken off its exponent, exact while both
 // are normal floats (every rs below 1e19 and min_size >= 1e-18, checked by
-// the build).  Particles keep w = -1.0f, whose bits no node word reaches
-// (L <= 46).
+// the build).  Massless nodes and particles carry the marker levels below
+// (L <= 46 for real levels); link[] holds every successor in both layouts.
 constexpr int kMetaWalkPacked = 13;
 constexpr int kMetaBigRoot = 14;   // tree meta word: some simulation's root size >= 1e19
 constexpr int kMetaWords = 32;     // tree meta words allocated
@@ -221,6 +221,17 @@ __device__ __forceinline__ float packed_size2(uint32_t w_bits, uint32_t rs2_bits
 constexpr uint32_t kPackSkipBits = 26, kPackMaxLevel = 46;
 __host__ __device__ constexpr uint32_t pack_entry_word(uint32_t level, uint32_t skip) {
     return (level << kPackSkipBits) | skip;
+}
+// Level values above kPackMaxLevel mark the packed entries that every opening
+// test accepts: a massless node (62; its successor follows) and a particle
+// (63; its successor is the next entry).  One unsigned compare of the word
+// tells them from the nodes, and every entry's successor is in its word.
+constexpr uint32_t kPackMassless = 62, kPackParticle = 63;
+__host__ __device__ __forceinline__ bool packed_accepts(uint32_t w_bits) {
+    return w_bits >= (kPackMassless << kPackSkipBits);
+}
+__host__ __device__ __forceinline__ bool packed_particle(uint32_t w_bits) {
+    return w_bits >= (kPackParticle << kPackSkipBits);
 }
 
 constexpr int kBBoxThreads = 256;

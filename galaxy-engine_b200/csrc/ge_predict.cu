@@ -24,9 +24,11 @@ __device__ __forceinline__ float entry_s2(const Tree &t, int D, uint32_t k, bool
                                           uint32_t rs_bits) {
     if (D == 3) return __uint_as_float(__ldg(&((const uint2 *)t.link)[k]).y);
     const float4 A = __ldg(&t.src[k]);
-    if (!packed || A.w == -1.0f) return A.w;
-    if (!(A.z > 0.0f)) return -2.0f;
-    return packed_size2(__float_as_uint(A.w), rs_bits);
+    if (!packed) return A.w;
+    const uint32_t wb = __float_as_uint(A.w);
+    if (packed_particle(wb)) return -1.0f;
+    if (packed_accepts(wb)) return -2.0f;   // a massless node
+    return packed_size2(wb, rs_bits);
 }
 __device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k) {
     return D == 2 ? __ldg(&((const uint32_t *)t.link)[k]) : __ldg(&((const uint2 *)t.link)[k]).x;

@@ -680,7 +680,8 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
         // carries no mass (the walk makes no interaction with a massless
         // node) and leads to its successor.
         t.src[me] = D == 2 ? make_float4(w.x, w.y, 0.0f,
-                                         packed ? __uint_as_float(pack_entry_word(ax.x, skip)) : -2.0f)
+                                         packed ? __uint_as_float(pack_entry_word(kPackMassless, skip))
+                                                : -2.0f)
                            : make_float4(w.x, w.y, w.z, 0.0f);
         if (D == 2) ((uint32_t *)t.link)[me] = skip;
         else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
@@ -711,7 +712,9 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
             t.slot_of[j] = e;
             if (massless) continue;   // never reached by the walk
             if (D == 2) {
-                t.src[e] = make_float4(px[q], py[q], pm[q], -1.0f);
+                t.src[e] = make_float4(px[q], py[q], pm[q],
+                                       packed ? __uint_as_float(pack_entry_word(kPackParticle, e + 1))
+                                              : -1.0f);
                 ((uint32_t *)t.link)[e] = e + 1;
             } else {
                 t.src[e] = make_float4(px[q], py[q], pz[q], pm[q]);

@@ -110,11 +110,13 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
                 float s2;          // a node's size^2 (plain layout: -1 particle, -2 massless)
                 uint32_t nxt_skip;
                 bool part;         // a particle's entry
+                bool always = false;   // packed: a particle or a massless node
                 if constexpr (PK) {
                     const uint32_t wb = __float_as_uint(A.w);
-                    part = A.w == -1.0f;
-                    s2 = packed_size2(wb, rs2_bits);   // not used for particles and massless nodes
-                    nxt_skip = wb & ((1u << kPackSkipBits) - 1u);
+                    always = packed_accepts(wb);
+                    part = packed_particle(wb);
+                    s2 = packed_size2(wb, rs2_bits);   // not used for marked entries
+                    nxt_skip = wb & ((1u << kPackSkipBits) - 1u);   // a particle's: k + 1
                 } else {
                     const LT L = __ldg(&link[k]);
                     s2 = link_s2(L, A.w);
@@ -135,7 +137,7 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
                 // MIXED entries hold the squared opening radius, which already
                 // includes 1 / theta
                 bool acc;
-                if constexpr (PK) acc = part || m <= 0.0f || s2 < fmul(th2, r2);   // as -1 / -2 would
+                if constexpr (PK) acc = always || s2 < fmul(th2, r2);   // as -1 / -2 would
                 else acc = MODE == GE_PREC_MIXED ? s2 < r2 : s2 < fmul(th2, r2);
                 if (kSelfTest) {
                     // heat exchange (physics.cpp:145-158, 183-191): an accepted node
@@ -224,8 +226,10 @@ k_walk(State s, StepParams p, Segs g, Tree t, int integrate_end, unsigned long l
                     for (int a = 0; a < D; a++) f[a] = fmaf(d[a], fm, f[a]);
                 }
                 // a valid skip lies past k; max() keeps k increasing whatever the
-                // layout holds, so the walk ends within end - begin entries
-                k = max(k + 1, acc && !part ? nxt_skip : k + 1);
+                // layout holds, so the walk ends within end - begin entries (a
+                // packed particle's own successor is k + 1)
+                if constexpr (PK) k = max(k + 1, acc ? nxt_skip : k + 1);
+                else k = max(k + 1, acc && !part ? nxt_skip : k + 1);
             }
         };
         if (packed) walk_range(std::true_type{});

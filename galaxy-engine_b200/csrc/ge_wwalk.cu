@@ -111,7 +111,7 @@ __device__ __forceinline__ void layout_entry(const Tree &t, uint32_t k, bool pac
     A = __ldg(&t.src[k]);
     if (D == 2 && packed) {
         const uint32_t wb = __float_as_uint(A.w);
-        part = A.w == -1.0f;
+        part = packed_particle(wb);   // (massless nodes: mass 0, accepted below)
         s2 = packed_size2(wb, rs2_bits);
         skip = wb & ((1u << kPackSkipBits) - 1u);
     } else if (D == 2) {
