@@ -46,7 +46,7 @@ constexpr uint32_t kSmallNode = 32;
 // meta[] words used by the build
 constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 3,
               kMetaSmall = 5, kMetaP2Alloc = 6, kMetaTimeline = 7, kMetaReal = 8, kMetaSlots = 9,
-              kMetaP2Task = 12;
+              kMetaP2Task = 12, kMetaDone = 15;
 constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
@@ -750,7 +750,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         t.meta[kMetaNodes] = 0u; t.meta[kMetaLevels] = 0u;
         t.meta[kMetaSmall] = 0u; t.meta[kMetaP2Alloc] = 0u; t.meta[kMetaTimeline] = 0u;
         t.meta[kMetaReal] = 0u; t.meta[kMetaSlots] = 0u; t.meta[kMetaP2Task] = 0u;
-        t.meta[kMetaBigRoot] = 0u;
+        t.meta[kMetaBigRoot] = 0u; t.meta[kMetaDone] = 0u;
         stamp(t);
     }
     for (uint32_t i = gtid; i < (uint32_t)kMaxLevels + 2u; i += nthreads) t.lvl_alloc[i] = 0u;
@@ -1043,6 +1043,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         }
         __syncthreads();
     }
+    if (gtid == 0) stamp(t);
     // scatter nodes and the particles of leaves into the walk layout, in which
     // each leaf's particles follow the leaf: with C(e) the number of nodes
     // whose range ends at or before e,
@@ -1086,6 +1087,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             scatter_entry<D>(s, g, t, kk[u], inf[u], ax[u], wv[u], s2[u], ez[u], ew[u], total, err,
                              packed);
         }
+    }
+    // the last block to finish stamps the end of the build
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&t.meta[kMetaDone], 1u) == gridDim.x - 1u) stamp(t);
     }
 }
 
