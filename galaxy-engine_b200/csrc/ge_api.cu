@@ -324,6 +324,8 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     t.ksus_cap = (uint32_t)key_suspect_cap((int64_t)N);
     GE_CHECK(c, dalloc(L, &t.ksus, (size_t)t.ksus_cap));
     GE_CHECK(c, dalloc(L, &t.kroots, N + 1));
+    GE_CHECK(c, dalloc(L, &t.kbig, kKeyBigCap));
+    GE_CHECK(c, dalloc(L, &t.kbig_keys, kKeyBigHash));
     t.ktile_cap = (uint32_t)(N / kKeyTile + 1);
     GE_CHECK(c, dalloc(L, &t.ktile, (size_t)t.ktile_cap * 22));
     GE_CHECK(c, dalloc(L, &t.kmeta, kKeyMetaWords));

@@ -131,6 +131,10 @@ struct Tree {
     uint2 *ksus;
     uint32_t ksus_cap;
     uint32_t *kroots;
+    // exact-rebuild roots too large for one warp to mark: {level, start, end}
+    // (kbig, kKeyBigCap entries), each once (kbig_keys: a set of {start, level})
+    uint4 *kbig;
+    unsigned long long *kbig_keys;
     uint32_t *ktile;
     uint32_t ktile_cap;
     uint32_t *kmeta;
@@ -306,6 +310,8 @@ cudaError_t launch_build(int dims, const State &s, const StepParams &p, const Se
 // their sorted keys (2D: key << 28 | index words; 3D: keys)
 constexpr int kKeyMaxCap = 32;   // leaf capacities the key-prefix build handles
 constexpr int kKeyTile = 256;    // particles per tile of its node-count scan (one per thread)
+constexpr int kKeyBigCap = 256;   // large exact-rebuild roots recorded per build
+constexpr int kKeyBigHash = 1024; // slots of their set
 constexpr int kKeyMetaWords = 64;
 int64_t key_suspect_cap(int64_t n);
 cudaError_t launch_key_build(int dims, const State &s, const StepParams &p, const Segs &g,

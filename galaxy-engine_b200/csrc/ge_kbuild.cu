@@ -50,7 +50,14 @@ constexpr int kKT = 256;                   // threads of the key passes
 constexpr int kHalo = kKeyMaxCap;          // window of the leaf-count test
 // kmeta words
 constexpr int kKmSus = 0, kKmRoots = 1, kKmOverflow = 2, kKmTotal = 3, kKmLevels = 4,
-              kKmLevelTot = 8;
+              kKmLevelTot = 8, kKmBig = 32;
+// an exact-rebuild root of more particles than this is recorded in the large
+// list and marked by the node-count pass (one thread per particle) instead of
+// by the warp that found it
+#ifndef GE_MARK_DIRECT
+#define GE_MARK_DIRECT 4096
+#endif
+constexpr uint32_t kMarkDirect = GE_MARK_DIRECT;
 
 template <int D> struct KeyBits;
 template <> struct KeyBits<2> { static constexpr int B = 18, W = 36; };
@@ -106,6 +113,8 @@ k_key_levels(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, T
             p4[k] = make_uint4(0u, 0u, 0u, 0u);
         if (blockIdx.x == 0 && threadIdx.x < (unsigned)(t.cap - n4 * 4))
             t.pend[n4 * 4 + threadIdx.x] = 0u;
+        if (blockIdx.x == 0)
+            for (int q = threadIdx.x; q < kKeyBigHash; q += kKT) t.kbig_keys[q] = 0ull;
     }
     // first levels whose cells are no larger than the size gate / min size
     // (the sizes are exact halvings of the root's: w * 2^-L)
@@ -267,8 +276,28 @@ k_key_check(State s, StepParams p, Segs g, const uint64_t *__restrict__ keys, Tr
             if (j < e && digit<D>(key_at<D>(keys, j), L) < lane) bad = true;
         }
         const bool differ = __any_sync(0xffffffffu, bad);
-        if (differ)
-            for (uint32_t j = a + lane; j < e; j += 32) atomicMin(&t.kxr[j], (uint32_t)L);
+        if (!differ) continue;
+        // a large root goes to the large list once (several suspects may find
+        // it), unless the set or the list is full
+        bool listed = false;
+        if (e - a > kMarkDirect && lane == 0) {
+            const unsigned long long key = (((unsigned long long)a << 8) | (unsigned)L) + 1ull;
+            uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 40) & (kKeyBigHash - 1u);
+            for (int probe = 0; probe < 32; probe++, h = (h + 1u) & (kKeyBigHash - 1u)) {
+                const unsigned long long old = atomicCAS(&t.kbig_keys[h], 0ull, key);
+                if (old == key) { listed = true; break; }   // recorded by another warp
+                if (old == 0ull) {
+                    const uint32_t k = atomicAdd(&t.kmeta[kKmBig], 1u);
+                    if (k < (uint32_t)kKeyBigCap) {
+                        t.kbig[k] = make_uint4((uint32_t)L, a, e, 0u);
+                        listed = true;
+                    }
+                    break;
+                }
+            }
+        }
+        if (__shfl_sync(0xffffffffu, listed, 0)) continue;
+        for (uint32_t j = a + lane; j < e; j += 32) atomicMin(&t.kxr[j], (uint32_t)L);
     }
 }
 
@@ -278,11 +307,39 @@ __global__ void __launch_bounds__(kKT)
 k_key_count(StepParams p, Tree t, int tiles) {
     dep_wait();
     constexpr int NL = KeyBits<D>::B + 1;
+    constexpr uint32_t kTileBig = 32;
     __shared__ uint32_t sc[NL];
+    __shared__ uint4 s_big[kTileBig];
+    __shared__ uint32_t s_nb;
     if (threadIdx.x < NL) sc[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) s_nb = 0u;
     __syncthreads();
     const uint32_t a = blockIdx.x * kKeyTile + threadIdx.x;
     const bool valid = a < (uint32_t)p.n;
+    // the large exact-rebuild roots that k_key_check listed instead of
+    // marking: the ones over this tile are applied to kxr here
+    const uint32_t nbig = min(t.kmeta[kKmBig], (uint32_t)kKeyBigCap);
+    if (nbig) {   // block-uniform
+        const uint32_t t0 = blockIdx.x * kKeyTile, t1 = t0 + kKeyTile;
+        for (uint32_t q = threadIdx.x; q < nbig; q += kKT) {
+            const uint4 b = t.kbig[q];
+            if (b.y < t1 && b.z > t0) {
+                const uint32_t k = atomicAdd(&s_nb, 1u);
+                if (k < kTileBig) s_big[k] = b;
+            }
+        }
+        __syncthreads();
+        const uint32_t nb = s_nb;
+        if (valid && nb) {
+            uint32_t x = t.kxr[a];
+            const uint32_t x0 = x;
+            for (uint32_t q = 0; q < (nb <= kTileBig ? nb : nbig); q++) {
+                const uint4 b = nb <= kTileBig ? s_big[q] : t.kbig[q];
+                if (b.y <= a && a < b.z) x = min(x, b.x);
+            }
+            if (x != x0) t.kxr[a] = x;
+        }
+    }
     const uint32_t dl = valid ? t.kdl[a] : 1u, T = valid ? key_depth(t, a) : 0u;
 #pragma unroll
     for (int L = 0; L < NL; L++) {

@@ -48,6 +48,14 @@ constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 
               kMetaSmall = 5, kMetaP2Alloc = 6, kMetaTimeline = 7, kMetaReal = 8, kMetaSlots = 9,
               kMetaP2Task = 12, kMetaDone = 15;
 constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
+// keyed builds: exact-rebuild roots and phase-1 nodes of at most kBlockRootMax
+// particles are rebuilt by one block each
+#ifndef GE_BLOCK_ROOT_MAX
+#define GE_BLOCK_ROOT_MAX 2048
+#endif
+constexpr uint32_t kBlockRootMax = GE_BLOCK_ROOT_MAX;
+constexpr int kBlkList = (int)(kBlockRootMax / kSmallNode);
+constexpr int kKmBlockQ = 33;   // key meta word: phase-1 nodes handed to the blocks
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
 __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_gen,
@@ -171,12 +179,113 @@ __device__ __forceinline__ void emit_children(Tree &t, uint32_t k, uint32_t firs
     __threadfence();
 }
 
+// Chains.  A node whose particles all lie in one quadrant of its cell has one
+// child with the same range; nearly coincident particles make long chains of
+// such nodes (one per halving of the cell) before the range splits.  The
+// quadrant of every particle at a level follows from the range's bounding
+// box: the compares p < mid are monotone in p, so all particles agree when the
+// box's two corners do (partition_point then returns the range's start or
+// end, whatever the order inside).  A chain is therefore written in one go,
+// level by level in the reference's float arithmetic, and only its last node
+// (a leaf, or a node that splits) is left to the level loops.
+
+// Bounding box of particles [st, en) (coordinates px/py/pz, element j at
+// index j - off) by the G lanes of a group; every lane of the group gets it.
+// `nan` is set when some coordinate is NaN (no chain is taken then).  All 32
+// lanes call this; lanes with act false contribute nothing.
+template <int D, int G>
+__device__ __forceinline__ void group_bbox(const float *px, const float *py, const float *pz,
+                                           uint32_t off, uint32_t st, uint32_t en, bool act,
+                                           float *mn, float *mx, bool &nan) {
+    const unsigned gl = threadIdx.x & (G - 1u);
+    const float *pc[3] = {px, py, pz};
+    bool bad = false;
+#pragma unroll
+    for (int a = 0; a < D; a++) { mn[a] = FLT_MAX; mx[a] = -FLT_MAX; }
+    if (act)
+        for (uint32_t j = st + gl; j < en; j += G)
+#pragma unroll
+            for (int a = 0; a < D; a++) {
+                const float v = pc[a][j - off];
+                bad |= v != v;
+                mn[a] = fminf(mn[a], v);
+                mx[a] = fmaxf(mx[a], v);
+            }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+        bad |= __shfl_xor_sync(0xffffffffu, (int)bad, o) != 0;
+    }
+    nan = bad;
+}
+
+// The quadrant of the cell (corner + half) that holds every particle of a
+// box, or -1 when the box straddles a midpoint.
+template <int D>
+__device__ __forceinline__ int box_quadrant(float4 cell, float half, const float *mn,
+                                            const float *mx) {
+    const float c[3] = {cell.x, cell.y, cell.z};
+    int q = 0;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        const float mid = fadd(c[a], half);
+        const bool lo = mn[a] < mid, hi = mx[a] < mid;
+        if (lo != hi) return -1;
+        q |= (lo ? 0 : 1) << a;
+    }
+    return q;
+}
+
+// Chain below a node's single child c (cell `cell`, depth `depth`): how many
+// more single-child levels follow before a node that is a leaf or splits;
+// `cell` becomes that last node's cell.
+template <int D>
+__device__ __forceinline__ uint32_t chain_length(const StepParams &p, uint32_t cnt, float4 &cell,
+                                                 uint32_t depth, const float *mn,
+                                                 const float *mx) {
+    uint32_t j = 0;
+    while (depth + j + 2u < (uint32_t)kMaxLevels && !is_leaf<D>(p, cnt, cell.w)) {
+        const float half = fmul(cell.w, 0.5f);
+        const int q = box_quadrant<D>(cell, half, mn, mx);
+        if (q < 0) break;
+        cell = child_cell<D>(cell, half, (unsigned)q);
+        j++;
+    }
+    return j;
+}
+
+// Write the chain: c (slot `first`, already written as a fresh child) and the
+// j nodes below it in slots first + 1 .. first + j, each the single child of
+// the one before; the last is left fresh (info.y = 0) for the level loops.
+// Returns the last node's cell.
+template <int D>
+__device__ __forceinline__ float4 write_chain(Tree &t, uint32_t first, uint32_t j, uint32_t st,
+                                              uint32_t en, float4 cell, uint4 cax,
+                                              const float *mn, const float *mx) {
+    for (uint32_t i = 0; i < j; i++) {
+        const uint32_t k = first + i;
+        const float half = fmul(cell.w, 0.5f);
+        const unsigned q = (unsigned)box_quadrant<D>(cell, half, mn, mx);
+        cell = child_cell<D>(cell, half, q);
+        t.cell[k + 1] = cell;
+        t.info[k + 1] = make_uint4(0u, 0u, st, en);
+        t.aux[k + 1] = make_uint4(cax.x + i + 1u, cax.y + i + 1u, k, 0u);
+        t.info[k] = make_uint4(k + 1, 1u << q, st, en);
+        t.pend[k] = 1u;
+    }
+    return cell;
+}
+
 // Phase 1 work of one node per group of G lanes.
 template <int D, int G>
 __device__ __forceinline__ void split_level_node(const State &s, const StepParams &p, Tree &t,
                                                  uint32_t k, bool valid, uint32_t level_end,
                                                  uint32_t *lvl_alloc, uint32_t *err,
-                                                 bool defer = false) {
+                                                 bool defer = false, uint32_t *handoff = nullptr) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
@@ -187,11 +296,15 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
         inf = __ldcg(&t.info[k]);
         cell = __ldcg(&t.cell[k]);
         ax = __ldcg(&t.aux[k]);
+        valid = inf.y == 0u;   // a chain's inner node is written whole already
     }
     const uint32_t cnt = inf.w - inf.z;
     const bool leaf = valid && is_leaf<D>(p, cnt, cell.w);
     const bool small = valid && !leaf && cnt <= kSmallNode;
-    const bool split = valid && !leaf && !small;
+    // with handoff (keyed), a node that one block can rebuild is listed for
+    // the blocks after the level loop
+    const bool block = handoff && valid && !leaf && !small && cnt <= kBlockRootMax;
+    const bool split = valid && !leaf && !small && !block;
     const float half = fmul(cell.w, 0.5f);
     const float mid[3] = {fadd(cell.x, half), fadd(cell.y, half), fadd(cell.z, half)};
     uint32_t b[Q + 1];
@@ -201,6 +314,18 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
 #pragma unroll
         for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
     }
+    // a single child: the chain below it (every lane of the group computes
+    // it; the box is read for ranges of at most 64 particles per lane)
+    const bool single = split && __popc(mask) == 1 && cnt <= 64u * G;
+    uint32_t j = 0;
+    float mn[3], mx[3];
+    const float4 c1 = child_cell<D>(cell, half, single ? (unsigned)(__ffs(mask) - 1) : 0u);
+    if (__any_sync(0xffffffffu, single)) {
+        bool nan;
+        group_bbox<D, G>(s.x, s.y, s.z, 0u, inf.z, inf.w, single, mn, mx, nan);
+        float4 cend = c1;
+        if (single && !nan) j = chain_length<D>(p, cnt, cend, ax.x + 1u, mn, mx);
+    }
     const bool leader = gl == 0;
     if (leader && leaf) {
         put_walk<D>(t, k, leaf_mass<D>(s, inf.z, inf.w), cell.w);
@@ -208,16 +333,21 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
         else finish_upward<D>(t, k);
         atomicMax(&t.meta[kMetaLevels], ax.x + 1u);
     }
-    // queue the small subtrees (one atomic per warp)
+    // queue the small subtrees and the block roots (one atomic per warp each)
     {
         const unsigned qb = __ballot_sync(0xffffffffu, leader && small);
         uint32_t qbase = 0;
         if (lane == 0 && qb) qbase = atomicAdd(&t.meta[kMetaSmall], (uint32_t)__popc(qb));
         qbase = __shfl_sync(0xffffffffu, qbase, 0);
         if (leader && small) t.small[qbase + __popc(qb & ((1u << lane) - 1u))] = k;
+        const unsigned bb = __ballot_sync(0xffffffffu, leader && block);
+        uint32_t bbase = 0;
+        if (lane == 0 && bb) bbase = atomicAdd(&t.kmeta[kKmBlockQ], (uint32_t)__popc(bb));
+        bbase = __shfl_sync(0xffffffffu, bbase, 0);
+        if (leader && block) handoff[bbase + __popc(bb & ((1u << lane) - 1u))] = k;
     }
     // children of the split nodes (one atomic per warp)
-    const uint32_t nch = (leader && split) ? (uint32_t)__popc(mask) : 0u;
+    const uint32_t nch = (leader && split) ? (uint32_t)__popc(mask) + j : 0u;
     uint32_t incl = nch;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -230,8 +360,16 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
     base = __shfl_sync(0xffffffffu, base, 0);
     if (nch) {
         const uint32_t first = level_end + base + incl - nch;
-        if ((uint64_t)first + nch > (uint64_t)t.cap) set_err(err, kErrNodeCap);
-        else emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+        if ((uint64_t)first + nch > (uint64_t)t.cap) {
+            set_err(err, kErrNodeCap);
+        } else {
+            emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+            if (j) {
+                write_chain<D>(t, first, j, inf.z, inf.w, c1,
+                               make_uint4(ax.x + 1u, ax.y + 1u, k, 0u), mn, mx);
+                __threadfence();
+            }
+        }
     }
 }
 
@@ -240,15 +378,16 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
 // level lists hold only its nodes of more than kSmallNode particles (at most
 // count / (kSmallNode + 1) per level); a child that is a leaf is summed and
 // passed upward at once, a small one goes to the subtree queue (phase 2).
-// Children's slots come from *alloc above `base`.
-constexpr int kBlkList = 64;
-constexpr uint32_t kBlockRootMax = kSmallNode * kBlkList;
+// Children's slots come from *alloc above `base`.  The root's coordinates are
+// staged in shared memory (sx[a][j - off]), so the searches' probes are
+// shared-memory loads.
 
 template <int D, int G>
 __device__ __forceinline__ void rebuild_large_node(const State &s, const StepParams &p, Tree &t,
                                                    uint32_t k, bool valid, uint32_t base,
                                                    uint32_t *alloc, uint32_t *next,
-                                                   uint32_t *next_cnt, uint32_t *err) {
+                                                   uint32_t *next_cnt, uint32_t *err,
+                                                   const float (*sx)[kBlockRootMax], uint32_t off) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
@@ -262,14 +401,26 @@ __device__ __forceinline__ void rebuild_large_node(const State &s, const StepPar
     const float half = fmul(cell.w, 0.5f);
     const float mid[3] = {fadd(cell.x, half), fadd(cell.y, half), fadd(cell.z, half)};
     uint32_t b[Q + 1];
-    cut_group<D, G>(s, valid ? inf.z : 0u, valid ? inf.w : 0u, mid, b);
+    cut_group_v<D, G, true>(sx[0], sx[1], sx[D - 1], off, valid ? inf.z : 0u, valid ? inf.w : 0u,
+                            mid, b);
     uint32_t mask = 0;
     if (valid) {
 #pragma unroll
         for (int q = 0; q < Q; q++) mask |= (b[q + 1] > b[q] ? 1u : 0u) << q;
     }
+    // a single child: the chain below it (every lane of the group computes it)
+    const bool single = valid && __popc(mask) == 1;
+    uint32_t j = 0;
+    float mn[3], mx[3];
+    const float4 c1 = child_cell<D>(cell, half, single ? (unsigned)(__ffs(mask) - 1) : 0u);
+    float4 cend = c1;
+    if (__any_sync(0xffffffffu, single)) {
+        bool nan;
+        group_bbox<D, G>(sx[0], sx[1], sx[D - 1], off, inf.z, inf.w, single, mn, mx, nan);
+        if (single && !nan) j = chain_length<D>(p, inf.w - inf.z, cend, ax.x + 1u, mn, mx);
+    }
     const bool leader = valid && gl == 0;
-    const uint32_t nch = leader ? (uint32_t)__popc(mask) : 0u;
+    const uint32_t nch = leader ? (uint32_t)__popc(mask) + j : 0u;
     uint32_t incl = nch;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -285,18 +436,26 @@ __device__ __forceinline__ void rebuild_large_node(const State &s, const StepPar
     first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1u));
     bool ok = (uint64_t)base + wbase + tot <= (uint64_t)t.cap;
     if (!ok && lane == 0) set_err(err, kErrNodeCap);
-    if (leader && ok) emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+    if (leader && ok) {
+        emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+        if (j) {
+            write_chain<D>(t, first, j, inf.z, inf.w, c1, make_uint4(ax.x + 1u, ax.y + 1u, k, 0u),
+                           mn, mx);
+            __threadfence();
+        }
+    }
     __syncwarp();
-    // the group's lane q takes child q
+    // the group's lane q takes child q (a chain's last node for a single child)
     if (valid && ok && gl < (unsigned)Q && ((mask >> gl) & 1u)) {
-        const uint32_t c = first + __popc(mask & ((1u << gl) - 1u));
+        const uint32_t c = first + __popc(mask & ((1u << gl) - 1u)) + j;
         const uint32_t cnt = b[gl + 1] - b[gl];
-        if (is_leaf<D>(p, cnt, half)) {
+        const float csize = j ? cend.w : half;
+        if (is_leaf<D>(p, cnt, csize)) {
             // its upward pass waits for the end of the rebuilds, so that no
             // level of this loop waits for a chain up the whole tree
-            put_walk<D>(t, c, leaf_mass<D>(s, b[gl], b[gl + 1]), half);
+            put_walk<D>(t, c, leaf_mass<D>(s, b[gl], b[gl + 1]), csize);
             t.kdone[atomicAdd(&t.kmeta[7], 1u)] = c;
-            atomicMax(&t.meta[kMetaLevels], ax.x + 2u);
+            atomicMax(&t.meta[kMetaLevels], ax.x + 2u + j);
         } else if (cnt <= kSmallNode) {
             t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = c;
         } else {
@@ -734,6 +893,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
     const uint32_t n = (uint32_t)p.n;
     uint32_t *bar_count = t.meta + kMetaBarCount, *bar_gen = t.meta + kMetaBarGen;
+    // the block rebuilds' staged coordinates, then phase 2's per-warp subtrees
+    constexpr size_t kSharedBytes = sizeof(SubTreeSmem) * (kBuildThreads / 32) >
+                                            sizeof(float) * D * kBlockRootMax
+                                        ? sizeof(SubTreeSmem) * (kBuildThreads / 32)
+                                        : sizeof(float) * D * kBlockRootMax;
+    __shared__ __align__(16) unsigned char s_shared[kSharedBytes];
 
     // Keyed: the key passes (ge_kbuild.cu) wrote key_nodes nodes in slots
     // [0, key_nodes), the segment roots first; pend holds each node's child
@@ -797,60 +962,16 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             t.aux[r] = make_uint4(0u, 0u, kEmpty, 0u);
     }
 
-    if (keyed) {
-        // exact-rebuild roots of up to kBlockRootMax particles: a block each
-        __shared__ uint32_t s_list[2][kBlkList];
-        __shared__ uint32_t s_cnt[2], s_m;
-        const uint32_t nroots = le;
-        const uint32_t xbase = front;
-        uint32_t *xalloc = &t.kmeta[6];
-        const unsigned w = threadIdx.x >> 5, W = kBuildThreads / 32;
-        for (uint32_t r = blockIdx.x; r < nroots; r += gridDim.x) {
-            const uint32_t root = __ldcg(&t.kroots[r]);
-            const uint4 ri = __ldcg(&t.info[root]);
-            const uint32_t cnt = ri.w - ri.z;
-            if (cnt > kBlockRootMax) continue;   // left to the grid's level loop
-            if (cnt <= kSmallNode) {
-                if (threadIdx.x == 0) t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = root;
-                continue;
-            }
-            if (threadIdx.x == 0) { s_list[0][0] = root; s_cnt[0] = 1u; }
-            int cur = 0;
-            for (int it = 0; it < kMaxLevels; it++) {
-                if (threadIdx.x == 0) {   // one decision for the whole block
-                    s_cnt[cur ^ 1] = 0u;
-                    s_m = ((*(volatile uint32_t *)err) & kErrNodeCap) ? 0u : s_cnt[cur];
-                }
-                __syncthreads();
-                const uint32_t m = s_m;
-                if (m == 0u) break;
-                if (m <= W) {
-                    for (uint32_t j = w; j < m; j += W)
-                        rebuild_large_node<D, 32>(s, p, t, s_list[cur][j], true, xbase, xalloc,
-                                                  s_list[cur ^ 1], &s_cnt[cur ^ 1], err);
-                } else {
-                    for (uint32_t jb = w * 4; jb < m; jb += W * 4) {
-                        const uint32_t j = jb + (lane >> 3);
-                        rebuild_large_node<D, 8>(s, p, t, j < m ? s_list[cur][j] : 0u, j < m,
-                                                 xbase, xalloc, s_list[cur ^ 1], &s_cnt[cur ^ 1],
-                                                 err);
-                    }
-                }
-                __syncthreads();
-                cur ^= 1;
-            }
-            __syncthreads();
-        }
-    }
-
     // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
     // the first level is the segment roots (or, keyed, the exact-rebuild roots
     // too large for one block, by list); children go to slots from `front` on
     int L = 0;
     if (gtid == 0) t.level[0] = lb;
-    grid_barrier(bar_count, bar_gen, err);
-    if (gtid == 0) stamp(t);
-    if (keyed) front += *(volatile uint32_t *)&t.kmeta[6];   // after the blocks' rebuilds
+    if (!keyed) {   // the roots' links above
+        grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
+    }
+    const uint32_t nroots0 = le;   // keyed: the key passes' exact-rebuild roots
     while (true) {
         if (le - lb <= nwarps) {
             for (uint32_t k = lb + gwarp; k < le; k += nwarps) {
@@ -860,7 +981,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                     const uint4 ri = __ldcg(&t.info[node]);
                     valid = ri.w - ri.z > kBlockRootMax;
                 }
-                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed);
+                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed,
+                                        keyed ? t.kroots + nroots0 : nullptr);
             }
         } else {
             for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
@@ -871,7 +993,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                     const uint4 ri = __ldcg(&t.info[node]);
                     valid = ri.w - ri.z > kBlockRootMax;
                 }
-                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed);
+                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed,
+                                       keyed ? t.kroots + nroots0 : nullptr);
             }
         }
         grid_barrier(bar_count, bar_gen, err);
@@ -897,11 +1020,72 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     }
     if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
 
+    if (keyed) {
+        // exact-rebuild roots of up to kBlockRootMax particles: a block each
+        __shared__ uint32_t s_list[2][kBlkList];
+        __shared__ uint32_t s_cnt[2], s_m;
+        // the root's coordinates (shares its memory with phase 2's subtrees)
+        float (*s_xs)[kBlockRootMax] = reinterpret_cast<float (*)[kBlockRootMax]>(s_shared);
+        // the key passes' roots of at most kBlockRootMax particles, then the
+        // nodes of at most kBlockRootMax particles that phase 1 handed over
+        const uint32_t nroots = nroots0 + *(volatile uint32_t *)&t.kmeta[kKmBlockQ];
+        const uint32_t xbase = le;
+        uint32_t *xalloc = &t.kmeta[6];
+        const unsigned w = threadIdx.x >> 5, W = kBuildThreads / 32;
+        for (uint32_t r = blockIdx.x; r < nroots; r += gridDim.x) {
+            const uint32_t root = __ldcg(&t.kroots[r]);
+            const uint4 ri = __ldcg(&t.info[root]);
+            const uint32_t cnt = ri.w - ri.z;
+            if (cnt > kBlockRootMax) continue;   // left to the grid's level loop
+            if (cnt <= kSmallNode) {
+                if (threadIdx.x == 0) t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = root;
+                continue;
+            }
+            if (threadIdx.x == 0) { s_list[0][0] = root; s_cnt[0] = 1u; }
+            for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+                s_xs[0][j] = s.x[ri.z + j];
+                s_xs[1][j] = s.y[ri.z + j];
+                if (D == 3) s_xs[D - 1][j] = s.z[ri.z + j];
+            }
+            int cur = 0;
+            for (int it = 0; it < kMaxLevels; it++) {
+                if (threadIdx.x == 0) {   // one decision for the whole block
+                    s_cnt[cur ^ 1] = 0u;
+                    s_m = ((*(volatile uint32_t *)err) & kErrNodeCap) ? 0u : s_cnt[cur];
+                }
+                __syncthreads();
+                const uint32_t m = s_m;
+                if (m == 0u) break;
+                if (m <= W) {
+                    for (uint32_t j = w; j < m; j += W)
+                        rebuild_large_node<D, 32>(s, p, t, s_list[cur][j], true, xbase, xalloc,
+                                                  s_list[cur ^ 1], &s_cnt[cur ^ 1], err, s_xs,
+                                                  ri.z);
+                } else {
+                    for (uint32_t jb = w * 4; jb < m; jb += W * 4) {
+                        const uint32_t j = jb + (lane >> 3);
+                        rebuild_large_node<D, 8>(s, p, t, j < m ? s_list[cur][j] : 0u, j < m,
+                                                 xbase, xalloc, s_list[cur ^ 1], &s_cnt[cur ^ 1],
+                                                 err, s_xs, ri.z);
+                    }
+                }
+                __syncthreads();
+                cur ^= 1;
+            }
+            __syncthreads();
+        }
+    }
+    if (keyed) {   // the blocks' slots follow phase 1's
+        grid_barrier(bar_count, bar_gen, err);
+        if (gtid == 0) stamp(t);
+        le += *(volatile uint32_t *)&t.kmeta[6];
+        if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
+    }
+
     // ---- phase 2: queued small subtrees, one warp each, no barriers --------
     const uint32_t nsmall = *(volatile uint32_t *)&t.meta[kMetaSmall];
     {
-        __shared__ SubTreeSmem s_sub[kBuildThreads / 32];
-        SubTreeSmem &sm = s_sub[threadIdx.x >> 5];
+        SubTreeSmem &sm = reinterpret_cast<SubTreeSmem *>(s_shared)[threadIdx.x >> 5];
         WarpAlloc wa{0u, 0u, 0u};
         // tasks are taken from a counter (their costs differ); lane j holds the
         // j-th finished subtree root whose upward pass is still to run, and the

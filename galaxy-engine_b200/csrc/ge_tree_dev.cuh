@@ -12,11 +12,12 @@ namespace ge {
 // node j of the search's decision tree (heap order; child 2j when the probe is
 // false, 2j+1 when true); one round evaluates all of them and walks log2(G)
 // steps.  All 32 lanes call this together; groups may differ in their
-// arguments (len 0 for a group with nothing to search).
-template <int G>
+// arguments (len 0 for a group with nothing to search).  With SH the values
+// are a shared-memory copy: element j is v[j - off].
+template <int G, bool SH = false>
 __device__ __forceinline__ uint32_t group_partition_point(const float *__restrict__ v,
                                                           uint32_t first, uint32_t len,
-                                                          float mid) {
+                                                          float mid, uint32_t off = 0u) {
     constexpr int DEPTH = (G == 32) ? 5 : (G == 16) ? 4 : (G == 8) ? 3 : (G == 4) ? 2 : 1;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
@@ -31,7 +32,7 @@ __device__ __forceinline__ uint32_t group_partition_point(const float *__restric
                 if ((gl >> b) & 1u) { f += half + 1; l -= half + 1; }
                 else { l = half; }
             }
-            if (l > 0) pred = __ldg(v + f + (l >> 1)) < mid;
+            if (l > 0) pred = (SH ? v[f + (l >> 1) - off] : __ldg(v + f + (l >> 1))) < mid;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, pred) >> gbase;
         unsigned j = 1;
@@ -50,39 +51,47 @@ __device__ __forceinline__ uint32_t group_partition_point(const float *__restric
 
 // Cut points of one node per group of G lanes: Node::subGridMaker (y, then x
 // in each half) / subGridMaker3D (z, then y in each half, then x in each
-// quarter).  Every lane of the group ends with the group's b[0..Q].
-template <int D, int G>
-__device__ __forceinline__ void cut_group(const State &s, uint32_t st, uint32_t en,
-                                          const float *mid, uint32_t *b) {
+// quarter).  Every lane of the group ends with the group's b[0..Q].  With SH
+// the coordinates are shared-memory copies of particles [off, off + len).
+template <int D, int G, bool SH = false>
+__device__ __forceinline__ void cut_group_v(const float *px, const float *py, const float *pz,
+                                            uint32_t off, uint32_t st, uint32_t en,
+                                            const float *mid, uint32_t *b) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u), gbase = lane & ~(G - 1u);
     b[0] = st; b[Q] = en;
     if (D == 2) {
-        b[2] = group_partition_point<G>(s.y, st, en - st, mid[1]);
+        b[2] = group_partition_point<G, SH>(py, st, en - st, mid[1], off);
         const bool lo = gl < G / 2;
         const uint32_t f = lo ? st : b[2];
         const uint32_t l = lo ? b[2] - st : en - b[2];
-        const uint32_t r = group_partition_point<G / 2>(s.x, f, l, mid[0]);
+        const uint32_t r = group_partition_point<G / 2, SH>(px, f, l, mid[0], off);
         b[1] = __shfl_sync(0xffffffffu, r, gbase);
         b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
     } else {
-        b[4] = group_partition_point<G>(s.z, st, en - st, mid[2]);
+        b[4] = group_partition_point<G, SH>(pz, st, en - st, mid[2], off);
         const bool lo = gl < G / 2;
         uint32_t f = lo ? st : b[4];
         uint32_t l = lo ? b[4] - st : en - b[4];
-        uint32_t r = group_partition_point<G / 2>(s.y, f, l, mid[1]);
+        uint32_t r = group_partition_point<G / 2, SH>(py, f, l, mid[1], off);
         b[2] = __shfl_sync(0xffffffffu, r, gbase);
         b[6] = __shfl_sync(0xffffffffu, r, gbase + G / 2);
         const unsigned g4 = gl / (G / 4);
         const uint32_t a0 = g4 == 0 ? st : (g4 == 1 ? b[2] : (g4 == 2 ? b[4] : b[6]));
         const uint32_t a1 = g4 == 0 ? b[2] : (g4 == 1 ? b[4] : (g4 == 2 ? b[6] : en));
-        r = group_partition_point<G / 4>(s.x, a0, a1 - a0, mid[0]);
+        r = group_partition_point<G / 4, SH>(px, a0, a1 - a0, mid[0], off);
         b[1] = __shfl_sync(0xffffffffu, r, gbase);
         b[3] = __shfl_sync(0xffffffffu, r, gbase + G / 4);
         b[5] = __shfl_sync(0xffffffffu, r, gbase + 2 * (G / 4));
         b[7] = __shfl_sync(0xffffffffu, r, gbase + 3 * (G / 4));
     }
+}
+
+template <int D, int G>
+__device__ __forceinline__ void cut_group(const State &s, uint32_t st, uint32_t en,
+                                          const float *mid, uint32_t *b) {
+    cut_group_v<D, G>(s.x, s.y, s.z, 0u, st, en, mid, b);
 }
 
 // std::partition_point over predicate bits held in a register (bit r is the

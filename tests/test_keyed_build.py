@@ -90,17 +90,38 @@ def test_clumps_of_coincident_particles(ge, O, dims):
 
 
 @pytest.mark.parametrize("dims", [2, 3])
-def test_particles_on_cell_midlines(ge, O, dims):
+def test_chains_that_end_in_splits(ge, O, dims):
+    """Tight clusters (40 to 4000 particles spread over 1e-5 to 1e-3) in a
+    wide box: each sits in one quadrant for many levels (a chain of
+    single-child nodes, written in one go from the cluster's bounding box)
+    and then splits; clusters inside clusters make chains below splits too.
+    Rebuilt by the warp subtrees, a block and the grid's level loop."""
+    rng = np.random.default_rng(70 + dims)
+    parts = [rng.uniform(-50, 50, (3000, dims))]
+    for c, w in [(40, 1e-5), (90, 3e-4), (700, 1e-3), (1500, 2e-5), (2600, 5e-4), (4000, 1e-4)]:
+        ctr = rng.uniform(-40, 40, (1, dims))
+        parts.append(ctr + rng.uniform(0.0, w, (c, dims)))
+        parts.append(ctr + 0.37 * w + rng.uniform(0.0, w * 1e-3, (c // 3, dims)))
+    P = np.concatenate(parts).astype(np.float32)
+    st = _state(P[:, 0], P[:, 1], P[:, 2] if dims == 3 else None)
+    _check(ge, O, st, dims, 4, eps2=1e-2 if dims == 3 else 1e-4)
+
+
+@pytest.mark.parametrize("nbg", [4000, 60000])
+@pytest.mark.parametrize("dims", [2, 3])
+def test_particles_on_cell_midlines(ge, O, dims, nbg):
     """Particles within a few ulps of the midlines of cells of many levels,
     where the Morton digit and the float compare can disagree: every such
     node is checked with the reference's cuts and rebuilt where they differ.
     The root box is offset and not a power of two wide (the two-disk
     workload's), so the keys' grid and the halved cells round differently;
-    with these seeds a pure key-prefix tree differs from the reference's in
-    91 (2D) / 338 (3D) nodes, all of which the exact check must repair."""
+    with these seeds and 4000 background particles a pure key-prefix tree
+    differs from the reference's in 91 (2D) / 338 (3D) nodes, all of which the
+    exact check must repair.  With 60000, the differing nodes of the top
+    levels hold more particles than one warp marks (the large-root list)."""
     rng = np.random.default_rng(17 + dims)
     lo, S = np.float32(-9.981265), np.float32(19.9565)
-    bg = rng.uniform(0.0, 1.0, (4000, dims)) * S + lo
+    bg = rng.uniform(0.0, 1.0, (nbg, dims)) * S + lo
     corners = np.array([[lo] * dims, [lo + S] * dims], np.float32)   # fixes the root box
     pts = []
     for L in range(1, 16):
