@@ -130,6 +130,7 @@ struct ge_ctx {
     uint32_t *h_meta = nullptr;   // pinned copy of the tree meta words
     int64_t slots = 0;            // node slots of the last build (holes included)
     bool count_inter = false;
+    bool tree_ranges = false;   // the last build wrote the layout ranges (warp walk)
     bool tree_valid = false;
     bool keys_valid = false;
     cudaEvent_t ev[8]{};
@@ -690,6 +691,11 @@ int enqueue_permute(ge_ctx *c, bool with_acc) {
 // last moved), so the tree can be built from them (ge_kbuild.cu)
 int enqueue_build(ge_ctx *c, bool fresh_keys = false) {
     StepParams p = step_params(c);
+    // the optional layout arrays this build's readers need
+    const bool temps = c->p.temp_enabled && c->b.temp;
+    p.layout_extras = (c->p.precision == GE_PREC_MIXED || temps ? kLayoutEntry : 0) |
+                      (c->p.walk_kind == 1 ? kLayoutRange : 0);
+    c->tree_ranges = c->p.walk_kind == 1;
     const bool keyed = fresh_keys && c->p.leaf_cap >= 1 && c->p.leaf_cap <= (uint32_t)kKeyMaxCap;
     if (keyed)
         GE_CHECK(c, launch_key_build(c->p.dims, cur_state(c), p, c->g, c->b.ss.keys[0], c->b.tree,
@@ -701,7 +707,7 @@ int enqueue_build(ge_ctx *c, bool fresh_keys = false) {
         GE_CHECK(c, launch_moments(c->p.dims, cur_state(c), p, t, c->d_err, c->num_sms,
                                    c->stream));
     }
-    if (c->p.temp_enabled && c->b.temp)
+    if (temps)
         GE_CHECK(c, launch_node_temps(c->p.dims, cur_state(c), p, c->b.tree, c->num_sms,
                                       c->stream));
     return GE_OK;
@@ -721,6 +727,8 @@ int ensure_mode(ge_ctx *c) {
 
 int enqueue_walk(ge_ctx *c, bool integrate_end) {
     StepParams p = step_params(c);
+    // a tree built without the layout ranges takes the per-particle walk
+    if (!c->tree_ranges) p.walk_kind = 0;
     unsigned long long *cnt = nullptr;
     if (c->count_inter) {
         GE_CHECK(c, cudaMemsetAsync(c->b.d_inter, 0, sizeof(unsigned long long), c->stream));

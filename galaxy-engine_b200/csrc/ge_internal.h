@@ -202,6 +202,7 @@ struct StepParams {
     int i0;              // the per-particle walk: first particle (up to n), 0 by default
     int mixed;           // GE_PREC_MIXED: the moment pass rewrites the node entries
     int walk_kind;       // GE_PREC_FAST: 0 per-particle walk, 1 warp-cooperative walk
+    int layout_extras;   // tree build: kLayoutEntry | kLayoutRange (the optional layout arrays)
 };
 
 // 2D walk entries {x, y, m, w}.  Plain layout: w = size^2 (-1 for a particle,
@@ -214,6 +215,10 @@ struct StepParams {
 // the build).  Massless nodes and particles carry the marker levels below
 // (L <= 46 for real levels); link[] holds every successor in both layouts.
 constexpr int kMetaWalkPacked = 13;
+// optional walk-layout arrays a build writes: each node's entry in aux.w (the
+// moment and node-temperature passes read it) and its entry range in nrange
+// (the warp-cooperative walk reads it)
+constexpr int kLayoutEntry = 1, kLayoutRange = 2;
 constexpr int kMetaBigRoot = 14;   // tree meta word: some simulation's root size >= 1e19
 constexpr int kMetaWords = 32;     // tree meta words allocated
 // warp-cooperative walk counters (Tree::wctr, zeroed before each launch): the

@@ -30,7 +30,11 @@ __device__ __forceinline__ float entry_s2(const Tree &t, int D, uint32_t k, bool
     if (packed_accepts(wb)) return -2.0f;   // a massless node
     return packed_size2(wb, rs_bits);
 }
-__device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k) {
+// successor of entry k (A = its src word): packed 2D entries carry it in
+// their fourth word's low bits (no link array is written then)
+__device__ __forceinline__ uint32_t entry_skip(const Tree &t, int D, uint32_t k, bool packed,
+                                               float4 A) {
+    if (D == 2 && packed) return __float_as_uint(A.w) & ((1u << kPackSkipBits) - 1u);
     return D == 2 ? __ldg(&((const uint32_t *)t.link)[k]) : __ldg(&((const uint2 *)t.link)[k]).x;
 }
 
@@ -42,7 +46,7 @@ __device__ void old_force(const Tree &t, const StepParams &p, uint32_t begin, ui
     uint32_t k = begin;
     while (k < end) {
         const float4 A = __ldg(&t.src[k]);
-        const uint32_t skip = entry_skip(t, D, k);
+        const uint32_t skip = entry_skip(t, D, k, packed, A);
         const uint32_t nxt = max(k + 1, skip);   // always moves forward
         const float gm = D == 2 ? A.z : A.w;
         if (!(gm > 0.0f)) { k = nxt; continue; }   // gridMass <= 0: skip the subtree

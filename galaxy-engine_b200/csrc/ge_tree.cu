@@ -56,6 +56,7 @@ constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase
 constexpr uint32_t kBlockRootMax = GE_BLOCK_ROOT_MAX;
 constexpr int kBlkList = (int)(kBlockRootMax / kSmallNode);
 constexpr int kKmBlockQ = 33;   // key meta word: phase-1 nodes handed to the blocks
+constexpr int kKmBlockTake = 34;   // key meta word: next block root to take
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
 __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_gen,
@@ -382,27 +383,92 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
 // staged in shared memory (sx[a][j - off]), so the searches' probes are
 // shared-memory loads.
 
+// The block's shared state during an exact rebuild: the root's particles
+// (coordinates and masses), the current and next level's nodes (slot, range,
+// cell, level and same-end count), and the root's deferred leaves and small
+// subtrees (bit 31), published with one atomic per kind when the buffer
+// fills or the root is done.
+constexpr int kBlkOut = 512;
+template <int D>
+struct BlockSmem {
+    float x[D][kBlockRootMax];
+    float m[kBlockRootMax];
+    uint32_t node[2][kBlkList];
+    uint4 inf[2][kBlkList];
+    float4 cell[2][kBlkList];
+    uint2 ax[2][kBlkList];
+    uint32_t out[kBlkOut];
+    uint32_t cnt[2], mcur, nout, maxlev, bad;
+    // the block's slots: a chunk [anext, aend) of the phase-2 pool (used up
+    // to aused), `real` slots used in all, a hole range to zero
+    uint32_t anext, aend, aused, real, hole_a, hole_b;
+};
+constexpr uint32_t kBlkChunk = 512;   // slots a block takes at a time (at least)
+
+// computeLeafMass / computeLeafMass3D over staged particles (the same
+// sequential sums as leaf_mass)
+template <int D>
+__device__ __forceinline__ float4 leaf_mass_smem(const BlockSmem<D> &b, uint32_t st, uint32_t en) {
+    float gm = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+    for (uint32_t i = st; i < en; i++) {
+        const float mi = b.m[i];
+        gm = fadd(gm, mi);
+        c[0] = fadd(c[0], fmul(b.x[0][i], mi));
+        c[1] = fadd(c[1], fmul(b.x[1][i], mi));
+        if (D == 3) c[2] = fadd(c[2], fmul(b.x[D - 1][i], mi));
+    }
+    if (gm > 0.0f) {
+        c[0] = fdiv(c[0], gm); c[1] = fdiv(c[1], gm);
+        if (D == 3) c[2] = fdiv(c[2], gm);
+    }
+    return make_float4(c[0], c[1], c[2], gm);
+}
+
+// Publish the block's buffered leaves and small subtrees (one thread).
+template <int D>
+__device__ __forceinline__ void flush_block_out(Tree &t, BlockSmem<D> &sb) {
+    uint32_t nl = 0, ns = 0;
+    for (uint32_t q = 0; q < sb.nout; q++) (sb.out[q] >> 31 ? ns : nl)++;
+    uint32_t bl = nl ? atomicAdd(&t.kmeta[7], nl) : 0u;
+    uint32_t bs = ns ? atomicAdd(&t.meta[kMetaSmall], ns) : 0u;
+    for (uint32_t q = 0; q < sb.nout; q++) {
+        const uint32_t v = sb.out[q];
+        if (v >> 31) t.small[bs++] = v & 0x7FFFFFFFu;
+        else t.kdone[bl++] = v;
+    }
+    sb.nout = 0u;
+}
+
+// Level-loop work of one node of a block rebuild (list entry e of the current
+// level) per group of G lanes.  Children's slots come from the block's chunk
+// (or the pool *alloc above `base`); the searches probe the staged
+// coordinates.  Children that are not
+// leaves and hold more than kSmallNode particles go to the next level's list;
+// leaves and small subtrees to the block's buffer.  No fence: the next level
+// reads the lists after a block barrier, and everything else reads these
+// nodes after a grid barrier.
 template <int D, int G>
-__device__ __forceinline__ void rebuild_large_node(const State &s, const StepParams &p, Tree &t,
-                                                   uint32_t k, bool valid, uint32_t base,
-                                                   uint32_t *alloc, uint32_t *next,
-                                                   uint32_t *next_cnt, uint32_t *err,
-                                                   const float (*sx)[kBlockRootMax], uint32_t off) {
+__device__ __forceinline__ void rebuild_level_node(const StepParams &p, Tree &t, BlockSmem<D> &sb,
+                                                   int cur, uint32_t e, bool valid, uint32_t base,
+                                                   uint32_t *alloc, uint32_t *err, uint32_t off) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
-    uint4 inf = make_uint4(0, 0, 0, 0), ax = make_uint4(0, 0, 0, 0);
+    uint32_t k = 0;
+    uint4 inf = make_uint4(0, 0, 0, 0);
+    uint2 ax = make_uint2(0u, 0u);
     float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-        inf = __ldcg(&t.info[k]);
-        cell = __ldcg(&t.cell[k]);
-        ax = __ldcg(&t.aux[k]);
+        k = sb.node[cur][e];
+        inf = sb.inf[cur][e];
+        cell = sb.cell[cur][e];
+        ax = sb.ax[cur][e];
     }
     const float half = fmul(cell.w, 0.5f);
     const float mid[3] = {fadd(cell.x, half), fadd(cell.y, half), fadd(cell.z, half)};
     uint32_t b[Q + 1];
-    cut_group_v<D, G, true>(sx[0], sx[1], sx[D - 1], off, valid ? inf.z : 0u, valid ? inf.w : 0u,
-                            mid, b);
+    cut_group_v<D, G, true>(sb.x[0], sb.x[1], sb.x[D - 1], off, valid ? inf.z : 0u,
+                            valid ? inf.w : 0u, mid, b);
     uint32_t mask = 0;
     if (valid) {
 #pragma unroll
@@ -416,7 +482,7 @@ __device__ __forceinline__ void rebuild_large_node(const State &s, const StepPar
     float4 cend = c1;
     if (__any_sync(0xffffffffu, single)) {
         bool nan;
-        group_bbox<D, G>(sx[0], sx[1], sx[D - 1], off, inf.z, inf.w, single, mn, mx, nan);
+        group_bbox<D, G>(sb.x[0], sb.x[1], sb.x[D - 1], off, inf.z, inf.w, single, mn, mx, nan);
         if (single && !nan) j = chain_length<D>(p, inf.w - inf.z, cend, ax.x + 1u, mn, mx);
     }
     const bool leader = valid && gl == 0;
@@ -428,38 +494,62 @@ __device__ __forceinline__ void rebuild_large_node(const State &s, const StepPar
         if (lane >= (unsigned)o) incl += v;
     }
     const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+    // slots from the block's chunk, or exactly tot from the pool when the
+    // chunk cannot hold them (chains)
     uint32_t wbase = 0;
-    if (lane == 0 && tot) wbase = atomicAdd(alloc, tot);
+    if (lane == 0 && tot) {
+        const uint32_t a = atomicAdd(&sb.anext, tot);
+        if (a + tot <= sb.aend && a + tot > a) {
+            wbase = a;
+            atomicMax(&sb.aused, a + tot);
+        } else {
+            wbase = base + atomicAdd(alloc, tot);
+        }
+        atomicAdd(&sb.real, tot);
+    }
     wbase = __shfl_sync(0xffffffffu, wbase, 0);
-    // every lane of the group learns where its node's children start
-    uint32_t first = base + wbase + incl - nch;
+    uint32_t first = wbase + incl - nch;
     first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1u));
-    bool ok = (uint64_t)base + wbase + tot <= (uint64_t)t.cap;
-    if (!ok && lane == 0) set_err(err, kErrNodeCap);
+    const bool ok = (uint64_t)wbase + tot <= (uint64_t)t.cap;
+    if (!ok && lane == 0) {
+        set_err(err, kErrNodeCap);
+        sb.bad = 1u;
+    }
     if (leader && ok) {
-        emit_children<D>(t, k, first, mask, b, cell, half, inf, ax);
+        t.info[k] = make_uint4(first, mask, inf.z, inf.w);
+        t.pend[k] = (uint32_t)__popc(mask);
         if (j) {
+            t.cell[first] = c1;
+            t.aux[first] = make_uint4(ax.x + 1u, ax.y + 1u, k, 0u);
+        }
+        if (j)
             write_chain<D>(t, first, j, inf.z, inf.w, c1, make_uint4(ax.x + 1u, ax.y + 1u, k, 0u),
                            mn, mx);
-            __threadfence();
-        }
     }
-    __syncwarp();
-    // the group's lane q takes child q (a chain's last node for a single child)
+    // the group's lane q writes child q (a chain's last node for a single child)
     if (valid && ok && gl < (unsigned)Q && ((mask >> gl) & 1u)) {
+        const uint32_t lo = b[gl], hi = b[gl + 1], cnt = hi - lo;
         const uint32_t c = first + __popc(mask & ((1u << gl) - 1u)) + j;
-        const uint32_t cnt = b[gl + 1] - b[gl];
-        const float csize = j ? cend.w : half;
-        if (is_leaf<D>(p, cnt, csize)) {
+        const float4 cc = j ? cend : child_cell<D>(cell, half, gl);
+        const uint32_t lvl = ax.x + 1u + j;
+        const uint32_t same = hi == inf.w ? ax.y + 1u + j : 0u;
+        t.cell[c] = cc;
+        t.info[c] = make_uint4(0u, 0u, lo, hi);
+        t.aux[c] = make_uint4(lvl, same, j ? first + j - 1u : k, 0u);
+        if (is_leaf<D>(p, cnt, cc.w)) {
             // its upward pass waits for the end of the rebuilds, so that no
             // level of this loop waits for a chain up the whole tree
-            put_walk<D>(t, c, leaf_mass<D>(s, b[gl], b[gl + 1]), csize);
-            t.kdone[atomicAdd(&t.kmeta[7], 1u)] = c;
-            atomicMax(&t.meta[kMetaLevels], ax.x + 2u + j);
+            put_walk<D>(t, c, leaf_mass_smem<D>(sb, lo - off, hi - off), cc.w);
+            sb.out[atomicAdd(&sb.nout, 1u)] = c;
+            atomicMax(&sb.maxlev, lvl + 1u);
         } else if (cnt <= kSmallNode) {
-            t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = c;
+            sb.out[atomicAdd(&sb.nout, 1u)] = c | 0x80000000u;
         } else {
-            next[atomicAdd(next_cnt, 1u)] = c;
+            const uint32_t q = atomicAdd(&sb.cnt[cur ^ 1], 1u);
+            sb.node[cur ^ 1][q] = c;
+            sb.inf[cur ^ 1][q] = make_uint4(0u, 0u, lo, hi);
+            sb.cell[cur ^ 1][q] = cc;
+            sb.ax[cur ^ 1][q] = make_uint2(lvl, same);
         }
     }
 }
@@ -818,15 +908,15 @@ template <int D>
 __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tree &t, uint32_t k,
                                               uint4 inf, uint4 ax, float4 w, float size2,
                                               uint32_t ez, uint32_t ew, uint32_t total,
-                                              uint32_t *err, bool packed) {
+                                              uint32_t *err, bool packed, int extras) {
     const uint32_t me = ez + ax.x + inf.z;
     const uint32_t skip = ew + ax.x - ax.y + inf.w;
     if (me >= total || skip > total) {   // cannot happen for a consistent tree
         set_err(err, kErrDepth);
         return;
     }
-    t.aux[k].w = me;   // the node's entry (read by the moment pass)
-    t.nrange[k] = make_uint2(me, skip);   // its layout range (read by the warp walk)
+    if (extras & kLayoutEntry) t.aux[k].w = me;   // the node's entry
+    if (extras & kLayoutRange) t.nrange[k] = make_uint2(me, skip);   // its layout range
     if (k < (uint32_t)g.S) {   // a segment's root: where its particles' walks start and end
         g.root_begin[k] = me;
         g.root_end[k] = skip;
@@ -842,13 +932,13 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
                                          packed ? __uint_as_float(pack_entry_word(kPackMassless, skip))
                                                 : -2.0f)
                            : make_float4(w.x, w.y, w.z, 0.0f);
-        if (D == 2) ((uint32_t *)t.link)[me] = skip;
-        else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
+        if (D == 3) ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(-2.0f));
+        else if (!packed) ((uint32_t *)t.link)[me] = skip;
     } else {
         t.src[me] = D == 2 && packed ? make_float4(w.x, w.y, w.z, __uint_as_float(pack_entry_word(ax.x, skip)))
                                      : w;
-        if (D == 2) ((uint32_t *)t.link)[me] = skip;
-        else ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(size2));
+        if (D == 3) ((uint2 *)t.link)[me] = make_uint2(skip, __float_as_uint(size2));
+        else if (!packed) ((uint32_t *)t.link)[me] = skip;
     }
     if (inf.y) return;
     // a leaf: its particles follow it, four at a time (loads before stores)
@@ -874,7 +964,7 @@ __device__ __forceinline__ void scatter_entry(const State &s, const Segs &g, Tre
                 t.src[e] = make_float4(px[q], py[q], pm[q],
                                        packed ? __uint_as_float(pack_entry_word(kPackParticle, e + 1))
                                               : -1.0f);
-                ((uint32_t *)t.link)[e] = e + 1;
+                if (!packed) ((uint32_t *)t.link)[e] = e + 1;
             } else {
                 t.src[e] = make_float4(px[q], py[q], pz[q], pm[q]);
                 ((uint2 *)t.link)[e] = make_uint2(e + 1, __float_as_uint(-1.0f));
@@ -895,9 +985,9 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     uint32_t *bar_count = t.meta + kMetaBarCount, *bar_gen = t.meta + kMetaBarGen;
     // the block rebuilds' staged coordinates, then phase 2's per-warp subtrees
     constexpr size_t kSharedBytes = sizeof(SubTreeSmem) * (kBuildThreads / 32) >
-                                            sizeof(float) * D * kBlockRootMax
+                                            sizeof(BlockSmem<D>)
                                         ? sizeof(SubTreeSmem) * (kBuildThreads / 32)
-                                        : sizeof(float) * D * kBlockRootMax;
+                                        : sizeof(BlockSmem<D>);
     __shared__ __align__(16) unsigned char s_shared[kSharedBytes];
 
     // Keyed: the key passes (ge_kbuild.cu) wrote key_nodes nodes in slots
@@ -1022,17 +1112,25 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
 
     if (keyed) {
         // exact-rebuild roots of up to kBlockRootMax particles: a block each
-        __shared__ uint32_t s_list[2][kBlkList];
-        __shared__ uint32_t s_cnt[2], s_m;
-        // the root's coordinates (shares its memory with phase 2's subtrees)
-        float (*s_xs)[kBlockRootMax] = reinterpret_cast<float (*)[kBlockRootMax]>(s_shared);
+        // (shares its memory with phase 2's subtrees)
+        BlockSmem<D> &sb = *reinterpret_cast<BlockSmem<D> *>(s_shared);
         // the key passes' roots of at most kBlockRootMax particles, then the
         // nodes of at most kBlockRootMax particles that phase 1 handed over
         const uint32_t nroots = nroots0 + *(volatile uint32_t *)&t.kmeta[kKmBlockQ];
+        // slots come from phase 2's pool (above the phase-1 slots)
         const uint32_t xbase = le;
-        uint32_t *xalloc = &t.kmeta[6];
+        uint32_t *xalloc = &t.meta[kMetaP2Alloc];
         const unsigned w = threadIdx.x >> 5, W = kBuildThreads / 32;
-        for (uint32_t r = blockIdx.x; r < nroots; r += gridDim.x) {
+        if (threadIdx.x == 0) {
+            sb.nout = 0u; sb.maxlev = 0u; sb.bad = 0u;
+            sb.anext = sb.aend = sb.aused = 0u; sb.real = 0u; sb.hole_a = sb.hole_b = 0u;
+        }
+        while (true) {   // roots taken from a counter (their costs differ)
+            __syncthreads();
+            if (threadIdx.x == 0) sb.mcur = atomicAdd(&t.kmeta[kKmBlockTake], 1u);
+            __syncthreads();
+            const uint32_t r = sb.mcur;
+            if (r >= nroots) break;
             const uint32_t root = __ldcg(&t.kroots[r]);
             const uint4 ri = __ldcg(&t.info[root]);
             const uint32_t cnt = ri.w - ri.z;
@@ -1041,32 +1139,59 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                 if (threadIdx.x == 0) t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = root;
                 continue;
             }
-            if (threadIdx.x == 0) { s_list[0][0] = root; s_cnt[0] = 1u; }
+            if (threadIdx.x == 0) {
+                const uint4 rx = __ldcg(&t.aux[root]);
+                sb.node[0][0] = root;
+                sb.inf[0][0] = ri;
+                sb.cell[0][0] = __ldcg(&t.cell[root]);
+                sb.ax[0][0] = make_uint2(rx.x, rx.y);
+                sb.cnt[0] = 1u;
+                if ((*(volatile uint32_t *)err) & kErrNodeCap) sb.bad = 1u;
+            }
             for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
-                s_xs[0][j] = s.x[ri.z + j];
-                s_xs[1][j] = s.y[ri.z + j];
-                if (D == 3) s_xs[D - 1][j] = s.z[ri.z + j];
+                sb.x[0][j] = s.x[ri.z + j];
+                sb.x[1][j] = s.y[ri.z + j];
+                if (D == 3) sb.x[D - 1][j] = s.z[ri.z + j];
+                sb.m[j] = s.m[ri.z + j];
             }
             int cur = 0;
             for (int it = 0; it < kMaxLevels; it++) {
                 if (threadIdx.x == 0) {   // one decision for the whole block
-                    s_cnt[cur ^ 1] = 0u;
-                    s_m = ((*(volatile uint32_t *)err) & kErrNodeCap) ? 0u : s_cnt[cur];
+                    sb.cnt[cur ^ 1] = 0u;
+                    sb.hole_a = sb.hole_b = 0u;
+                    sb.mcur = sb.bad ? 0u : sb.cnt[cur];
+                    if (sb.nout + sb.mcur * (1u << D) > (uint32_t)kBlkOut) flush_block_out<D>(t, sb);
+                    // a fresh chunk when this level's children may not fit (the
+                    // old chunk's unused tail becomes holes)
+                    const uint32_t need = sb.mcur * (1u << D);
+                    if (sb.mcur && sb.aend - sb.aused < need) {
+                        sb.hole_a = sb.aused;
+                        sb.hole_b = sb.aend;
+                        const uint32_t want = need > kBlkChunk / 2 ? 2u * need : kBlkChunk;
+                        const uint32_t g = xbase + atomicAdd(xalloc, want);
+                        if ((uint64_t)g + want > (uint64_t)t.cap) {
+                            set_err(err, kErrNodeCap);
+                            sb.bad = 1u;
+                            sb.mcur = 0u;
+                            sb.anext = sb.aend = sb.aused = 0u;
+                        } else {
+                            sb.anext = sb.aused = g;
+                            sb.aend = g + want;
+                        }
+                    }
                 }
                 __syncthreads();
-                const uint32_t m = s_m;
+                const uint32_t m = sb.mcur;
+                for (uint32_t q = sb.hole_a + threadIdx.x; q < sb.hole_b; q += blockDim.x)
+                    t.info[q] = make_uint4(0u, 0u, 0u, 0u);
                 if (m == 0u) break;
                 if (m <= W) {
                     for (uint32_t j = w; j < m; j += W)
-                        rebuild_large_node<D, 32>(s, p, t, s_list[cur][j], true, xbase, xalloc,
-                                                  s_list[cur ^ 1], &s_cnt[cur ^ 1], err, s_xs,
-                                                  ri.z);
+                        rebuild_level_node<D, 32>(p, t, sb, cur, j, true, xbase, xalloc, err, ri.z);
                 } else {
                     for (uint32_t jb = w * 4; jb < m; jb += W * 4) {
                         const uint32_t j = jb + (lane >> 3);
-                        rebuild_large_node<D, 8>(s, p, t, j < m ? s_list[cur][j] : 0u, j < m,
-                                                 xbase, xalloc, s_list[cur ^ 1], &s_cnt[cur ^ 1],
-                                                 err, s_xs, ri.z);
+                        rebuild_level_node<D, 8>(p, t, sb, cur, j, j < m, xbase, xalloc, err, ri.z);
                     }
                 }
                 __syncthreads();
@@ -1074,11 +1199,21 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             }
             __syncthreads();
         }
+        if (threadIdx.x == 0) {
+            flush_block_out<D>(t, sb);
+            if (sb.maxlev) atomicMax(&t.meta[kMetaLevels], sb.maxlev);
+            if (sb.real) atomicAdd(&t.meta[kMetaReal], sb.real);
+            sb.hole_a = sb.aused;
+            sb.hole_b = sb.aend;
+        }
+        __syncthreads();
+        for (uint32_t q = sb.hole_a + threadIdx.x; q < sb.hole_b; q += blockDim.x)
+            t.info[q] = make_uint4(0u, 0u, 0u, 0u);
     }
-    if (keyed) {   // the blocks' slots follow phase 1's
+
+    if (keyed) {   // the small subtrees and deferred leaves are all listed
         grid_barrier(bar_count, bar_gen, err);
         if (gtid == 0) stamp(t);
-        le += *(volatile uint32_t *)&t.kmeta[6];
         if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
     }
 
@@ -1269,7 +1404,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         for (int u = 0; u < 2; u++) {
             if (inf[u].w == 0u) continue;
             scatter_entry<D>(s, g, t, kk[u], inf[u], ax[u], wv[u], s2[u], ez[u], ew[u], total, err,
-                             packed);
+                             packed, p.layout_extras);
         }
     }
     // the last block to finish stamps the end of the build
@@ -1284,9 +1419,12 @@ static int g_build_blocks[2] = {0, 0};
 
 int build_grid_blocks(int dims, int num_sms);
 
-// Node slots the build may leave unused: each warp's last phase-2 chunk.
+// Node slots the build may leave unused: each warp's last phase-2 chunk and
+// each block's last block-rebuild chunk.
 int64_t build_node_slack(int dims, int num_sms) {
-    return (int64_t)build_grid_blocks(dims, num_sms) * (kBuildThreads / 32) * kChunk;
+    const int64_t blk = 2 * (int64_t)kBlkList * (dims == 2 ? 4 : 8);
+    return (int64_t)build_grid_blocks(dims, num_sms) *
+           ((kBuildThreads / 32) * kChunk + (blk > kBlkChunk ? blk : kBlkChunk));
 }
 
 int build_grid_blocks(int dims, int num_sms) {
