@@ -297,6 +297,9 @@ int alloc_buffers(ge_ctx *c, Buffers &nb, int64_t cap, int64_t node_cap, bool pr
     GE_CHECK(c, dalloc(L, &t.aux, (size_t)node_cap));
     GE_CHECK(c, dalloc(L, &t.pend, (size_t)node_cap));
     GE_CHECK(c, dalloc(L, &t.small, N / 2 + 1));
+    t.small_cap = (uint32_t)(N / 2 + 1);
+    // entries carry the id of the build that queued them (ids start at 1)
+    if (!L.dry) GE_CHECK(c, cudaMemsetAsync(t.small, 0, sizeof(uint2) * (N / 2 + 1), c->stream));
     GE_CHECK(c, dalloc(L, &t.endcnt, N + 1));
     const int bblocks = build_grid_blocks(D, c->num_sms);
     if (bblocks < 1) return fail(c, GE_ERR_CUDA, "tree build kernel cannot be made resident");

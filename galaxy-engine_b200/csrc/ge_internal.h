@@ -80,7 +80,8 @@ struct Tree {
     float4 *cell;
     uint4 *aux;
     uint32_t *pend;
-    uint32_t *small;      // [n / 2] queued small subtrees (build only)
+    uint2 *small;         // [small_cap] queued small subtrees {node slot, build id} (build only)
+    uint32_t small_cap;
     uint32_t *endcnt;    // [n + 1] node-end histogram, scanned in place
     uint32_t *blocksum;   // [build grid] scan partials
     float4 *src;          // [n + cap + 1]
@@ -317,7 +318,7 @@ constexpr int kKeyMaxCap = 32;   // leaf capacities the key-prefix build handles
 constexpr int kKeyTile = 256;    // particles per tile of its node-count scan (one per thread)
 constexpr int kKeyBigCap = 256;   // large exact-rebuild roots recorded per build
 constexpr int kKeyBigHash = 1024; // slots of their set
-constexpr int kKeyMetaWords = 64;
+constexpr int kKeyMetaWords = 96;
 int64_t key_suspect_cap(int64_t n);
 cudaError_t launch_key_build(int dims, const State &s, const StepParams &p, const Segs &g,
                              const uint64_t *keys, Tree &t, uint32_t *err, int num_sms,

@@ -46,7 +46,7 @@ constexpr uint32_t kSmallNode = 32;
 // meta[] words used by the build
 constexpr int kMetaNodes = 0, kMetaLevels = 1, kMetaBarCount = 2, kMetaBarGen = 3,
               kMetaSmall = 5, kMetaP2Alloc = 6, kMetaTimeline = 7, kMetaReal = 8, kMetaSlots = 9,
-              kMetaP2Task = 12, kMetaDone = 15;
+              kMetaP2Task = 12, kMetaDone = 15, kMetaBuildId = 16;
 constexpr uint32_t kChunk = 256;   // node slots a warp takes at a time in phase 2
 // keyed builds: exact-rebuild roots and phase-1 nodes of at most kBlockRootMax
 // particles are rebuilt by one block each
@@ -57,6 +57,7 @@ constexpr uint32_t kBlockRootMax = GE_BLOCK_ROOT_MAX;
 constexpr int kBlkList = (int)(kBlockRootMax / kSmallNode);
 constexpr int kKmBlockQ = 33;   // key meta word: phase-1 nodes handed to the blocks
 constexpr int kKmBlockTake = 34;   // key meta word: next block root to take
+constexpr int kKmProdDone = 64;    // key meta word (a cache line of its own): blocks done queueing
 
 // Bounded grid-wide barrier for a cooperative launch (all blocks resident).
 __device__ __forceinline__ void grid_barrier(uint32_t *bar_count, uint32_t *bar_gen,
@@ -286,7 +287,8 @@ template <int D, int G>
 __device__ __forceinline__ void split_level_node(const State &s, const StepParams &p, Tree &t,
                                                  uint32_t k, bool valid, uint32_t level_end,
                                                  uint32_t *lvl_alloc, uint32_t *err,
-                                                 bool defer = false, uint32_t *handoff = nullptr) {
+                                                 uint32_t bid, bool defer = false,
+                                                 uint32_t *handoff = nullptr) {
     constexpr int Q = 1 << D;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gl = lane & (G - 1u);
@@ -340,7 +342,7 @@ __device__ __forceinline__ void split_level_node(const State &s, const StepParam
         uint32_t qbase = 0;
         if (lane == 0 && qb) qbase = atomicAdd(&t.meta[kMetaSmall], (uint32_t)__popc(qb));
         qbase = __shfl_sync(0xffffffffu, qbase, 0);
-        if (leader && small) t.small[qbase + __popc(qb & ((1u << lane) - 1u))] = k;
+        if (leader && small) t.small[qbase + __popc(qb & ((1u << lane) - 1u))] = make_uint2(k, bid);
         const unsigned bb = __ballot_sync(0xffffffffu, leader && block);
         uint32_t bbase = 0;
         if (lane == 0 && bb) bbase = atomicAdd(&t.kmeta[kKmBlockQ], (uint32_t)__popc(bb));
@@ -402,6 +404,7 @@ struct BlockSmem {
     // the block's slots: a chunk [anext, aend) of the phase-2 pool (used up
     // to aused), `real` slots used in all, a hole range to zero
     uint32_t anext, aend, aused, real, hole_a, hole_b;
+    uint32_t r0;   // the block's current root (list position)
 };
 constexpr uint32_t kBlkChunk = 512;   // slots a block takes at a time (at least)
 
@@ -424,16 +427,19 @@ __device__ __forceinline__ float4 leaf_mass_smem(const BlockSmem<D> &b, uint32_t
     return make_float4(c[0], c[1], c[2], gm);
 }
 
-// Publish the block's buffered leaves and small subtrees (one thread).
+// Publish the block's buffered leaves and small subtrees (one thread, after a
+// block barrier: the fence makes the block's node writes visible before the
+// entries that lead other warps to them).
 template <int D>
-__device__ __forceinline__ void flush_block_out(Tree &t, BlockSmem<D> &sb) {
+__device__ __forceinline__ void flush_block_out(Tree &t, BlockSmem<D> &sb, uint32_t bid) {
+    __threadfence();
     uint32_t nl = 0, ns = 0;
     for (uint32_t q = 0; q < sb.nout; q++) (sb.out[q] >> 31 ? ns : nl)++;
     uint32_t bl = nl ? atomicAdd(&t.kmeta[7], nl) : 0u;
     uint32_t bs = ns ? atomicAdd(&t.meta[kMetaSmall], ns) : 0u;
     for (uint32_t q = 0; q < sb.nout; q++) {
         const uint32_t v = sb.out[q];
-        if (v >> 31) t.small[bs++] = v & 0x7FFFFFFFu;
+        if (v >> 31) t.small[bs++] = make_uint2(v & 0x7FFFFFFFu, bid);
         else t.kdone[bl++] = v;
     }
     sb.nout = 0u;
@@ -1005,7 +1011,9 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         t.meta[kMetaNodes] = 0u; t.meta[kMetaLevels] = 0u;
         t.meta[kMetaSmall] = 0u; t.meta[kMetaP2Alloc] = 0u; t.meta[kMetaTimeline] = 0u;
         t.meta[kMetaReal] = 0u; t.meta[kMetaSlots] = 0u; t.meta[kMetaP2Task] = 0u;
-        t.meta[kMetaBigRoot] = 0u; t.meta[kMetaDone] = 0u;
+        t.meta[kMetaBigRoot] = 0u; t.meta[kMetaDone] = 0u; t.kmeta[kKmProdDone] = 0u;
+        const uint32_t id = t.meta[kMetaBuildId] + 1u;   // read after the first grid barrier
+        t.meta[kMetaBuildId] = id ? id : 1u;
         stamp(t);
     }
     for (uint32_t i = gtid; i < (uint32_t)kMaxLevels + 2u; i += nthreads) t.lvl_alloc[i] = 0u;
@@ -1053,8 +1061,9 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     }
 
     // ---- phase 1: nodes of more than kSmallNode particles, level by level ----
-    // the first level is the segment roots (or, keyed, the exact-rebuild roots
-    // too large for one block, by list); children go to slots from `front` on
+    // the first level is the segment roots (or, keyed, the exact-rebuild roots,
+    // by list: those of at most kBlockRootMax particles go to the block list,
+    // the small ones to the subtree queue); children go to slots from `front` on
     int L = 0;
     if (gtid == 0) t.level[0] = lb;
     if (!keyed) {   // the roots' links above
@@ -1062,28 +1071,20 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         if (gtid == 0) stamp(t);
     }
     const uint32_t nroots0 = le;   // keyed: the key passes' exact-rebuild roots
+    const uint32_t bid = *(volatile uint32_t *)&t.meta[kMetaBuildId];   // this build's id
     while (true) {
         if (le - lb <= nwarps) {
             for (uint32_t k = lb + gwarp; k < le; k += nwarps) {
                 const uint32_t node = list ? __ldcg(&list[k]) : k;
-                bool valid = true;
-                if (list) {   // keyed first level: only the roots no block took
-                    const uint4 ri = __ldcg(&t.info[node]);
-                    valid = ri.w - ri.z > kBlockRootMax;
-                }
-                split_level_node<D, 32>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed,
+                split_level_node<D, 32>(s, p, t, node, true, front, &t.lvl_alloc[L], err, bid, keyed,
                                         keyed ? t.kroots + nroots0 : nullptr);
             }
         } else {
             for (uint32_t kb = lb + gwarp * 4; kb < le; kb += nwarps * 4) {
                 const uint32_t k = kb + (lane >> 3);
                 const uint32_t node = list && k < le ? __ldcg(&list[k]) : k;
-                bool valid = k < le;
-                if (valid && list) {
-                    const uint4 ri = __ldcg(&t.info[node]);
-                    valid = ri.w - ri.z > kBlockRootMax;
-                }
-                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, keyed,
+                const bool valid = k < le;
+                split_level_node<D, 8>(s, p, t, node, valid, front, &t.lvl_alloc[L], err, bid, keyed,
                                        keyed ? t.kroots + nroots0 : nullptr);
             }
         }
@@ -1114,9 +1115,9 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         // exact-rebuild roots of up to kBlockRootMax particles: a block each
         // (shares its memory with phase 2's subtrees)
         BlockSmem<D> &sb = *reinterpret_cast<BlockSmem<D> *>(s_shared);
-        // the key passes' roots of at most kBlockRootMax particles, then the
-        // nodes of at most kBlockRootMax particles that phase 1 handed over
-        const uint32_t nroots = nroots0 + *(volatile uint32_t *)&t.kmeta[kKmBlockQ];
+        // the nodes of 33 .. kBlockRootMax particles that phase 1 handed over
+        // (its first level is the key passes' exact-rebuild roots)
+        const uint32_t nblk = *(volatile uint32_t *)&t.kmeta[kKmBlockQ];
         // slots come from phase 2's pool (above the phase-1 slots)
         const uint32_t xbase = le;
         uint32_t *xalloc = &t.meta[kMetaP2Alloc];
@@ -1125,20 +1126,16 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             sb.nout = 0u; sb.maxlev = 0u; sb.bad = 0u;
             sb.anext = sb.aend = sb.aused = 0u; sb.real = 0u; sb.hole_a = sb.hole_b = 0u;
         }
-        while (true) {   // roots taken from a counter (their costs differ)
+        // roots taken one at a time from a counter (their costs differ)
+        while (true) {
             __syncthreads();
-            if (threadIdx.x == 0) sb.mcur = atomicAdd(&t.kmeta[kKmBlockTake], 1u);
+            if (threadIdx.x == 0) sb.r0 = atomicAdd(&t.kmeta[kKmBlockTake], 1u);
             __syncthreads();
-            const uint32_t r = sb.mcur;
-            if (r >= nroots) break;
-            const uint32_t root = __ldcg(&t.kroots[r]);
+            const uint32_t r = sb.r0;
+            if (r >= nblk) break;
+            const uint32_t root = __ldcg(&t.kroots[nroots0 + r]);
             const uint4 ri = __ldcg(&t.info[root]);
             const uint32_t cnt = ri.w - ri.z;
-            if (cnt > kBlockRootMax) continue;   // left to the grid's level loop
-            if (cnt <= kSmallNode) {
-                if (threadIdx.x == 0) t.small[atomicAdd(&t.meta[kMetaSmall], 1u)] = root;
-                continue;
-            }
             if (threadIdx.x == 0) {
                 const uint4 rx = __ldcg(&t.aux[root]);
                 sb.node[0][0] = root;
@@ -1160,7 +1157,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                     sb.cnt[cur ^ 1] = 0u;
                     sb.hole_a = sb.hole_b = 0u;
                     sb.mcur = sb.bad ? 0u : sb.cnt[cur];
-                    if (sb.nout + sb.mcur * (1u << D) > (uint32_t)kBlkOut) flush_block_out<D>(t, sb);
+                    if (sb.nout + sb.mcur * (1u << D) > (uint32_t)kBlkOut) flush_block_out<D>(t, sb, bid);
                     // a fresh chunk when this level's children may not fit (the
                     // old chunk's unused tail becomes holes)
                     const uint32_t need = sb.mcur * (1u << D);
@@ -1200,7 +1197,7 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             __syncthreads();
         }
         if (threadIdx.x == 0) {
-            flush_block_out<D>(t, sb);
+            flush_block_out<D>(t, sb, bid);
             if (sb.maxlev) atomicMax(&t.meta[kMetaLevels], sb.maxlev);
             if (sb.real) atomicAdd(&t.meta[kMetaReal], sb.real);
             sb.hole_a = sb.aused;
@@ -1211,14 +1208,45 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
             t.info[q] = make_uint4(0u, 0u, 0u, 0u);
     }
 
-    if (keyed) {   // the small subtrees and deferred leaves are all listed
-        grid_barrier(bar_count, bar_gen, err);
-        if (gtid == 0) stamp(t);
-        if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
+    // this block queues nothing more (its entries and nodes are visible first)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&t.kmeta[kKmProdDone], 1u);
     }
 
     // ---- phase 2: queued small subtrees, one warp each, no barriers --------
-    const uint32_t nsmall = *(volatile uint32_t *)&t.meta[kMetaSmall];
+    // A warp claims queue positions from a counter and takes each one's entry
+    // once it is written (an entry of this build carries its id), while other
+    // blocks may still be rebuilding and queueing; it stops at a position
+    // past the final count, known once every block has finished queueing.
+    // The wait polls the claimed entry (and, every eighth poll, the
+    // producers' count, which has a cache line of its own), backing off.
+    auto take = [&](uint32_t task) -> uint32_t {   // lane 0
+        uint32_t ns = 32;
+        for (uint32_t spins = 0;; spins++) {
+            if (task < t.small_cap) {
+                const uint2 e = __ldcv(&t.small[task]);
+                if (e.y == bid) {
+                    __threadfence();   // the subtree's nodes were written before its entry
+                    return e.x;
+                }
+            }
+            if ((spins & 7u) == 7u) {
+                if (*(volatile uint32_t *)&t.kmeta[kKmProdDone] == gridDim.x) {
+                    __threadfence();
+                    if (task >= *(volatile uint32_t *)&t.meta[kMetaSmall]) return kEmpty;
+                }
+                if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return kEmpty;
+            }
+            if (spins > kSpinLimit) {
+                set_err(err, kErrSpin);
+                return kEmpty;
+            }
+            __nanosleep(ns);
+            if (ns < 2048) ns *= 2;
+        }
+    };
     {
         SubTreeSmem &sm = reinterpret_cast<SubTreeSmem *>(s_shared)[threadIdx.x >> 5];
         WarpAlloc wa{0u, 0u, 0u};
@@ -1226,13 +1254,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         // j-th finished subtree root whose upward pass is still to run, and the
         // warp runs 32 of them at once, so their atomics' round trips overlap
         uint32_t held = kEmpty, nheld = 0;
-        uint32_t task = 0;
-        if (lane == 0) task = atomicAdd(&t.meta[kMetaP2Task], 1u);
-        task = __shfl_sync(0xffffffffu, task, 0);
-        while (task < nsmall) {
+        uint32_t R = kEmpty;
+        if (lane == 0) R = take(atomicAdd(&t.meta[kMetaP2Task], 1u));
+        R = __shfl_sync(0xffffffffu, R, 0);
+        while (R != kEmpty) {
             uint32_t next = 0;
             if (lane == 0) next = atomicAdd(&t.meta[kMetaP2Task], 1u);
-            const uint32_t R = __ldcg(&t.small[task]);
             if (build_small_subtree_smem<D>(s, p, t, R, le, sm, wa, err)) {
                 if (lane == nheld) held = R;
                 if (++nheld == 32u) {
@@ -1245,7 +1272,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                 build_small_subtree<D>(s, p, t, R, le, wa, err);   // passes its own leaves upward
             }
             __syncwarp();
-            task = __shfl_sync(0xffffffffu, next, 0);
+            if (lane == 0) R = take(next);
+            R = __shfl_sync(0xffffffffu, R, 0);
         }
         __syncwarp();
         if (held != kEmpty) finish_upward<D>(t, held);
