@@ -210,13 +210,52 @@ __device__ __forceinline__ void flush_parts(const GWSmem<D> &sm, int pl, GroupSt
 // into one group while the run holds at most GS particles.  A group is then
 // a contiguous particle range inside one cell (its parent's), so its
 // bounding box stays compact.  A leaf of more than GS particles (a cell at
-// the minimum size) is cut into GS-particle pieces.  The groups depend only
-// on the tree, so a simulation forms the same groups alone and in a batch.
+// the minimum size) is cut into GS-particle pieces.  A sparse child (below)
+// is split down its subtree instead.  The groups depend only on the tree, so
+// a simulation forms the same groups alone and in a batch.
 __device__ __forceinline__ void emit_group(const Tree &t, uint32_t a, uint32_t b) {
     const uint32_t k = atomicAdd(&t.meta[kMetaGroupCount], 1u);
     t.grp[k] = make_uint2(a, b);
 }
 
+// A node of c particles and cell size s is sparse, relative to a parent of
+// C particles and size S, when its particles' mean spacing is more than four
+// times the parent's: (s / S)^D C > 4^D c.  A group made of it would have a
+// box far larger than the matter around it warrants (halo and tidal-tail
+// particles in a cell beside a dense disk: one such group of 57 particles
+// spread over 6 x 10 units opened ~11,000 particles for every member and
+// held one warp for 3.5 ms), so it is split down its subtree, depth first
+// with a stack of 256 entries, into nodes dense enough by the same reference,
+// or leaves (the node whole when the stack is full).
+template <int D>
+__device__ __forceinline__ bool sparse_node(float s, uint32_t c, float S, uint32_t C) {
+    const double r = (double)s / (double)S;
+    const double rd = D == 2 ? r * r : r * r * r;
+    return rd * (double)C > (D == 2 ? 16.0 : 64.0) * (double)c;
+}
+
+template <int D>
+__device__ void emit_split(const Tree &t, uint32_t node, float S, uint32_t C) {
+    constexpr int kStack = 256;
+    uint32_t stack[kStack];
+    int top = 0;
+    stack[top++] = node;
+    while (top > 0) {
+        const uint32_t k = stack[--top];
+        const uint4 inf = __ldcg(&t.info[k]);
+        if (inf.w <= inf.z) continue;
+        const int nc = __popc(inf.y);
+        // a leaf, a node dense enough, or (stack full) the node whole
+        if (!inf.y || !sparse_node<D>(__ldcg(&t.cell[k]).w, inf.w - inf.z, S, C) ||
+            top + nc > kStack) {
+            emit_group(t, inf.z, inf.w);
+            continue;
+        }
+        for (int q = nc - 1; q >= 0; q--) stack[top++] = inf.x + (uint32_t)q;
+    }
+}
+
+template <int D>
 __global__ void k_make_groups(Tree t, uint32_t GS) {
     dep_wait();
     const uint32_t slots = __ldcg(&t.meta[kMetaSlotsW]);
@@ -234,13 +273,21 @@ __global__ void k_make_groups(Tree t, uint32_t GS) {
             continue;
         }
         const int nc = __popc(inf.y);
+        const float S = __ldcg(&t.cell[k]).w;
         uint32_t ra = 0, rb = 0;   // current run of small adjacent children
         for (int c = 0; c < nc; c++) {
-            const uint4 ci = __ldcg(&t.info[inf.x + (uint32_t)c]);
+            const uint32_t ck = inf.x + (uint32_t)c;
+            const uint4 ci = __ldcg(&t.info[ck]);
             const uint32_t cc = ci.w - ci.z;
             if (cc > GS) {
                 if (rb > ra) emit_group(t, ra, rb);
                 ra = rb = 0;
+                continue;
+            }
+            if (ci.y && sparse_node<D>(__ldcg(&t.cell[ck]).w, cc, S, cnt)) {
+                if (rb > ra) emit_group(t, ra, rb);
+                ra = rb = 0;
+                emit_split<D>(t, ck, S, cnt);
                 continue;
             }
             if (rb > ra && rb == ci.z && (ci.w - ra) <= GS) {
@@ -537,7 +584,7 @@ uint32_t group_walk_stack_entries() { return kGWStack; }
 template <int D, int PPL, bool COUNT>
 static cudaError_t gw_launch(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                              int ie, unsigned long long *inter, uint32_t *err, cudaStream_t st) {
-    cudaError_t e = launch_dep(k_make_groups, grid_blocks(p.n), 256, st, t, 32u * PPL);
+    cudaError_t e = launch_dep(k_make_groups<D>, grid_blocks(p.n), 256, st, t, 32u * PPL);
     if (e != cudaSuccess) return e;
     // one work stack per warp bounds the grid; groups number at most n
     int blocks = (int)(t.wl_warps / kGWWarps);
@@ -565,7 +612,7 @@ static cudaError_t gw_dims(const State &s, const StepParams &p, const Segs &g, c
 template <int D, int PPL>
 static cudaError_t gw_pot(const State &s, const StepParams &p, const Segs &g, const Tree &t,
                           uint32_t *err, double *epot, cudaStream_t st) {
-    k_make_groups<<<grid_blocks(p.n), 256, 0, st>>>(t, 32u * PPL);
+    k_make_groups<D><<<grid_blocks(p.n), 256, 0, st>>>(t, 32u * PPL);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int blocks = (int)(t.wl_warps / kGWWarps);

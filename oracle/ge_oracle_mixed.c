@@ -201,11 +201,43 @@ void or_walk_mixed(int64_t n, const float *x, const float *y, const float *z, co
  * most GS particles whose parent holds more (or that is the root); runs of
  * such nodes that are adjacent children of one parent are packed into one
  * group while the run holds at most GS particles; a leaf of more than GS
- * particles is cut into GS-particle pieces.  ranges receives {start, end}. */
+ * particles is cut into GS-particle pieces.  A sparse child (mean spacing
+ * more than four times its parent's: (s / S)^D C > 4^D c) is split down its
+ * subtree, depth first with an explicit stack of 256 entries, into leaves and
+ * nodes dense enough by the same reference (the node whole when the stack is
+ * full).  ranges receives {start, end}. */
 static void push_range(int64_t *ranges, int64_t *ng, int64_t a, int64_t b) {
     ranges[2 * *ng] = a;
     ranges[2 * *ng + 1] = b;
     (*ng)++;
+}
+
+static int sparse_node(int D, float s, int64_t c, float S, int64_t C) {
+    const double r = (double)s / (double)S;
+    const double rd = D == 2 ? r * r : r * r * r;
+    return rd * (double)C > (D == 2 ? 16.0 : 64.0) * (double)c;
+}
+
+static void split_sparse(const or_tree *t, int64_t node, float S, int64_t C, int64_t *ranges,
+                         int64_t *ng) {
+    enum { kStack = 256 };
+    const int D = t->dims, nq = 1 << D;
+    int64_t stack[kStack];
+    int top = 0;
+    stack[top++] = node;
+    while (top > 0) {
+        const int64_t k = stack[--top];
+        const int64_t a = t->start[k], b = t->end[k];
+        if (b <= a) continue;
+        int nc = 0;
+        for (int q = 0; q < nq; q++) nc += t->child[k * nq + q] != EMPTY;
+        if (is_leaf(t, k) || !sparse_node(D, t->size[k], b - a, S, C) || top + nc > kStack) {
+            push_range(ranges, ng, a, b);
+            continue;
+        }
+        for (int q = nq - 1; q >= 0; q--)
+            if (t->child[k * nq + q] != EMPTY) stack[top++] = t->child[k * nq + q];
+    }
 }
 
 static void make_groups(const or_tree *t, int64_t k, int64_t GS, int is_root, int64_t *ranges,
@@ -229,6 +261,12 @@ static void make_groups(const or_tree *t, int64_t k, int64_t GS, int is_root, in
             if (rb > ra) push_range(ranges, ng, ra, rb);
             ra = rb = 0;
             make_groups(t, c, GS, 0, ranges, ng);
+            continue;
+        }
+        if (!is_leaf(t, c) && sparse_node(t->dims, t->size[c], cb - ca, t->size[k], b - a)) {
+            if (rb > ra) push_range(ranges, ng, ra, rb);
+            ra = rb = 0;
+            split_sparse(t, c, t->size[k], b - a, ranges, ng);
             continue;
         }
         if (rb > ra && rb == ca && cb - ra <= GS) {
