@@ -172,6 +172,7 @@ __device__ __forceinline__ void emit_children(Tree &t, uint32_t k, uint32_t firs
         if (!((mask >> q) & 1u)) continue;
         t.cell[ci] = child_cell<D>(cell, half, (unsigned)q);
         t.info[ci] = make_uint4(0u, 0u, b[q], b[q + 1]);
+        atomicAdd(&t.endcnt[b[q + 1]], 1u);   // the walk layout's end counts
         // same-end ancestors: the child ends where its parent ends
         t.aux[ci] = make_uint4(ax.x + 1u, b[q + 1] == inf.w ? ax.y + 1u : 0u, k, 0u);
         ci++;
@@ -275,6 +276,7 @@ __device__ __forceinline__ float4 write_chain(Tree &t, uint32_t first, uint32_t 
         cell = child_cell<D>(cell, half, q);
         t.cell[k + 1] = cell;
         t.info[k + 1] = make_uint4(0u, 0u, st, en);
+        atomicAdd(&t.endcnt[en], 1u);
         t.aux[k + 1] = make_uint4(cax.x + i + 1u, cax.y + i + 1u, k, 0u);
         t.info[k] = make_uint4(k + 1, 1u << q, st, en);
         t.pend[k] = 1u;
@@ -524,9 +526,10 @@ __device__ __forceinline__ void rebuild_level_node(const StepParams &p, Tree &t,
     if (leader && ok) {
         t.info[k] = make_uint4(first, mask, inf.z, inf.w);
         t.pend[k] = (uint32_t)__popc(mask);
-        if (j) {
+        if (j) {   // the chain's first node (write_chain writes and counts the rest)
             t.cell[first] = c1;
             t.aux[first] = make_uint4(ax.x + 1u, ax.y + 1u, k, 0u);
+            atomicAdd(&t.endcnt[inf.w], 1u);
         }
         if (j)
             write_chain<D>(t, first, j, inf.z, inf.w, c1, make_uint4(ax.x + 1u, ax.y + 1u, k, 0u),
@@ -541,6 +544,7 @@ __device__ __forceinline__ void rebuild_level_node(const StepParams &p, Tree &t,
         const uint32_t same = hi == inf.w ? ax.y + 1u + j : 0u;
         t.cell[c] = cc;
         t.info[c] = make_uint4(0u, 0u, lo, hi);
+        if (!j) atomicAdd(&t.endcnt[hi], 1u);
         t.aux[c] = make_uint4(lvl, same, j ? first + j - 1u : k, 0u);
         if (is_leaf<D>(p, cnt, cc.w)) {
             // its upward pass waits for the end of the rebuilds, so that no
@@ -899,6 +903,7 @@ __device__ bool build_small_subtree_smem(const State &s, const StepParams &p, Tr
             t.cell[gid] = cl;
             const uint32_t gpar = nd.z == 0 ? R : base + nd.z - 1u;
             t.aux[gid] = make_uint4(nd.w & 0xFFFFu, nd.w >> 16, gpar, 0u);
+            atomicAdd(&t.endcnt[st + bb], 1u);   // the walk layout's end counts
         }
         put_walk<D>(t, gid, sm.cm[j], cl.w);
     }
@@ -1069,6 +1074,12 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     if (!keyed) {   // the roots' links above
         grid_barrier(bar_count, bar_gen, err);
         if (gtid == 0) stamp(t);
+        // the roots' ends (every other node's end is counted where it is made;
+        // the key passes count the key nodes')
+        for (uint32_t r = gtid; r < (uint32_t)g.S; r += nthreads) {
+            const uint32_t e = __ldcg(&t.info[r]).w;
+            if (e) atomicAdd(&t.endcnt[e], 1u);
+        }
     }
     const uint32_t nroots0 = le;   // keyed: the key passes' exact-rebuild roots
     const uint32_t bid = *(volatile uint32_t *)&t.meta[kMetaBuildId];   // this build's id
@@ -1220,32 +1231,43 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     // once it is written (an entry of this build carries its id), while other
     // blocks may still be rebuilding and queueing; it stops at a position
     // past the final count, known once every block has finished queueing.
-    // The wait polls the claimed entry (and, every eighth poll, the
-    // producers' count, which has a cache line of its own), backing off.
-    auto take = [&](uint32_t task) -> uint32_t {   // lane 0
-        uint32_t ns = 32;
-        for (uint32_t spins = 0;; spins++) {
-            if (task < t.small_cap) {
-                const uint2 e = __ldcv(&t.small[task]);
-                if (e.y == bid) {
-                    __threadfence();   // the subtree's nodes were written before its entry
-                    return e.x;
-                }
+    // poll(task): its entry (1), nothing yet (0), or the queue is final and
+    // ends before it, or the build failed (2).  Lane 0.
+    constexpr uint32_t kNotYet = 0xFFFFFFFEu;
+    auto poll = [&](uint32_t task) -> uint32_t {
+        if (task < t.small_cap) {
+            const uint2 e = __ldcv(&t.small[task]);
+            if (e.y == bid) {
+                __threadfence();   // the subtree's nodes were written before its entry
+                return e.x;
             }
-            if ((spins & 7u) == 7u) {
-                if (*(volatile uint32_t *)&t.kmeta[kKmProdDone] == gridDim.x) {
-                    __threadfence();
-                    if (task >= *(volatile uint32_t *)&t.meta[kMetaSmall]) return kEmpty;
-                }
-                if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return kEmpty;
-            }
-            if (spins > kSpinLimit) {
-                set_err(err, kErrSpin);
-                return kEmpty;
-            }
-            __nanosleep(ns);
-            if (ns < 2048) ns *= 2;
         }
+        if (*(volatile uint32_t *)&t.kmeta[kKmProdDone] == gridDim.x) {
+            __threadfence();
+            if (task >= *(volatile uint32_t *)&t.meta[kMetaSmall]) return kEmpty;
+        }
+        if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return kEmpty;
+        return kNotYet;
+    };
+    // the listed key nodes whose children are all final (known since phase
+    // 0): combined and passed upward 32 at a time, by warps waiting for
+    // queue entries or done with them
+    const uint32_t nready = keyed ? *(volatile uint32_t *)&t.kmeta[5] : 0u;
+    uint32_t *ready_ctr = &t.kmeta[kKeyMetaWords - 2];   // zeroed with the key passes' words
+    auto climb_ready = [&]() -> bool {   // false when none are left
+        uint32_t b = 0;
+        if (lane == 0) b = atomicAdd(ready_ctr, 32u);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (b >= nready) return false;
+        const uint32_t idx = b + lane;
+        if (idx < nready) {
+            const uint32_t cur = __ldcg(&t.slot_of[idx]);
+            put_walk<D>(t, cur, combine_children<D>(t, __ldcg(&t.info[cur])),
+                        __ldcg(&t.cell[cur]).w);
+            finish_upward<D>(t, cur);
+        }
+        __syncwarp();
+        return true;
     };
     {
         SubTreeSmem &sm = reinterpret_cast<SubTreeSmem *>(s_shared)[threadIdx.x >> 5];
@@ -1254,12 +1276,27 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
         // j-th finished subtree root whose upward pass is still to run, and the
         // warp runs 32 of them at once, so their atomics' round trips overlap
         uint32_t held = kEmpty, nheld = 0;
-        uint32_t R = kEmpty;
-        if (lane == 0) R = take(atomicAdd(&t.meta[kMetaP2Task], 1u));
-        R = __shfl_sync(0xffffffffu, R, 0);
-        while (R != kEmpty) {
-            uint32_t next = 0;
-            if (lane == 0) next = atomicAdd(&t.meta[kMetaP2Task], 1u);
+        uint32_t task = 0;
+        if (lane == 0) task = atomicAdd(&t.meta[kMetaP2Task], 1u);
+        bool ready_left = nready > 0;
+        uint32_t ns = 32, spins = 0;
+        while (true) {
+            uint32_t R = 0;
+            if (lane == 0) R = poll(task);
+            R = __shfl_sync(0xffffffffu, R, 0);
+            if (R == kEmpty) break;
+            if (R == kNotYet) {
+                if (ready_left && (ready_left = climb_ready())) continue;
+                if (++spins > kSpinLimit) {
+                    if (lane == 0) set_err(err, kErrSpin);
+                    break;
+                }
+                if (lane == 0) __nanosleep(ns);
+                if (ns < 256) ns *= 2;
+                continue;
+            }
+            ns = 32;
+            if (lane == 0) task = atomicAdd(&t.meta[kMetaP2Task], 1u);
             if (build_small_subtree_smem<D>(s, p, t, R, le, sm, wa, err)) {
                 if (lane == nheld) held = R;
                 if (++nheld == 32u) {
@@ -1272,39 +1309,31 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
                 build_small_subtree<D>(s, p, t, R, le, wa, err);   // passes its own leaves upward
             }
             __syncwarp();
-            if (lane == 0) R = take(next);
-            R = __shfl_sync(0xffffffffu, R, 0);
         }
         __syncwarp();
         if (held != kEmpty) finish_upward<D>(t, held);
         mark_holes(t, wa.next, wa.end);
         if (lane == 0 && wa.real) atomicAdd(&t.meta[kMetaReal], wa.real);
+        while (ready_left && (ready_left = climb_ready())) {
+        }
     }
     if (keyed) {
-        // the listed nodes (children all final) and the exact rebuilds'
-        // deferred leaves (already summed), upward from each: a warp takes 32
-        // at a time from a counter, so the warps that drew no small subtree
-        // above start at once and the climbs overlap the subtrees' own
-        const uint32_t nready = *(volatile uint32_t *)&t.kmeta[5];
-        const uint32_t total = nready + *(volatile uint32_t *)&t.kmeta[7];
+        // the exact rebuilds' deferred leaves (already summed), upward from
+        // each, 32 at a time (the list is final once the queue is)
+        const uint32_t ndone = *(volatile uint32_t *)&t.kmeta[7];
         uint32_t *take = &t.kmeta[kKeyMetaWords - 1];   // zeroed with the key passes' words
         while (true) {
             uint32_t b = 0;
             if (lane == 0) b = atomicAdd(take, 32u);
             b = __shfl_sync(0xffffffffu, b, 0);
-            if (b >= total) break;
-            const uint32_t idx = b + lane;
-            if (idx < nready) {
-                const uint32_t cur = __ldcg(&t.slot_of[idx]);
-                put_walk<D>(t, cur, combine_children<D>(t, __ldcg(&t.info[cur])),
-                            __ldcg(&t.cell[cur]).w);
-                finish_upward<D>(t, cur);
-            } else if (idx < total) {
-                finish_upward<D>(t, __ldcg(&t.kdone[idx - nready]));
-            }
+            if (b >= ndone) break;
+            if (b + lane < ndone) finish_upward<D>(t, __ldcg(&t.kdone[b + lane]));
             __syncwarp();
         }
     }
+    // root sizes whose square is not a normal float rule out packed entries
+    for (uint32_t sg = gtid; sg < (uint32_t)g.S; sg += nthreads)
+        if (!(g.box[sg].w < 1e19f)) atomicOr(&t.meta[kMetaBigRoot], 1u);
     grid_barrier(bar_count, bar_gen, err);
     if (gtid == 0) stamp(t);
     // slots in use (phase-2 holes included) and real nodes (the walk's extent)
@@ -1318,18 +1347,8 @@ k_build(State s, StepParams p, Segs g, Tree t, uint32_t *err, int keyed) {
     if ((*(volatile uint32_t *)err) & (kErrNodeCap | kErrSpin | kErrDepth)) return;
 
     // ---- phase 3: depth-first walk layout ------------------------------------
-    // histogram of range ends (endcnt was zeroed above, or holds the key
-    // nodes' ends from the emit pass); holes have an empty range ending at 0
-    // and are skipped
-    for (uint32_t k = key_nodes + gtid; k < slots; k += nthreads) {
-        const uint32_t e = __ldcg(&t.info[k]).w;
-        if (e) atomicAdd(&t.endcnt[e], 1u);
-    }
-    // root sizes whose square is not a normal float rule out packed entries
-    for (uint32_t sg = gtid; sg < (uint32_t)g.S; sg += nthreads)
-        if (!(g.box[sg].w < 1e19f)) atomicOr(&t.meta[kMetaBigRoot], 1u);
-    grid_barrier(bar_count, bar_gen, err);
-    if (gtid == 0) stamp(t);
+    // endcnt holds the histogram of range ends: the key nodes' from the emit
+    // pass (or zeroed above), every other node's added where it was made
     // inclusive scan of endcnt[0..n] in place, by block chunks; each chunk's
     // offset (the earlier chunks' total) is added where the scatter reads it:
     //   C(e) = endcnt[e] + s_boff[e / chunk]
