@@ -205,6 +205,43 @@ def test_two_disks_1m_theta_sweep(ge, ics, O, theta):
     assert inter == int(cnt.astype(np.int64).sum())
 
 
+def test_two_disks_1m_evolved_tree_and_walk(ge, ics, O):
+    """The 1M two-disk workload after 1,000 steps (theta 0.7): particles flung
+    out by the central masses make the box ~20x the disks, so long runs of
+    equal keys, about 17,000 exact-rebuild roots, roots larger than one warp
+    marks, chains of single-child nodes down to the minimum cell size and
+    handed-over block rebuilds all occur.  The tree of the next step is
+    bit-exact with the oracle's build of the same sorted state; FAST
+    accelerations within the conditioning-aware tolerance of the oracle
+    walk, with its interaction count."""
+    st = ics.two_disks2d(1 << 20, seed=0)
+    eps2 = 0.005 ** 2
+    p = ge.default_params(2, G=1.0, theta=0.7, eps2=eps2, leaf_cap=4, dt=1e-3,
+                          precision=ge.PREC_FAST)
+    with ge.Simulation(p) as s:
+        s.upload(st)
+        s.step(1000)
+        s.count_interactions(True)
+        s.step(1)
+        inter = s.stats().interactions
+        out = s.download()
+        t = s.export_tree()
+        bb = s.bounding_box()   # after the export: it reseeds the root nodes
+    assert bb[2] > 100.0   # the evolved box (it starts near 20)
+    x, y, m = out["x"], out["y"], out["m"]
+    h = O.build_tree(x, y, m, bb, leaf_cap=4, holder=True)
+    tr = h.to_numpy()
+    for a in ("pos", "size", "com", "mass", "start", "end", "next", "child"):
+        assert np.array_equal(t[a], getattr(tr, a)), a
+    prm = O.make_params(dims=2, theta=0.7, eps2=eps2, leaf_cap=4, dt=1e-3)
+    ax, ay, cnt, cond = O.walk(x, y, m, h, prm, nthreads=NT, want_counts=True, want_cond=True)
+    err = _rel_err([out["ax"], out["ay"]], [ax, ay], 2)
+    bound = np.maximum(FAST_TOL, 5e-6 * cond.astype(np.float64))
+    assert np.all(err <= bound), (err / bound).max()
+    assert np.mean(err <= FAST_TOL) >= 0.9999, np.mean(err <= FAST_TOL)
+    assert inter == int(cnt.astype(np.int64).sum())
+
+
 def test_plummer_3d_1m_fast(ge, ics, O):
     """3D Plummer sphere of 1,048,576 particles, theta 0.5, softening 0.01
     (added un-squared, physics3D.cpp:166): octree bit-exact with the
