@@ -390,9 +390,11 @@ int ge_sums_f64(ge_ctx *ctx, double *out);
    periodic); builds the tree when the last step's is not current. */
 int ge_energy_f64(ge_ctx *ctx, double *out);
 /* Timeline of the last tree build: device time (ns, from the first entry) at
-   each of its grid-wide barriers, in order (one per level of the large-node
-   phase, then the subtree phase, then the three layout steps).  Profiling aid
-   with no counterpart in the reference. */
+   each of its grid-wide barriers, in order (the pending-count phase, one per
+   level of the large-node phase, the rebuild and subtree phase, the
+   end-count scan), then the start of the layout scatter and the end of the
+   build (stamped by the last block to finish).  Profiling aid with no
+   counterpart in the reference. */
 int ge_build_timeline(ge_ctx *ctx, int32_t cap, uint64_t *ns, int32_t *count);
 
 /* --- 2D Morton sort without device allocation --------------------------
